@@ -1,0 +1,130 @@
+/*
+ * surfatt_gpu.h -- C ABI of the B200 engine for SurfATTPP's forward + adjoint
+ * misfit-gradient hot path (libsurfatt_gpu.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an sa_status code
+ * (0 = success); the reference's exceptions and Fortran `stop` become codes,
+ * and the adapter layer turns them back into the reference's behaviour.
+ * Per-call diagnostics are available from sa_ctx_error().
+ *
+ * Array layout (same as the reference):
+ *   2-D surface fields: Eigen column-major nx x ny, index ix + nx*iy.
+ *   Per-period media:   [iper][iy][ix] planes (one nx*ny plane per period).
+ *   3-D model fields:   (nx, ny, nz) row-major, as ModelGrid::vs3d_loc.
+ *   Depth kernels:      (nx, ny, nz, nper) row-major, nper fastest, as
+ *                       SurfGrid::sen_vs_loc (src/surf_grid.cpp:3-8).
+ *   Events:             one per (source, period) as SrcRec::events_local;
+ *                       receivers in CSR form rec_ptr[ne+1] / rec_idx[].
+ *
+ * Precision: SA_FP64 reproduces the reference's FP64 arithmetic (parity
+ * path); SA_FP32 sweeps in FP32 with FP64 T0, travel times, residuals,
+ * adjoint coefficients and accumulation.
+ */
+#ifndef SURFATT_GPU_H
+#define SURFATT_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sa_ctx sa_ctx;
+typedef struct sa_plan sa_plan;
+
+enum sa_status {
+    SA_OK = 0,
+    SA_ERR_ARG = 1,        /* invalid argument (reference: std::invalid_argument / runtime_error) */
+    SA_ERR_CUDA = 2,       /* CUDA runtime failure */
+    SA_ERR_NOCONV = 3,     /* a sweep hit its iteration cap (reference: stderr warning) */
+    SA_ERR_NOROOT = 4,     /* dispersion root not found (reference: stop 'Dispersion calculation failed') */
+    SA_ERR_NONFINITE = 5,  /* NaN/Inf in an output field */
+    SA_ERR_NOMEM = 6       /* device allocation failed */
+};
+
+enum sa_precision { SA_FP64 = 0, SA_FP32 = 1 };
+
+/* ---- context -------------------------------------------------------------- */
+/* Binds a CUDA device, a stream and a grow-only pool of device scratch. */
+int sa_ctx_create(int device, sa_ctx** out);
+void sa_ctx_destroy(sa_ctx* ctx);
+const char* sa_ctx_error(const sa_ctx* ctx);
+int sa_version(void);
+
+/* ---- eikonal:: drop-ins (host arrays, one solve) --------------------------- */
+
+/* Replaces eikonal::FSM_UW_PS_lonlat_2d (reference include/eikonal_solver.h:32-40,
+ * src/eikonal_solver.cpp:22-318).  spha/sphb/sphc/fun/T_out: nx*ny.
+ * niter (may be NULL) receives the number of sweep iterations. */
+int sa_eik_fwd_field(sa_ctx* ctx, int precision, int nx, int ny, const double* xx_deg,
+                     const double* yy_deg, const double* spha, const double* sphb,
+                     const double* sphc, const double* fun, double x0_deg, double y0_deg,
+                     double* T_out, int* niter);
+
+/* Replaces eikonal::FSM_O1_JSE_lonlat_2d (reference include/eikonal_solver.h:74-83,
+ * src/eikonal_solver.cpp:323-511).  Ta_out is unmasked, zero on the boundary. */
+int sa_eik_adj_field(sa_ctx* ctx, int precision, int nx, int ny, const double* xx_deg,
+                     const double* yy_deg, const double* spha, const double* sphb,
+                     const double* sphc, const double* T, int nr, const double* xrec_deg,
+                     const double* yrec_deg, const double* source_adj, double* Ta_out,
+                     int* niter);
+
+/* Replaces eikonal::mask_uniform_grid (reference include/eikonal_solver.h:85-89,
+ * src/eikonal_solver.cpp:514-536) on a host field. */
+int sa_mask_uniform_grid(int nx, int ny, const double* xx, const double* yy, double* table,
+                         double x0, double y0);
+
+/* ---- preproc::forward_for_event (batched) ---------------------------------- */
+
+/* A plan fixes the surface grid, the periods count and the event set
+ * (reference SrcRec::events_local, src/src_rec.cpp:138-228): unique sources,
+ * great-circle geometry per source and the scratch pool are built once and
+ * reused by every sa_plan_forward_adjoint() call (one per misfit evaluation).
+ * All arrays are host arrays; evlo/evla/stlo/stla in degrees. */
+int sa_plan_create(sa_ctx* ctx, int precision, int nx, int ny, int nper, const double* xx_deg,
+                   const double* yy_deg, int ne, const double* evlo, const double* evla,
+                   const int* iper, const int* rec_ptr, const int* rec_idx, int nsta,
+                   const double* stlo, const double* stla, sa_plan** out);
+void sa_plan_destroy(sa_plan* plan);
+
+/* Replay the whole misfit evaluation as one CUDA graph when the argument
+ * pointers repeat (default on). */
+int sa_plan_set_graph(sa_plan* plan, int enable);
+
+/* One forward (+ adjoint) evaluation of every event of the plan: replaces
+ * preproc::forward_for_event (reference include/preproc.h:14,
+ * src/preproc.cpp:71-148) with accumulate_kernels (:19-34), isotropic
+ * branch, is_kden = false.
+ *   svel           [nper][ny][nx] phase/group velocity (device)
+ *   m11, m12, m22  [nper][ny][nx] media (device) or all NULL for the flat
+ *                  isotropic surface (m11 = m22 = 1, m12 = -0, reference
+ *                  src/surf_grid.cpp:178-190)
+ *   tt_obs, weight [npair] observed times and weights (device)
+ * Outputs (device, any may be NULL unless required):
+ *   syn [npair]; adj_s [nper][ny][nx] (overwritten, FP64); chi (1 double,
+ *   0.5*sum w r^2 over all events); fwd_iters/adj_iters/status [ne].
+ *   stream: a cudaStream_t, or NULL for the context's stream.
+ * Returns SA_ERR_NOCONV / SA_ERR_NONFINITE when any event reports it. */
+int sa_plan_forward_adjoint(sa_plan* plan, const double* svel, const double* m11,
+                            const double* m12, const double* m22, const double* tt_obs,
+                            const double* weight, int calc_adj, double* syn, double* adj_s,
+                            double* chi, int* fwd_iters, int* adj_iters, int* status,
+                            void* stream);
+
+/* Host-array convenience over a transient plan (uploads, runs, downloads):
+ * the drop-in for one call of preproc::forward_for_event. */
+int sa_forward_for_events(sa_ctx* ctx, int precision, int nx, int ny, int nper,
+                          const double* xx_deg, const double* yy_deg, const double* svel,
+                          const double* m11, const double* m12, const double* m22, int ne,
+                          const double* evlo, const double* evla, const int* iper,
+                          const int* rec_ptr, const int* rec_idx, int nsta, const double* stlo,
+                          const double* stla, const double* tt_obs, const double* weight,
+                          int calc_adj, double* syn, double* adj_s, double* chi, int* fwd_iters,
+                          int* adj_iters);
+
+/* Full-field outputs for testing (device arrays [ne][ny][nx], may be NULL):
+ * forward T and the masked adjoint field of the next sa_plan_forward_adjoint. */
+int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,126 @@
+/*
+ * CPU oracle for the SurfATTPP forward + adjoint misfit-gradient path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain C++ restatement, operation
+ * for operation, of the reference's CPU arithmetic.  It is the parity checker for
+ * the CUDA engine in surfattpp_b200/ and the timed CPU baseline; nothing in the
+ * product links or calls it.
+ *
+ * Build rule: -O2 -ffp-contract=off, no -march, no -ffast-math, so every
+ * expression rounds in source order exactly as written (the reference's own
+ * release build uses -O3 -march=native, whose FMA contraction is machine
+ * dependent; the oracle fixes the uncontracted IEEE semantics).
+ *
+ * Storage conventions follow the reference:
+ *   2-D fields are Eigen column-major (nx x ny): index ix + nx*iy.
+ *   Per-period media are [iper][iy][ix] planes here (one plane per period).
+ *   Depth kernels sen_* are row-major (nx, ny, nz, nper), nper fastest
+ *   (reference src/surf_grid.cpp:5-8).
+ */
+#ifndef SURFATT_ORACLE_H
+#define SURFATT_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* eikonal::FSM_UW_PS_lonlat_2d (src/eikonal_solver.cpp:22-318).
+ * Returns 0, or -1 for a grid smaller than 3x3.  *niter = sweep iterations run. */
+int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                const double* spha, const double* sphb, const double* sphc,
+                const double* fun, double x0_deg, double y0_deg,
+                double* T_out, int* niter);
+
+/* eikonal::FSM_O1_JSE_lonlat_2d (src/eikonal_solver.cpp:323-511). */
+int orc_eik_adj(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                const double* spha, const double* sphb, const double* sphc,
+                const double* T, int nr, const double* xrec_deg,
+                const double* yrec_deg, const double* source_adj,
+                double* Ta_out, int* niter);
+
+/* eikonal::mask_uniform_grid (src/eikonal_solver.cpp:514-536). */
+void orc_mask_uniform_grid(int nx, int ny, const double* xx, const double* yy,
+                           double* table, double x0, double y0);
+
+/* interp2d (include/utils.h:358-409). */
+void orc_interp2d(int nx, int ny, const double* xgrid, const double* ygrid,
+                  const double* z, int nq, const double* xq, const double* yq,
+                  double* zq);
+
+/* preproc::forward_for_event over a flat event list (src/preproc.cpp:71-148),
+ * isotropic branch, is_kden = false.
+ *   svel, m11, m12, m22 : [nper][ny][nx] planes (column-major per period)
+ *   events              : evlo[ne], evla[ne], iper[ne], rec_ptr[ne+1] (CSR),
+ *                         rec_idx[rec_ptr[ne]] station indices
+ *   stations            : stlo[nsta], stla[nsta]
+ *   obs per pair        : tt_obs[rec_ptr[ne]], weight[rec_ptr[ne]]
+ * Outputs: syn[rec_ptr[ne]] synthetic times; if calc_adj, adj_s [nper][ny][nx]
+ * is ACCUMULATED (caller zeroes it) and the misfit is returned in *chi.
+ * fwd_iters/adj_iters (may be NULL) receive per-event iteration counts.
+ * nthreads > 1 deals events round-robin over threads (reference
+ * include/parallel.h:39-41) and sums per-thread accumulators in thread order. */
+int orc_forward_for_events(int nx, int ny, int nper, const double* xx_deg,
+                           const double* yy_deg, const double* svel,
+                           const double* m11, const double* m12, const double* m22,
+                           int ne, const double* evlo, const double* evla,
+                           const int* iper, const int* rec_ptr, const int* rec_idx,
+                           const double* stlo, const double* stla,
+                           const double* tt_obs, const double* weight,
+                           int calc_adj, double* syn, double* adj_s, double* chi,
+                           int* fwd_iters, int* adj_iters, int nthreads);
+
+/* preproc::combine_kernels, vs-only branch (src/preproc.cpp:276-304).
+ *   adj_s [nper][ny][nx]; vs3d, vp3d (nx, ny, nz) row-major;
+ *   sen_vs/vp/rho (nx, ny, nz, nper) row-major; ker_vs (nx, ny, nz) out. */
+void orc_combine_kernels_vs(int nx, int ny, int nz, int nper, const double* adj_s,
+                            const double* vs3d, const double* vp3d,
+                            const double* sen_vs, const double* sen_vp,
+                            const double* sen_rho, double* ker_vs);
+
+/* Brocher (2005) relations (include/utils.h:185-234). */
+double orc_vs2vp(double vs);
+double orc_vp2rho(double vp);
+double orc_dalpha_dbeta(double vs);
+double orc_drho_dalpha(double vp);
+
+/* surfdisp96 (src/surfker/surfdisp96.f:57-373) via the C ABI surfdisp96_c.
+ * Returns 0 on success, 1 when the root search failed for the fundamental mode
+ * (where the Fortran executes `stop 'Dispersion calculation failed'`). */
+int orc_surfdisp96(const float* thkm, const float* vpm, const float* vsm,
+                   const float* rhom, int nlayer, int iflsph, int iwave, int mode,
+                   int igr, int kmax, const double* t, double* cg);
+
+/* sregn96_hti (src/surfker/sregn96.f90:1745-1849). All arrays length nlayer. */
+void orc_sregn96_hti(const float* thk, const float* vp, const float* vs,
+                     const float* rhom, int nlayer, double* t, double* cp,
+                     double* cg, double* dispu, double* dispw, double* stressu,
+                     double* stressw, double* dc2da, double* dc2db, double* dc2dh,
+                     double* dc2dr, double* dc2dgc, double* dc2dgs, int iflsph);
+
+/* sregn96 (src/surfker/sregn96.f90:1640-1743). */
+void orc_sregn96(const float* thk, const float* vp, const float* vs,
+                 const float* rhom, int nlayer, double* t, double* cp, double* cg,
+                 double* dispu, double* dispw, double* stressu, double* stressw,
+                 double* dc2da, double* dc2db, double* dc2dh, double* dc2dr,
+                 int iflsph);
+
+/* SurfGrid::fwdsurf over columns (src/surf_grid.cpp:194-245) with the
+ * Brocher branch (use_alpha_beta_rho = false).
+ *   zgrid[nz]; vs3d (nx, ny, nz) row-major; periods[nper]
+ *   svel out: [nper][ny][nx] planes.  status[nx*ny] (0 ok, 1 no root). */
+int orc_fwdsurf(int nx, int ny, int nz, const double* zgrid, const double* vs3d,
+                int nper, const double* periods, int iwave, int igr,
+                double* svel, int* status, int nthreads);
+
+/* SurfGrid::compute_dispersion_kernel for phase velocity (PH) columns, which
+ * always runs depthkernelHTI1d (src/surf_grid.cpp:247-305,
+ * src/surfdisp.cpp:481-547).  sen_vs/vp/rho out (nx, ny, nz, nper) row-major. */
+int orc_depthkernel_hti(int nx, int ny, int nz, const double* zgrid,
+                        const double* vs3d, int nper, const double* periods,
+                        double* sen_vs, double* sen_vp, double* sen_rho,
+                        int* status, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,201 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` as the parity checker and the timed CPU
+restatement of the reference.  The product (``surfattpp_b200``) never imports it.
+
+Array conventions: 2-D fields are numpy arrays shaped (ny, nx) in C order, which
+is the reference's Eigen column-major (nx x ny) layout, index ix + nx*iy.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (g++ only, a few seconds)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    L = C.CDLL(_LIB_PATH)
+    i, d = C.c_int, C.c_double
+    L.orc_eik_fwd.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, _dp, C.POINTER(i)]
+    L.orc_eik_fwd.restype = i
+    L.orc_eik_adj.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp,
+                              C.POINTER(i)]
+    L.orc_eik_adj.restype = i
+    L.orc_mask_uniform_grid.argtypes = [i, i, _dp, _dp, _dp, d, d]
+    L.orc_interp2d.argtypes = [i, i, _dp, _dp, _dp, i, _dp, _dp, _dp]
+    L.orc_forward_for_events.argtypes = [i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _dp, _dp,
+                                         _ip, _ip, _ip, _dp, _dp, _dp, _dp, i, _dp, _dp,
+                                         C.POINTER(d), _ip, _ip, i]
+    L.orc_combine_kernels_vs.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    for f in ("orc_vs2vp", "orc_vp2rho", "orc_dalpha_dbeta", "orc_drho_dalpha"):
+        getattr(L, f).argtypes = [d]
+        getattr(L, f).restype = d
+    L.orc_surfdisp96.argtypes = [_fp, _fp, _fp, _fp, i, i, i, i, i, i, _dp, _dp]
+    L.orc_surfdisp96.restype = i
+    L.orc_sregn96_hti.argtypes = [_fp, _fp, _fp, _fp, i, _dp, _dp, _dp] + [_dp] * 10 + [i]
+    L.orc_sregn96.argtypes = [_fp, _fp, _fp, _fp, i, _dp, _dp, _dp] + [_dp] * 8 + [i]
+    L.orc_fwdsurf.argtypes = [i, i, i, _dp, _dp, i, _dp, i, i, _dp, _ip, i]
+    L.orc_depthkernel_hti.argtypes = [i, i, i, _dp, _dp, i, _dp, _dp, _dp, _dp, _ip, i]
+    _lib = L
+    return L
+
+
+def _c(a, dt=np.float64):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def eik_fwd(xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg, y0_deg):
+    """eikonal::FSM_UW_PS_lonlat_2d. Fields (ny, nx). Returns (T, niter)."""
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    nx, ny = xx.size, yy.size
+    T = np.zeros((ny, nx))
+    it = C.c_int(0)
+    rc = lib().orc_eik_fwd(nx, ny, xx, yy, _c(spha), _c(sphb), _c(sphc), _c(fun),
+                           float(x0_deg), float(y0_deg), T, C.byref(it))
+    if rc != 0:
+        raise ValueError("Grid must be at least 3x3")
+    return T, it.value
+
+
+def eik_adj(xx_deg, yy_deg, spha, sphb, sphc, T, xrec, yrec, sadj):
+    """eikonal::FSM_O1_JSE_lonlat_2d. Returns (Ta, niter)."""
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    nx, ny = xx.size, yy.size
+    Ta = np.zeros((ny, nx))
+    it = C.c_int(0)
+    xr, yr, sa = _c(xrec).ravel(), _c(yrec).ravel(), _c(sadj).ravel()
+    lib().orc_eik_adj(nx, ny, xx, yy, _c(spha), _c(sphb), _c(sphc), _c(T), xr.size,
+                      xr if xr.size else np.zeros(1), yr if yr.size else np.zeros(1),
+                      sa if sa.size else np.zeros(1), Ta, C.byref(it))
+    return Ta, it.value
+
+
+def mask_uniform_grid(xx_deg, yy_deg, table, x0, y0):
+    t = _c(table).copy()
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    lib().orc_mask_uniform_grid(xx.size, yy.size, xx, yy, t, float(x0), float(y0))
+    return t
+
+
+def interp2d(xgrid, ygrid, z, xq, yq):
+    xg, yg = _c(xgrid), _c(ygrid)
+    xq, yq = _c(xq).ravel(), _c(yq).ravel()
+    out = np.zeros(xq.size)
+    lib().orc_interp2d(xg.size, yg.size, xg, yg, _c(z), xq.size, xq, yq, out)
+    return out
+
+
+def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, nthreads=1):
+    """preproc::forward_for_event over an event set.
+
+    svel/m11/m12/m22: (nper, ny, nx).  ``ev`` is a dict with evlo, evla, iper,
+    rec_ptr, rec_idx, stlo, stla, tt_obs, weight (see tests/workloads.py).
+    Returns dict(syn, adj_s, chi, fwd_iters, adj_iters).
+    """
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    nper, ny, nx = svel.shape
+    ne = len(ev["evlo"])
+    nrec = int(ev["rec_ptr"][-1])
+    syn = np.zeros(max(nrec, 1))
+    adj_s = np.zeros((nper, ny, nx))
+    chi = C.c_double(0.0)
+    fi = np.zeros(max(ne, 1), np.int32)
+    ai = np.zeros(max(ne, 1), np.int32)
+    lib().orc_forward_for_events(
+        nx, ny, nper, xx, yy, _c(svel), _c(m11), _c(m12), _c(m22), ne,
+        _c(ev["evlo"]), _c(ev["evla"]), _c(ev["iper"], np.int32), _c(ev["rec_ptr"], np.int32),
+        _c(ev["rec_idx"], np.int32), _c(ev["stlo"]), _c(ev["stla"]), _c(ev["tt_obs"]),
+        _c(ev["weight"]), int(calc_adj), syn, adj_s, C.byref(chi), fi, ai, int(nthreads))
+    return dict(syn=syn[:nrec], adj_s=adj_s, chi=chi.value, fwd_iters=fi[:ne], adj_iters=ai[:ne])
+
+
+def combine_kernels_vs(adj_s, vs3d, vp3d, sen_vs, sen_vp, sen_rho):
+    nper, ny, nx = adj_s.shape
+    nz = vs3d.shape[2]
+    ker = np.zeros((nx, ny, nz))
+    lib().orc_combine_kernels_vs(nx, ny, nz, nper, _c(adj_s), _c(vs3d), _c(vp3d), _c(sen_vs),
+                                 _c(sen_vp), _c(sen_rho), ker)
+    return ker
+
+
+def vs2vp(vs):
+    return lib().orc_vs2vp(float(vs))
+
+
+def vp2rho(vp):
+    return lib().orc_vp2rho(float(vp))
+
+
+def dalpha_dbeta(vs):
+    return lib().orc_dalpha_dbeta(float(vs))
+
+
+def drho_dalpha(vp):
+    return lib().orc_drho_dalpha(float(vp))
+
+
+def surfdisp96(thk, vp, vs, rho, periods, iflsph=1, iwave=2, mode=1, igr=0):
+    """surfdisp96_c. Returns (velocities, status)."""
+    t = _c(periods)
+    cg = np.zeros(t.size)
+    st = lib().orc_surfdisp96(_c(thk, np.float32), _c(vp, np.float32), _c(vs, np.float32),
+                              _c(rho, np.float32), len(thk), iflsph, iwave, mode, igr, t.size,
+                              t, cg)
+    return cg, st
+
+
+def sregn96_hti(thk, vp, vs, rho, t, cp, iflsph=1):
+    """sregn96_hti_c for one period. Returns dict of outputs."""
+    n = len(thk)
+    outs = {k: np.zeros(n) for k in ("dispu", "dispw", "stressu", "stressw", "dc2da", "dc2db",
+                                      "dc2dh", "dc2dr", "dc2dgc", "dc2dgs")}
+    tt, cpp, cg = np.array([float(t)]), np.array([float(cp)]), np.zeros(1)
+    lib().orc_sregn96_hti(_c(thk, np.float32), _c(vp, np.float32), _c(vs, np.float32),
+                          _c(rho, np.float32), n, tt, cpp, cg, *outs.values(), iflsph)
+    outs["cp"], outs["cg"] = cpp[0], cg[0]
+    return outs
+
+
+def fwdsurf(zgrid, vs3d, periods, iwave=2, igr=0, nthreads=1):
+    """SurfGrid::fwdsurf: vs3d (nx, ny, nz) -> svel (nper, ny, nx), status (ny, nx)."""
+    nx, ny, nz = vs3d.shape
+    p = _c(periods)
+    svel = np.zeros((p.size, ny, nx))
+    st = np.zeros((ny, nx), np.int32)
+    lib().orc_fwdsurf(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, iwave, igr, svel, st,
+                      int(nthreads))
+    return svel, st
+
+
+def depthkernel_hti(zgrid, vs3d, periods, nthreads=1):
+    """compute_dispersion_kernel (PH): returns sen_vs, sen_vp, sen_rho (nx,ny,nz,nper), status."""
+    nx, ny, nz = vs3d.shape
+    p = _c(periods)
+    shp = (nx, ny, nz, p.size)
+    sv, sp, sr = np.zeros(shp), np.zeros(shp), np.zeros(shp)
+    st = np.zeros((ny, nx), np.int32)
+    lib().orc_depthkernel_hti(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
+                              int(nthreads))
+    return sv, sp, sr, st

@@ -1,0 +1,128 @@
+"""ctypes binding of libsurfatt_gpu.so (the C ABI declared in include/surfatt_gpu.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsurfatt_gpu.so")
+
+SA_OK, SA_ERR_ARG, SA_ERR_CUDA, SA_ERR_NOCONV, SA_ERR_NOROOT, SA_ERR_NONFINITE, SA_ERR_NOMEM = range(7)
+SA_FP64, SA_FP32 = 0, 1
+STATUS_NAMES = {0: "SA_OK", 1: "SA_ERR_ARG", 2: "SA_ERR_CUDA", 3: "SA_ERR_NOCONV",
+                4: "SA_ERR_NOROOT", 5: "SA_ERR_NONFINITE", 6: "SA_ERR_NOMEM"}
+
+# Every symbol include/surfatt_gpu.h declares.
+EXPORTED = (
+    "sa_ctx_create", "sa_ctx_destroy", "sa_ctx_error", "sa_version",
+    "sa_eik_fwd_field", "sa_eik_adj_field", "sa_mask_uniform_grid",
+    "sa_plan_create", "sa_plan_destroy", "sa_plan_set_graph", "sa_plan_forward_adjoint",
+    "sa_forward_for_events", "sa_plan_debug_fields",
+)
+
+
+class SAError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class NoConvergence(SAError):
+    pass
+
+
+_lib = None
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m surfattpp_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    i, d = C.c_int, C.c_double
+    L.sa_ctx_create.argtypes = [i, C.POINTER(_vp)]
+    L.sa_ctx_destroy.argtypes = [_vp]
+    L.sa_ctx_error.argtypes = [_vp]
+    L.sa_ctx_error.restype = C.c_char_p
+    L.sa_version.restype = i
+    L.sa_eik_fwd_field.argtypes = [_vp, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, _dp,
+                                   C.POINTER(i)]
+    L.sa_eik_adj_field.argtypes = [_vp, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _vp, _vp, _vp,
+                                   _dp, C.POINTER(i)]
+    L.sa_mask_uniform_grid.argtypes = [i, i, _dp, _dp, _dp, d, d]
+    L.sa_plan_create.argtypes = [_vp, i, i, i, i, _dp, _dp, i, _vp, _vp, _vp, _vp, _vp, i, _vp,
+                                 _vp, C.POINTER(_vp)]
+    L.sa_plan_destroy.argtypes = [_vp]
+    L.sa_plan_set_graph.argtypes = [_vp, i]
+    L.sa_plan_forward_adjoint.argtypes = [_vp] + [_vp] * 6 + [i] + [_vp] * 6 + [_vp]
+    L.sa_plan_debug_fields.argtypes = [_vp, _vp, _vp]
+    L.sa_forward_for_events.argtypes = [_vp, i, i, i, i, _dp, _dp, _dp, _vp, _vp, _vp, i, _dp,
+                                        _dp, _ip, _ip, _ip, i, _dp, _dp, _dp, _dp, i, _dp, _dp,
+                                        C.POINTER(d), _ip, _ip]
+    if hasattr(L, "sa_surfdisp_batch"):
+        L.sa_surfdisp_batch.argtypes = [_vp] * 2 + [i] * 4 + [_vp] * 4 + [i] * 4 + [_vp] * 3
+        L.sa_depthkernel_batch.argtypes = [_vp] * 2 + [i] * 3 + [_vp] * 7 + [_vp]
+        L.sa_combine_kernels_vs.argtypes = [_vp] + [i] * 4 + [_vp] * 7 + [_vp]
+    _lib = L
+    return L
+
+
+def check(ctx, rc):
+    if rc == SA_OK:
+        return
+    msg = lib().sa_ctx_error(ctx).decode() if ctx else ""
+    if rc == SA_ERR_NOCONV:
+        raise NoConvergence(rc, msg)
+    raise SAError(rc, msg)
+
+
+class Context:
+    """One CUDA device + stream (sa_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        rc = lib().sa_ctx_create(device, C.byref(h))
+        if rc != SA_OK:
+            raise SAError(rc, "sa_ctx_create failed (no CUDA device?)")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().sa_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(int(os.environ.get("SA_DEVICE", "0")))
+    return _default_ctx
+
+
+def ptr(t) -> int | None:
+    """Device pointer of a torch tensor (or None)."""
+    if t is None:
+        return None
+    return t.data_ptr()

@@ -1,0 +1,437 @@
+// Persistent (source, period) batch kernel, templated on the sweep precision.
+//
+// One warp per event, events pulled from a device work queue (atomicAdd on a
+// counter), so solves of uneven iteration count balance across the GPU.  Per
+// event, fused: forward FSM -> T = tau*T0 -> receiver interpolation ->
+// residuals and misfit -> adjoint source -> face fluxes -> adjoint FSM ->
+// source mask -> adj_s += Ta * svel^-3 (FP64 atomics).
+// Reference: preproc::forward_for_event (src/preproc.cpp:71-148).
+#pragma once
+#include "common.cuh"
+#include "event_common.cuh"
+#include "fsm.cuh"
+#include "launch.h"
+
+#include <type_traits>
+
+namespace sa {
+
+template <class S>
+struct BatchArgs {
+    Grid g;
+    int iso;
+    const S* fun;          // sweep-precision slowness planes
+    const double* fun64;   // FP64 slowness planes (fun0, T0 for T)
+    const double* inv3;
+    const S* a_f_row;
+    const double* a_a_row64;
+    S b_iso;
+    double b_iso64;
+    const S* a_f;
+    const S* b_p;
+    const S* c_f;
+    const double* b_p64;
+    const double* a_a64;
+    const double* c_a64;
+    const S* G;
+    const S* Gx;
+    const S* Gy;
+    const double* G64;
+    Events ev;
+    Outputs out;
+    Scratch sc;
+    int mode;
+};
+
+// Scratch slot layout (bytes, every plane 256-byte aligned).
+struct SlotLayout {
+    size_t tau, tst, T, A, B, D, delta, Ta, W, sadj, syn, total;
+};
+template <class S>
+__host__ __device__ inline SlotLayout slot_layout(int nx, int ny) {
+    const size_t n = (size_t)nx * ny;
+    SlotLayout L;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t r = o;
+        o += align_up(bytes, 256);
+        return r;
+    };
+    L.tau = take(n * sizeof(S));
+    L.tst = take(n * sizeof(S));
+    L.T = take(n * sizeof(double));
+    L.delta = take(n * sizeof(double));
+    L.sadj = take(n * sizeof(double));
+    L.syn = take(n * sizeof(double));
+    if (sizeof(S) == sizeof(double)) {
+        L.A = take(n * sizeof(double));
+        L.B = take(n * sizeof(double));
+        L.D = take(n * sizeof(double));
+        L.Ta = take(n * sizeof(double));
+        L.W = 0;
+    } else {
+        L.A = L.B = L.D = 0;
+        L.W = take(5 * n * sizeof(float));
+        L.Ta = take(n * sizeof(float));
+    }
+    L.total = o;
+    return L;
+}
+
+template <class S>
+__device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo& si, int ip,
+                                            int src, S* tau, S* tst, double* T, int& iters,
+                                            int& status) {
+    const Grid& g = B.g;
+    const int nx = g.nx, ny = g.ny;
+    const size_t n = (size_t)nx * ny;
+    const int lane = threadIdx.x & 31;
+    const double fun0_64 = bilinear64(B.fun64 + (size_t)ip * n, nx, si.idx0, si.idy0, si.r1, si.r2);
+    using Pol = typename std::conditional<sizeof(S) == sizeof(double), FwdPolicy<double>,
+                                          FwdPolicyDelta32>::type;
+    Pol P;
+    P.nx = nx;
+    P.ny = ny;
+    if constexpr (sizeof(S) == sizeof(double)) {
+        P.dx = g.dx;
+        P.dy = g.dy;
+    } else {
+        P.idx = (float)(1.0 / g.dx);
+        P.idy = (float)(1.0 / g.dy);
+    }
+    P.fun0 = (S)fun0_64;
+    P.G = B.G + (size_t)src * n;
+    P.Gx = B.Gx + (size_t)src * n;
+    P.Gy = B.Gy + (size_t)src * n;
+    P.fun = B.fun + (size_t)ip * n;
+    P.a_row = B.a_f_row;
+    P.b_iso = B.b_iso;
+    P.a_pl = B.iso ? nullptr : B.a_f + (size_t)ip * n;
+    P.b_pl = B.iso ? nullptr : B.b_p + (size_t)ip * n;
+    P.c_pl = B.iso ? nullptr : B.c_f + (size_t)ip * n;
+    P.tau = tau;
+    P.tau_start = tst;
+    P.fix_x0 = si.fix_x0;
+    P.fix_x1 = si.fix_x1;
+    P.yy = g.yy;
+    P.y0 = si.y0;
+    P.dy64 = g.dy;
+    // initial tau (src/eikonal_solver.cpp:118-129); FP32 stores u = tau - 1
+    const S off = (sizeof(S) == sizeof(double)) ? S(0) : S(1);
+    for (size_t k = lane; k < n; k += 32) {
+        const int iy = (int)(k / nx), ix = (int)(k % nx);
+        const bool fixed =
+            fabs((g.yy[iy] - si.y0) / g.dy) <= 1.0 && ix >= si.fix_x0 && ix <= si.fix_x1;
+        const S v = (fixed ? S(1) : S(10)) - off;
+        tau[k] = v;
+        tst[k] = v;
+    }
+    __syncwarp();
+    iters = 0;
+    for (int iter = 0; iter < 2000; iter++) {
+        double l1 = 0.0, linf = 0.0;
+        systolic_sweep(P, +1, +1, false, l1, linf);
+        systolic_sweep(P, +1, -1, false, l1, linf);
+        systolic_sweep(P, -1, +1, false, l1, linf);
+        systolic_sweep(P, -1, -1, true, l1, linf);
+        iters = iter + 1;
+        const double L1 = warp_sum(l1) / (double)(nx * ny);
+        const double Linf = warp_max(linf);
+        if (L1 < 1e-4 && Linf < 1e-4) break;
+        if (iter == 1999) status = ST_NOCONV;
+    }
+    // T = tau * T0 in FP64 (src/eikonal_solver.cpp:317)
+    const double* G64 = B.G64 + (size_t)src * n;
+    bool finite = true;
+    for (size_t k = lane; k < n; k += 32) {
+        const double t0 = G64[k] * fun0_64;
+        const double t = (sizeof(S) == sizeof(double)) ? (double)tau[k] * t0
+                                                         : t0 + (double)tau[k] * t0;
+        T[k] = t;
+        if (!isfinite(t)) finite = false;
+    }
+    if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;
+    __syncwarp();
+    return fun0_64;
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= B.sc.nslots) return;
+    const Grid& g = B.g;
+    const int nx = g.nx, ny = g.ny;
+    const size_t n = (size_t)nx * ny;
+    const SlotLayout L = slot_layout<S>(nx, ny);
+    unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
+    S* P_tau = reinterpret_cast<S*>(base + L.tau);
+    S* P_tst = reinterpret_cast<S*>(base + L.tst);
+    double* P_T = reinterpret_cast<double*>(base + L.T);
+    double* P_delta = reinterpret_cast<double*>(base + L.delta);   // zero between events
+    double* P_sadj = reinterpret_cast<double*>(base + L.sadj);
+    double* P_syn = reinterpret_cast<double*>(base + L.syn);
+
+    for (;;) {
+        const unsigned int e = warp_next_event(B.sc.queue);
+        if (e >= (unsigned)B.ev.ne) break;
+        const int ip = B.ev.iper[e];
+        const int r0 = B.ev.rec_ptr[e];
+        const int nr = B.ev.rec_ptr[e + 1] - r0;
+        const SrcInfo si = source_info(g, B.ev.evlo[e], B.ev.evla[e]);
+        int status = ST_OK;
+        const double* T = P_T;
+
+        if (B.mode != MODE_ADJ_ONLY) {
+            int iters = 0;
+            fwd_solve<S>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_T, iters, status);
+            if (lane == 0 && B.out.fwd_iters) B.out.fwd_iters[e] = iters;
+            if (B.out.T_out)
+                for (size_t k = lane; k < n; k += 32) B.out.T_out[(size_t)e * n + k] = P_T[k];
+            // synthetic times at the receivers (src/preproc.cpp:105-115)
+            for (int ir = lane; ir < nr; ir += 32) {
+                const int st = B.ev.rec_idx[r0 + ir];
+                const double ts =
+                    interp2d_pt(g.xx_deg, nx, g.yy_deg, ny, P_T, B.ev.stlo[st], B.ev.stla[st]);
+                if (B.out.syn) B.out.syn[r0 + ir] = ts;
+                P_syn[ir] = ts;
+                P_sadj[ir] = B.ev.weight[r0 + ir] * (ts - B.ev.tt_obs[r0 + ir]);
+            }
+            __syncwarp();
+            if (B.mode == MODE_FWD_ADJ && lane == 0 && B.out.chi_ev) {
+                double s = 0.0;   // src/preproc.cpp:142, receivers in order
+                for (int ir = 0; ir < nr; ir++) {
+                    const double r = P_syn[ir] - B.ev.tt_obs[r0 + ir];
+                    s += B.ev.weight[r0 + ir] * (r * r);
+                }
+                B.out.chi_ev[e] = 0.5 * s;
+            }
+        } else {
+            T = B.ev.T_in + (size_t)e * n;
+            for (int ir = lane; ir < nr; ir += 32) P_sadj[ir] = B.ev.sadj[r0 + ir];
+            __syncwarp();
+        }
+
+        if (B.mode != MODE_FWD) {
+            // adjoint source (src/eikonal_solver.cpp:354-375), receivers in order
+            if (lane == 0) spread_delta(g, B.ev, r0, nr, P_sadj, P_delta, false);
+            __syncwarp();
+            const double* a_a = B.iso ? nullptr : B.a_a64 + (size_t)ip * n;
+            const double* b_p = B.iso ? nullptr : B.b_p64 + (size_t)ip * n;
+            const double* c_a = B.iso ? nullptr : B.c_a64 + (size_t)ip * n;
+            auto faceA = [&](int ix, int iy) -> double {
+                return B.iso ? face_a1_iso(T, B.a_a_row64[iy], nx, ix, iy, g.dx, g.dy)
+                             : face_a1(T, a_a, c_a, nx, ix, iy, g.dx, g.dy);
+            };
+            auto faceB = [&](int ix, int iy) -> double {
+                return B.iso ? face_b1_iso(T, B.b_iso64, B.b_iso64, nx, ix, iy, g.dx, g.dy)
+                             : face_b1(T, b_p, c_a, nx, ix, iy, g.dx, g.dy);
+            };
+            int iters = 0;
+            const bool big = nx >= 3 && ny >= 3;
+            if constexpr (sizeof(S) == sizeof(double)) {
+                double* P_A = reinterpret_cast<double*>(base + L.A);
+                double* P_B = reinterpret_cast<double*>(base + L.B);
+                double* P_D = reinterpret_cast<double*>(base + L.D);
+                double* P_Ta = reinterpret_cast<double*>(base + L.Ta);
+                double* P_Tst = reinterpret_cast<double*>(P_tst);
+                // face fluxes (src/eikonal_solver.cpp:404-441)
+                for (size_t k = lane; k < n; k += 32) {
+                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                    P_A[k] = (ix >= 1 && iy >= 1 && iy <= ny - 2) ? faceA(ix, iy) : 0.0;
+                    P_B[k] = (iy >= 1 && ix >= 1 && ix <= nx - 2) ? faceB(ix, iy) : 0.0;
+                    const bool interior = ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2;
+                    const double v0 = interior ? 100.0 : 0.0;   // :446-449
+                    P_Ta[k] = v0;
+                    P_Tst[k] = v0;
+                }
+                __syncwarp();
+                for (size_t k = lane; k < n; k += 32) {   // diagonal, :479-481
+                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                    double d = 0.0;
+                    if (ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2) {
+                        const double a1 = P_A[k], a2 = P_A[k + 1], b1 = P_B[k], b2 = P_B[k + nx];
+                        const double a1m = (a1 - fabs(a1)) / 2.0;
+                        const double a2p = (a2 + fabs(a2)) / 2.0;
+                        const double b1m = (b1 - fabs(b1)) / 2.0;
+                        const double b2p = (b2 + fabs(b2)) / 2.0;
+                        d = (a2p - a1m) / g.dx + (b2p - b1m) / g.dy;
+                    }
+                    P_D[k] = d;
+                }
+                __syncwarp();
+                AdjPolicyExact Q;
+                Q.nx = nx;
+                Q.ny = ny;
+                Q.dx = g.dx;
+                Q.dy = g.dy;
+                Q.A = P_A;
+                Q.B = P_B;
+                Q.D = P_D;
+                Q.delta = P_delta;
+                Q.Ta = P_Ta;
+                Q.Ta_start = P_Tst;
+                if (big)
+                    for (int iter = 0; iter < 1000; iter++) {
+                        double l1 = 0.0, linf = 0.0;
+                        systolic_sweep(Q, +1, +1, false, l1, linf);
+                        systolic_sweep(Q, +1, -1, false, l1, linf);
+                        systolic_sweep(Q, -1, +1, false, l1, linf);
+                        systolic_sweep(Q, -1, -1, true, l1, linf);
+                        iters = iter + 1;
+                        const double L1 = warp_sum(l1) / (double)(nx * ny);
+                        const double Linf = warp_max(linf);
+                        if (L1 < 1e-9 && Linf < 1e-9) break;
+                    }
+            } else {
+                float* P_W = reinterpret_cast<float*>(base + L.W);
+                float* P_Ta = reinterpret_cast<float*>(base + L.Ta);
+                // weights of the rewritten update, computed in FP64 from FP64 T
+                for (size_t k = lane; k < n; k += 32) {
+                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                    const bool interior = ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2;
+                    float c0 = 0.f, wxm = 0.f, wxp = 0.f, wym = 0.f, wyp = 0.f;
+                    if (interior) {
+                        const double a1 = faceA(ix, iy), a2 = faceA(ix + 1, iy);
+                        const double b1 = faceB(ix, iy), b2 = faceB(ix, iy + 1);
+                        const double a1m = (a1 - fabs(a1)) / 2.0, a1p = (a1 + fabs(a1)) / 2.0;
+                        const double a2m = (a2 - fabs(a2)) / 2.0, a2p = (a2 + fabs(a2)) / 2.0;
+                        const double b1m = (b1 - fabs(b1)) / 2.0, b1p = (b1 + fabs(b1)) / 2.0;
+                        const double b2m = (b2 - fabs(b2)) / 2.0, b2p = (b2 + fabs(b2)) / 2.0;
+                        const double d = (a2p - a1m) / g.dx + (b2p - b1m) / g.dy;
+                        if (!(fabs(d) < 1e-14)) {
+                            c0 = (float)(P_delta[k] / d);
+                            wxm = (float)(a1p / g.dx / d);
+                            wxp = (float)(-a2m / g.dx / d);
+                            wym = (float)(b1p / g.dy / d);
+                            wyp = (float)(-b2m / g.dy / d);
+                        }
+                    }
+                    P_W[k] = c0;
+                    P_W[n + k] = wxm;
+                    P_W[2 * n + k] = wxp;
+                    P_W[3 * n + k] = wym;
+                    P_W[4 * n + k] = wyp;
+                    const float v0 = interior ? 100.f : 0.f;
+                    P_Ta[k] = v0;
+                    P_tst[k] = v0;
+                }
+                __syncwarp();
+                AdjPolicyW32 Q;
+                Q.nx = nx;
+                Q.ny = ny;
+                Q.W = P_W;
+                Q.Ta = P_Ta;
+                Q.Ta_start = P_tst;
+                if (big)
+                    for (int iter = 0; iter < 1000; iter++) {
+                        double l1 = 0.0, linf = 0.0;
+                        systolic_sweep(Q, +1, +1, false, l1, linf);
+                        systolic_sweep(Q, +1, -1, false, l1, linf);
+                        systolic_sweep(Q, -1, +1, false, l1, linf);
+                        systolic_sweep(Q, -1, -1, true, l1, linf);
+                        iters = iter + 1;
+                        const double L1 = warp_sum(l1) / (double)(nx * ny);
+                        const double Linf = warp_max(linf);
+                        if (L1 < 1e-9 && Linf < 1e-9) break;
+                        // FP32 fixed point: no cell changed by more than a few ulps
+                        double vmax = 0.0;
+                        for (size_t k = lane; k < n; k += 32) vmax = fmax(vmax, fabs((double)P_Ta[k]));
+                        vmax = warp_max(vmax);
+                        if (Linf <= 4.0 * 5.960464477539063e-08 * vmax) break;
+                    }
+            }
+            if (lane == 0 && B.out.adj_iters) B.out.adj_iters[e] = iters;
+            if (lane == 0) spread_delta(g, B.ev, r0, nr, P_sadj, P_delta, true);
+            bool finite = true;
+            const S* TaS = reinterpret_cast<const S*>(base + L.Ta);
+            if (B.mode == MODE_ADJ_ONLY) {
+                for (size_t k = lane; k < n; k += 32) {
+                    const double v = (double)TaS[k];
+                    if (!isfinite(v)) finite = false;
+                    if (B.out.Ta_out) B.out.Ta_out[(size_t)e * n + k] = v;
+                }
+            } else {
+                // mask (src/eikonal_solver.cpp:514-536) + accumulate (src/preproc.cpp:28-31)
+                const MaskBox mb = mask_box(g, B.ev.evlo[e], B.ev.evla[e]);
+                const double* inv3 = B.inv3 + (size_t)ip * n;
+                double* acc = B.out.adj_s ? B.out.adj_s + (size_t)ip * n : nullptr;
+                for (size_t k = lane; k < n; k += 32) {
+                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                    double v = (double)TaS[k];
+                    if (ix >= mb.ix_lo && ix <= mb.ix_hi && iy >= mb.iy_lo && iy <= mb.iy_hi) v = 0.0;
+                    if (!isfinite(v)) finite = false;
+                    if (B.out.Ta_out) B.out.Ta_out[(size_t)e * n + k] = v;
+                    const double c = v * inv3[k];
+                    if (acc && c != 0.0) atomicAdd(acc + k, c);
+                }
+            }
+            if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;
+        }
+        if (lane == 0 && B.out.status) B.out.status[e] = status;
+        __syncwarp();
+    }
+}
+
+template <class S>
+inline BatchArgs<S> make_batch_args(const BatchDesc& d);
+
+template <>
+inline BatchArgs<double> make_batch_args<double>(const BatchDesc& d) {
+    BatchArgs<double> B{};
+    B.g = d.g;
+    B.iso = d.iso;
+    B.fun = d.fun64;
+    B.fun64 = d.fun64;
+    B.inv3 = d.inv3;
+    B.a_f_row = d.a_f_row64;
+    B.a_a_row64 = d.a_a_row64;
+    B.b_iso = d.b_iso;
+    B.b_iso64 = d.b_iso;
+    B.a_f = d.a_f64;
+    B.b_p = d.b_p64;
+    B.c_f = d.c_f64;
+    B.b_p64 = d.b_p64;
+    B.a_a64 = d.a_a64;
+    B.c_a64 = d.c_a64;
+    B.G = d.G64;
+    B.Gx = d.Gx64;
+    B.Gy = d.Gy64;
+    B.G64 = d.G64;
+    B.ev = d.ev;
+    B.out = d.out;
+    B.sc = d.sc;
+    B.mode = d.mode;
+    return B;
+}
+
+template <>
+inline BatchArgs<float> make_batch_args<float>(const BatchDesc& d) {
+    BatchArgs<float> B{};
+    B.g = d.g;
+    B.iso = d.iso;
+    B.fun = d.fun32;
+    B.fun64 = d.fun64;
+    B.inv3 = d.inv3;
+    B.a_f_row = d.a_f_row32;
+    B.a_a_row64 = d.a_a_row64;
+    B.b_iso = d.b_iso32;
+    B.b_iso64 = d.b_iso;
+    B.a_f = d.a_f32;
+    B.b_p = d.b_p32;
+    B.c_f = d.c_f32;
+    B.b_p64 = d.b_p64;
+    B.a_a64 = d.a_a64;
+    B.c_a64 = d.c_a64;
+    B.G = d.G32;
+    B.Gx = d.Gx32;
+    B.Gy = d.Gy32;
+    B.G64 = d.G64;
+    B.ev = d.ev;
+    B.out = d.out;
+    B.sc = d.sc;
+    B.mode = d.mode;
+    return B;
+}
+
+}  // namespace sa

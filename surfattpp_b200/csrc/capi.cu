@@ -1,0 +1,682 @@
+// C ABI of libsurfatt_gpu.so (declared in include/surfatt_gpu.h).
+//
+// Host-side work here is bookkeeping only: argument checks, unique-source
+// grouping of the event list, C-library trigonometric row/column tables (so
+// the device geometry matches a CPU evaluation bit for bit), uploads, and
+// launching / graph-replaying the device pipeline.  No numerical path of the
+// engine runs on the host.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "launch.h"
+#include "surfatt_gpu.h"
+
+using namespace sa;
+
+struct sa_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int fail(sa_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+#define SA_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? SA_ERR_NOMEM : SA_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+template <class T>
+struct DArr {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DArr() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+    cudaError_t upload(const T* h, size_t count, cudaStream_t st) {
+        cudaError_t e = alloc(count);
+        if (e != cudaSuccess) return e;
+        if (count) e = cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st);
+        return e;
+    }
+};
+
+struct GraphKey {
+    const void* ptr[17];
+    int calc_adj;
+    bool operator==(const GraphKey& o) const {
+        return calc_adj == o.calc_adj && std::memcmp(ptr, o.ptr, sizeof(ptr)) == 0;
+    }
+};
+
+}  // namespace
+
+struct sa_plan {
+    sa_ctx* ctx = nullptr;
+    int prec = SA_FP64;
+    int nx = 0, ny = 0, nper = 0, ne = 0, nsta = 0, nsrc = 0, npair = 0;
+    double dx = 0, dy = 0;
+    DArr<double> xx_deg, yy_deg, xx, yy, cosy, siny, a_f_row64, a_a_row64;
+    DArr<float> a_f_row32;
+    DArr<double> evlo, evla, stlo, stla, cos_stla;
+    DArr<int> iper, src, rec_ptr, rec_idx;
+    DArr<double> G64, Gx64, Gy64;
+    DArr<float> G32, Gx32, Gy32;
+    DArr<double> fun64, inv3, a_f64, b_p64, c_f64, a_a64, c_a64;
+    DArr<float> fun32, a_f32, b_p32, c_f32;
+    DArr<double> chi_ev;
+    DArr<int> status_tmp, worst;
+    DArr<unsigned char> scratch;
+    DArr<unsigned int> queue;
+    int nslots = 0;
+    size_t slot_bytes = 0;
+    double* dbg_T = nullptr;
+    double* dbg_Ta = nullptr;
+    bool use_graph = true;
+    bool have_graph = false;
+    GraphKey key{};
+    cudaGraphExec_t gexec = nullptr;
+    ~sa_plan() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+    }
+};
+
+extern "C" int sa_version(void) { return 100; }
+
+extern "C" int sa_ctx_create(int device, sa_ctx** out) {
+    if (!out) return SA_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return SA_ERR_CUDA;
+    if (device < 0 || device >= ndev) return SA_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return SA_ERR_CUDA;
+    sa_ctx* c = new sa_ctx();
+    c->device = device;
+    if (cudaStreamCreate(&c->stream) != cudaSuccess) {   // blocking: orders with the legacy stream
+        delete c;
+        return SA_ERR_CUDA;
+    }
+    *out = c;
+    return SA_OK;
+}
+
+extern "C" void sa_ctx_destroy(sa_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char* sa_ctx_error(const sa_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+// src/eikonal_solver.cpp:514-536
+extern "C" int sa_mask_uniform_grid(int nx, int ny, const double* xx, const double* yy,
+                                    double* table, double x0, double y0) {
+    if (nx < 2 || ny < 2) return SA_OK;
+    if (!xx || !yy || !table) return SA_ERR_ARG;
+    const double dx = xx[1] - xx[0];
+    const double dy = yy[1] - yy[0];
+    const int ix_lo = std::max(0, static_cast<int>(std::floor((x0 - 1.5 * dx - xx[0]) / dx)) + 1);
+    const int ix_hi = std::min(nx - 1, static_cast<int>(std::ceil((x0 + 1.5 * dx - xx[0]) / dx)) - 1);
+    const int iy_lo = std::max(0, static_cast<int>(std::floor((y0 - 1.5 * dy - yy[0]) / dy)) + 1);
+    const int iy_hi = std::min(ny - 1, static_cast<int>(std::ceil((y0 + 1.5 * dy - yy[0]) / dy)) - 1);
+    if (ix_lo <= ix_hi && iy_lo <= iy_hi)
+        for (int iy = iy_lo; iy <= iy_hi; iy++)
+            for (int ix = ix_lo; ix <= ix_hi; ix++) table[ix + (size_t)nx * iy] = 0.0;
+    return SA_OK;
+}
+
+namespace {
+
+// Grid tables and (optionally) events/geometry of a plan.
+int plan_grid(sa_plan* P, const double* xx_deg, const double* yy_deg) {
+    sa_ctx* ctx = P->ctx;
+    const int nx = P->nx, ny = P->ny;
+    cudaStream_t st = ctx->stream;
+    std::vector<double> xr(nx), yr(ny), cy(ny), sy(ny), af(ny), aa(ny);
+    std::vector<float> af32(ny);
+    const double R2 = R_EARTH * R_EARTH;
+    for (int i = 0; i < nx; i++) xr[i] = xx_deg[i] * DEG2RAD;
+    for (int i = 0; i < ny; i++) {
+        yr[i] = yy_deg[i] * DEG2RAD;
+        cy[i] = std::cos(yr[i]);
+        sy[i] = std::sin(yr[i]);
+        const double cos2_y = cy[i] * cy[i];
+        af[i] = 1.0 / (R2 * cos2_y);            // src/eikonal_solver.cpp:61, spha = 1
+        aa[i] = 1.0 / (R2 * cy[i] * cy[i]);     // src/eikonal_solver.cpp:385
+        af32[i] = (float)af[i];
+    }
+    P->dx = xr[1] - xr[0];
+    P->dy = yr[1] - yr[0];
+    SA_CUDA(P->xx_deg.upload(xx_deg, nx, st));
+    SA_CUDA(P->yy_deg.upload(yy_deg, ny, st));
+    SA_CUDA(P->xx.upload(xr.data(), nx, st));
+    SA_CUDA(P->yy.upload(yr.data(), ny, st));
+    SA_CUDA(P->cosy.upload(cy.data(), ny, st));
+    SA_CUDA(P->siny.upload(sy.data(), ny, st));
+    SA_CUDA(P->a_f_row64.upload(af.data(), ny, st));
+    SA_CUDA(P->a_a_row64.upload(aa.data(), ny, st));
+    SA_CUDA(P->a_f_row32.upload(af32.data(), ny, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+
+int plan_events(sa_plan* P, int ne, const double* evlo, const double* evla, const int* iper,
+                const int* rec_ptr, const int* rec_idx, int nsta, const double* stlo,
+                const double* stla) {
+    sa_ctx* ctx = P->ctx;
+    cudaStream_t st = ctx->stream;
+    const int nx = P->nx, ny = P->ny;
+    const size_t n = (size_t)nx * ny;
+    P->ne = ne;
+    P->nsta = nsta;
+    P->npair = ne > 0 ? rec_ptr[ne] : 0;
+    if (ne > 0 && rec_ptr[0] != 0) return fail(ctx, SA_ERR_ARG, "rec_ptr[0] must be 0");
+    for (int e = 0; e < ne; e++) {
+        if (iper[e] < 0 || iper[e] >= P->nper) return fail(ctx, SA_ERR_ARG, "iper out of range");
+        const int nr = rec_ptr[e + 1] - rec_ptr[e];
+        if (nr < 0) return fail(ctx, SA_ERR_ARG, "rec_ptr must be non-decreasing");
+        if ((size_t)nr > n) return fail(ctx, SA_ERR_ARG, "more receivers than grid cells");
+    }
+    for (int i = 0; i < P->npair; i++)
+        if (rec_idx[i] < 0 || rec_idx[i] >= nsta)
+            return fail(ctx, SA_ERR_ARG, "rec_idx out of range");
+    // unique sources (SrcRec groups events by source name; here by position)
+    std::unordered_map<uint64_t, std::vector<int>> buckets;
+    std::vector<int> src(ne);
+    std::vector<double> ux, uy;
+    for (int e = 0; e < ne; e++) {
+        uint64_t a, b;
+        std::memcpy(&a, &evlo[e], 8);
+        std::memcpy(&b, &evla[e], 8);
+        const uint64_t h = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull);
+        int found = -1;
+        for (int s : buckets[h])
+            if (ux[s] == evlo[e] && uy[s] == evla[e]) found = s;
+        if (found < 0) {
+            found = (int)ux.size();
+            ux.push_back(evlo[e]);
+            uy.push_back(evla[e]);
+            buckets[h].push_back(found);
+        }
+        src[e] = found;
+    }
+    const int nsrc = (int)ux.size();
+    P->nsrc = nsrc;
+    std::vector<double> hxx(nx);
+    SA_CUDA(cudaMemcpy(hxx.data(), P->xx.p, nx * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<double> sy0(std::max(nsrc, 1)), cy0(std::max(nsrc, 1));
+    std::vector<double> cdl((size_t)std::max(nsrc, 1) * nx), sdl((size_t)std::max(nsrc, 1) * nx);
+    for (int s = 0; s < nsrc; s++) {
+        const double x0 = ux[s] * DEG2RAD, y0 = uy[s] * DEG2RAD;
+        sy0[s] = std::sin(y0);
+        cy0[s] = std::cos(y0);
+        for (int ix = 0; ix < nx; ix++) {
+            const double dlon = hxx[ix] - x0;
+            cdl[(size_t)s * nx + ix] = std::cos(dlon);
+            sdl[(size_t)s * nx + ix] = std::sin(dlon);
+        }
+    }
+    std::vector<double> cst(std::max(nsta, 1));
+    for (int i = 0; i < nsta; i++) cst[i] = std::cos(stla[i] * DEG2RAD);
+    SA_CUDA(P->evlo.upload(evlo, ne, st));
+    SA_CUDA(P->evla.upload(evla, ne, st));
+    SA_CUDA(P->iper.upload(iper, ne, st));
+    SA_CUDA(P->src.upload(src.data(), ne, st));
+    SA_CUDA(P->rec_ptr.upload(rec_ptr, ne + 1, st));
+    SA_CUDA(P->rec_idx.upload(rec_idx, P->npair, st));
+    SA_CUDA(P->stlo.upload(stlo, nsta, st));
+    SA_CUDA(P->stla.upload(stla, nsta, st));
+    SA_CUDA(P->cos_stla.upload(cst.data(), nsta, st));
+    DArr<double> d_sy0, d_cy0, d_cdl, d_sdl;
+    SA_CUDA(d_sy0.upload(sy0.data(), nsrc, st));
+    SA_CUDA(d_cy0.upload(cy0.data(), nsrc, st));
+    SA_CUDA(d_cdl.upload(cdl.data(), (size_t)nsrc * nx, st));
+    SA_CUDA(d_sdl.upload(sdl.data(), (size_t)nsrc * nx, st));
+    const size_t ng = (size_t)std::max(nsrc, 1) * n;
+    SA_CUDA(P->G64.alloc(ng));
+    if (P->prec == SA_FP64) {
+        SA_CUDA(P->Gx64.alloc(ng));
+        SA_CUDA(P->Gy64.alloc(ng));
+        if (nsrc)
+            SA_CUDA(launch_geometry<double>(nx, ny, nsrc, P->siny.p, P->cosy.p, d_sy0.p, d_cy0.p,
+                                            d_cdl.p, d_sdl.p, P->G64.p, P->Gx64.p, P->Gy64.p,
+                                            nullptr, st));
+    } else {
+        SA_CUDA(P->G32.alloc(ng));
+        SA_CUDA(P->Gx32.alloc(ng));
+        SA_CUDA(P->Gy32.alloc(ng));
+        if (nsrc)
+            SA_CUDA(launch_geometry<float>(nx, ny, nsrc, P->siny.p, P->cosy.p, d_sy0.p, d_cy0.p,
+                                           d_cdl.p, d_sdl.p, P->G32.p, P->Gx32.p, P->Gy32.p,
+                                           P->G64.p, st));
+    }
+    SA_CUDA(P->chi_ev.alloc(std::max(ne, 1)));
+    SA_CUDA(P->status_tmp.alloc(std::max(ne, 1)));
+    SA_CUDA(P->worst.alloc(1));
+    SA_CUDA(P->queue.alloc(1));
+    // scratch slots: one per resident warp, bounded by events and free memory
+    const int maxs = P->prec == SA_FP64 ? batch64_max_slots(ctx->device) : batch32_max_slots(ctx->device);
+    P->slot_bytes = P->prec == SA_FP64 ? batch64_slot_bytes(nx, ny) : batch32_slot_bytes(nx, ny);
+    size_t fr = 0, tot = 0;
+    SA_CUDA(cudaMemGetInfo(&fr, &tot));
+    const size_t budget = fr / 10 * 7;
+    int ns = std::min(maxs, std::max(ne, 1));
+    while (ns > 1 && (size_t)ns * P->slot_bytes > budget) ns--;
+    P->nslots = ns;
+    SA_CUDA(P->scratch.alloc((size_t)ns * P->slot_bytes));
+    // the adjoint-source plane of every slot must start at zero
+    SA_CUDA(cudaMemsetAsync(P->scratch.p, 0, (size_t)ns * P->slot_bytes, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+
+int plan_media(sa_plan* P, const double* svel, const double* m11, const double* m12,
+               const double* m22, bool general, cudaStream_t st) {
+    sa_ctx* ctx = P->ctx;
+    const size_t np = (size_t)P->nx * P->ny * P->nper;
+    SA_CUDA(P->fun64.alloc(np));
+    SA_CUDA(P->inv3.alloc(np));
+    if (general) {
+        SA_CUDA(P->a_f64.alloc(np));
+        SA_CUDA(P->b_p64.alloc(np));
+        SA_CUDA(P->c_f64.alloc(np));
+        SA_CUDA(P->a_a64.alloc(np));
+        SA_CUDA(P->c_a64.alloc(np));
+    }
+    SA_CUDA(launch_media64(P->nx, P->ny, P->nper, svel, general ? m11 : nullptr, m12, m22,
+                           P->cosy.p, P->fun64.p, P->inv3.p, P->a_f64.p, P->b_p64.p, P->c_f64.p,
+                           P->a_a64.p, P->c_a64.p, st));
+    if (P->prec == SA_FP32) {
+        SA_CUDA(P->fun32.alloc(np));
+        if (general) {
+            SA_CUDA(P->a_f32.alloc(np));
+            SA_CUDA(P->b_p32.alloc(np));
+            SA_CUDA(P->c_f32.alloc(np));
+        }
+        SA_CUDA(launch_media32(P->nx, P->ny, P->nper, P->fun64.p, general ? P->a_f64.p : nullptr,
+                               P->b_p64.p, P->c_f64.p, P->fun32.p, P->a_f32.p, P->b_p32.p,
+                               P->c_f32.p, st));
+    }
+    return SA_OK;
+}
+
+BatchDesc plan_desc(sa_plan* P, bool general) {
+    BatchDesc d{};
+    d.g.nx = P->nx;
+    d.g.ny = P->ny;
+    d.g.xx_deg = P->xx_deg.p;
+    d.g.yy_deg = P->yy_deg.p;
+    d.g.xx = P->xx.p;
+    d.g.yy = P->yy.p;
+    d.g.cosy = P->cosy.p;
+    d.g.siny = P->siny.p;
+    d.g.dx = P->dx;
+    d.g.dy = P->dy;
+    d.nper = P->nper;
+    d.iso = general ? 0 : 1;
+    d.fun64 = P->fun64.p;
+    d.inv3 = P->inv3.p;
+    d.a_f_row64 = P->a_f_row64.p;
+    d.a_a_row64 = P->a_a_row64.p;
+    d.b_iso = 1.0 / (R_EARTH * R_EARTH);
+    d.a_f64 = P->a_f64.p;
+    d.b_p64 = P->b_p64.p;
+    d.c_f64 = P->c_f64.p;
+    d.a_a64 = P->a_a64.p;
+    d.c_a64 = P->c_a64.p;
+    d.G64 = P->G64.p;
+    d.Gx64 = P->Gx64.p;
+    d.Gy64 = P->Gy64.p;
+    d.fun32 = P->fun32.p;
+    d.a_f_row32 = P->a_f_row32.p;
+    d.b_iso32 = (float)d.b_iso;
+    d.a_f32 = P->a_f32.p;
+    d.b_p32 = P->b_p32.p;
+    d.c_f32 = P->c_f32.p;
+    d.G32 = P->G32.p;
+    d.Gx32 = P->Gx32.p;
+    d.Gy32 = P->Gy32.p;
+    d.ev.ne = P->ne;
+    d.ev.src = P->src.p;
+    d.ev.iper = P->iper.p;
+    d.ev.evlo = P->evlo.p;
+    d.ev.evla = P->evla.p;
+    d.ev.rec_ptr = P->rec_ptr.p;
+    d.ev.rec_idx = P->rec_idx.p;
+    d.ev.stlo = P->stlo.p;
+    d.ev.stla = P->stla.p;
+    d.ev.cos_stla = P->cos_stla.p;
+    d.sc.nslots = P->nslots;
+    d.sc.slot_bytes = P->slot_bytes;
+    d.sc.base = P->scratch.p;
+    d.sc.queue = P->queue.p;
+    return d;
+}
+
+// Enqueue one evaluation (no synchronisation).
+int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double* m12,
+                 const double* m22, const double* tt_obs, const double* weight, int calc_adj,
+                 double* syn, double* adj_s, double* chi, int* fwd_iters, int* adj_iters,
+                 int* status, cudaStream_t st) {
+    sa_ctx* ctx = P->ctx;
+    const bool general = m11 != nullptr;
+    int rc = plan_media(P, svel, m11, m12, m22, general, st);
+    if (rc) return rc;
+    BatchDesc d = plan_desc(P, general);
+    d.ev.tt_obs = tt_obs;
+    d.ev.weight = weight;
+    d.out.syn = syn;
+    d.out.chi_ev = (calc_adj && chi) ? P->chi_ev.p : nullptr;
+    d.out.adj_s = calc_adj ? adj_s : nullptr;
+    d.out.fwd_iters = fwd_iters;
+    d.out.adj_iters = adj_iters;
+    d.out.status = status ? status : P->status_tmp.p;
+    d.out.T_out = P->dbg_T;
+    d.out.Ta_out = P->dbg_Ta;
+    d.mode = calc_adj ? MODE_FWD_ADJ : MODE_FWD;
+    SA_CUDA(cudaMemsetAsync(P->queue.p, 0, sizeof(unsigned int), st));
+    if (calc_adj && adj_s)
+        SA_CUDA(cudaMemsetAsync(adj_s, 0, (size_t)P->nx * P->ny * P->nper * sizeof(double), st));
+    if (P->ne > 0) {
+        SA_CUDA(P->prec == SA_FP64 ? launch_batch64(d, st) : launch_batch32(d, st));
+        if (calc_adj && chi) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi, st));
+        SA_CUDA(launch_fold_status(P->ne, d.out.status, P->worst.p, st));
+    } else {
+        if (calc_adj && chi) SA_CUDA(cudaMemsetAsync(chi, 0, sizeof(double), st));
+        SA_CUDA(cudaMemsetAsync(P->worst.p, 0, sizeof(int), st));
+    }
+    return SA_OK;
+}
+
+}  // namespace
+
+extern "C" int sa_plan_create(sa_ctx* ctx, int precision, int nx, int ny, int nper,
+                              const double* xx_deg, const double* yy_deg, int ne,
+                              const double* evlo, const double* evla, const int* iper,
+                              const int* rec_ptr, const int* rec_idx, int nsta,
+                              const double* stlo, const double* stla, sa_plan** out) {
+    if (!ctx || !out) return SA_ERR_ARG;
+    *out = nullptr;
+    if (precision != SA_FP64 && precision != SA_FP32) return fail(ctx, SA_ERR_ARG, "precision");
+    if (nx < 3 || ny < 3) return fail(ctx, SA_ERR_ARG, "Grid must be at least 3x3");
+    if (nper < 1 || ne < 0 || nsta < 0) return fail(ctx, SA_ERR_ARG, "nper/ne/nsta");
+    if (!xx_deg || !yy_deg || (ne > 0 && (!evlo || !evla || !iper || !rec_ptr)))
+        return fail(ctx, SA_ERR_ARG, "null input");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    sa_plan* P = new sa_plan();
+    P->ctx = ctx;
+    P->prec = precision;
+    P->nx = nx;
+    P->ny = ny;
+    P->nper = nper;
+    int rc = plan_grid(P, xx_deg, yy_deg);
+    if (!rc) rc = plan_events(P, ne, evlo, evla, iper, rec_ptr, rec_idx, nsta, stlo, stla);
+    if (rc) {
+        delete P;
+        return rc;
+    }
+    *out = P;
+    return SA_OK;
+}
+
+extern "C" void sa_plan_destroy(sa_plan* plan) { delete plan; }
+
+extern "C" int sa_plan_set_graph(sa_plan* plan, int enable) {
+    if (!plan) return SA_ERR_ARG;
+    plan->use_graph = enable != 0;
+    return SA_OK;
+}
+
+extern "C" int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out) {
+    if (!plan) return SA_ERR_ARG;
+    plan->dbg_T = T_out;
+    plan->dbg_Ta = Ta_out;
+    plan->have_graph = false;
+    return SA_OK;
+}
+
+extern "C" int sa_plan_forward_adjoint(sa_plan* P, const double* svel, const double* m11,
+                                       const double* m12, const double* m22,
+                                       const double* tt_obs, const double* weight, int calc_adj,
+                                       double* syn, double* adj_s, double* chi, int* fwd_iters,
+                                       int* adj_iters, int* status, void* stream) {
+    if (!P) return SA_ERR_ARG;
+    sa_ctx* ctx = P->ctx;
+    if (!svel) return fail(ctx, SA_ERR_ARG, "svel is required");
+    if ((m11 == nullptr) != (m22 == nullptr) || (m11 == nullptr) != (m12 == nullptr))
+        return fail(ctx, SA_ERR_ARG, "m11, m12, m22 must be all set or all NULL");
+    if (P->npair > 0 && (!tt_obs || !weight)) return fail(ctx, SA_ERR_ARG, "tt_obs/weight");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    if (!P->use_graph)
+        return plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj, syn, adj_s, chi,
+                            fwd_iters, adj_iters, status, st);
+    GraphKey k{};
+    const void* ptrs[17] = {svel, m11, m12, m22, tt_obs, weight, syn, adj_s, chi, fwd_iters,
+                            adj_iters, status, P->dbg_T, P->dbg_Ta, nullptr, nullptr, nullptr};
+    std::memcpy(k.ptr, ptrs, sizeof(ptrs));
+    k.calc_adj = calc_adj;
+    if (!(P->have_graph && P->key == k)) {
+        if (P->gexec) {
+            cudaGraphExecDestroy(P->gexec);
+            P->gexec = nullptr;
+        }
+        P->have_graph = false;
+        // allocations happen outside the capture
+        int rc = plan_media(P, svel, m11, m12, m22, m11 != nullptr, st);
+        if (rc) return rc;
+        SA_CUDA(cudaStreamSynchronize(st));
+        cudaGraph_t graph = nullptr;
+        SA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        rc = plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj, syn, adj_s, chi,
+                          fwd_iters, adj_iters, status, st);
+        cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        SA_CUDA(ce);
+        ce = cudaGraphInstantiate(&P->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        SA_CUDA(ce);
+        P->key = k;
+        P->have_graph = true;
+    }
+    SA_CUDA(cudaGraphLaunch(P->gexec, st));
+    return SA_OK;
+}
+
+namespace {
+int plan_worst_status(sa_plan* P, cudaStream_t st) {
+    sa_ctx* ctx = P->ctx;
+    int w = 0;
+    SA_CUDA(cudaMemcpyAsync(&w, P->worst.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    if (w == ST_NOCONV) return fail(ctx, SA_ERR_NOCONV, "an event reached the sweep iteration cap");
+    if (w == ST_NONFINITE) return fail(ctx, SA_ERR_NONFINITE, "non-finite travel-time or adjoint field");
+    return SA_OK;
+}
+}  // namespace
+
+extern "C" int sa_forward_for_events(sa_ctx* ctx, int precision, int nx, int ny, int nper,
+                                     const double* xx_deg, const double* yy_deg,
+                                     const double* svel, const double* m11, const double* m12,
+                                     const double* m22, int ne, const double* evlo,
+                                     const double* evla, const int* iper, const int* rec_ptr,
+                                     const int* rec_idx, int nsta, const double* stlo,
+                                     const double* stla, const double* tt_obs,
+                                     const double* weight, int calc_adj, double* syn,
+                                     double* adj_s, double* chi, int* fwd_iters,
+                                     int* adj_iters) {
+    sa_plan* P = nullptr;
+    int rc = sa_plan_create(ctx, precision, nx, ny, nper, xx_deg, yy_deg, ne, evlo, evla, iper,
+                            rec_ptr, rec_idx, nsta, stlo, stla, &P);
+    if (rc) return rc;
+    P->use_graph = false;
+    cudaStream_t st = ctx->stream;
+    const size_t np = (size_t)nx * ny * nper;
+    const int npair = P->npair;
+    const bool general = m11 != nullptr;
+    DArr<double> d_svel, d_m11, d_m12, d_m22, d_tt, d_w, d_syn, d_adj, d_chi;
+    DArr<int> d_fi, d_ai;
+    auto done = [&](int code) {
+        delete P;
+        return code;
+    };
+#define SA_CUDA_P(call)                                                                     \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return done(fail(ctx, SA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+    SA_CUDA_P(d_svel.upload(svel, np, st));
+    if (general) {
+        SA_CUDA_P(d_m11.upload(m11, np, st));
+        SA_CUDA_P(d_m12.upload(m12, np, st));
+        SA_CUDA_P(d_m22.upload(m22, np, st));
+    }
+    SA_CUDA_P(d_tt.upload(tt_obs, npair, st));
+    SA_CUDA_P(d_w.upload(weight, npair, st));
+    SA_CUDA_P(d_syn.alloc(npair));
+    SA_CUDA_P(d_adj.alloc(np));
+    SA_CUDA_P(d_chi.alloc(1));
+    SA_CUDA_P(d_fi.alloc(std::max(ne, 1)));
+    SA_CUDA_P(d_ai.alloc(std::max(ne, 1)));
+    rc = sa_plan_forward_adjoint(P, d_svel.p, general ? d_m11.p : nullptr,
+                                 general ? d_m12.p : nullptr, general ? d_m22.p : nullptr, d_tt.p,
+                                 d_w.p, calc_adj, d_syn.p, d_adj.p, d_chi.p, d_fi.p, d_ai.p,
+                                 nullptr, st);
+    if (rc) return done(rc);
+    if (syn && npair) SA_CUDA_P(cudaMemcpyAsync(syn, d_syn.p, npair * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (calc_adj && adj_s) SA_CUDA_P(cudaMemcpyAsync(adj_s, d_adj.p, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (calc_adj && chi) SA_CUDA_P(cudaMemcpyAsync(chi, d_chi.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (fwd_iters && ne) SA_CUDA_P(cudaMemcpyAsync(fwd_iters, d_fi.p, ne * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (calc_adj && adj_iters && ne) SA_CUDA_P(cudaMemcpyAsync(adj_iters, d_ai.p, ne * sizeof(int), cudaMemcpyDeviceToHost, st));
+    rc = plan_worst_status(P, st);
+    return done(rc);
+#undef SA_CUDA_P
+}
+
+// Single-solve drop-ins reuse the batch engine with one event.
+namespace {
+int single_solve(sa_ctx* ctx, int precision, int nx, int ny, const double* xx_deg,
+                 const double* yy_deg, const double* spha, const double* sphb,
+                 const double* sphc, const double* fun_or_T, double x0, double y0, int nr,
+                 const double* xrec, const double* yrec, const double* sadj, bool adjoint,
+                 double* out, int* niter) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 3 || ny < 3) return fail(ctx, SA_ERR_ARG, "Grid must be at least 3x3");
+    if (!xx_deg || !yy_deg || !spha || !sphb || !sphc || !fun_or_T || !out)
+        return fail(ctx, SA_ERR_ARG, "null input");
+    if (nr < 0 || (nr > 0 && (!xrec || !yrec || !sadj))) return fail(ctx, SA_ERR_ARG, "receivers");
+    const size_t n = (size_t)nx * ny;
+    std::vector<int> rp = {0, nr}, ri(std::max(nr, 1));
+    for (int i = 0; i < nr; i++) ri[i] = i;
+    const int iper = 0;
+    sa_plan* P = nullptr;
+    int rc = sa_plan_create(ctx, precision, nx, ny, 1, xx_deg, yy_deg, 1, &x0, &y0, &iper,
+                            rp.data(), ri.data(), nr, nr ? xrec : nullptr, nr ? yrec : nullptr, &P);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    DArr<double> m11, m12, m22, svel, fin, o, sa_, ones, tt;
+    DArr<int> it, stt;
+    std::vector<double> neg(n);
+    for (size_t k = 0; k < n; k++) neg[k] = -sphc[k];    // media uses sphc = -m12
+    auto done = [&](int code) {
+        delete P;
+        return code;
+    };
+    auto chk = [&](cudaError_t e) { return e == cudaSuccess ? 0 : fail(ctx, SA_ERR_CUDA, cudaGetErrorString(e)); };
+    if ((rc = chk(m11.upload(spha, n, st))) || (rc = chk(m12.upload(neg.data(), n, st))) ||
+        (rc = chk(m22.upload(sphb, n, st))) || (rc = chk(fin.upload(fun_or_T, n, st))) ||
+        (rc = chk(o.alloc(n))) || (rc = chk(it.alloc(1))) || (rc = chk(stt.alloc(1))) ||
+        (rc = chk(svel.alloc(n))) || (rc = chk(cudaMemsetAsync(svel.p, 0, n * sizeof(double), st))))
+        return done(rc);
+    if (nr && (rc = chk(sa_.upload(sadj, nr, st)))) return done(rc);
+    // media planes from spha/sphb/sphc; the slowness plane is set directly
+    rc = plan_media(P, svel.p, m11.p, m12.p, m22.p, true, st);
+    if (rc) return done(rc);
+    if ((rc = chk(cudaMemcpyAsync(P->fun64.p, fin.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st))))
+        return done(rc);
+    if (precision == SA_FP32 &&
+        (rc = chk(launch_media32(nx, ny, 1, P->fun64.p, P->a_f64.p, P->b_p64.p, P->c_f64.p,
+                                 P->fun32.p, P->a_f32.p, P->b_p32.p, P->c_f32.p, st))))
+        return done(rc);
+    BatchDesc d = plan_desc(P, true);
+    d.ev.sadj = sa_.p;
+    d.ev.T_in = fin.p;
+    d.out.status = stt.p;
+    if (adjoint) {
+        d.mode = MODE_ADJ_ONLY;
+        d.out.Ta_out = o.p;
+        d.out.adj_iters = it.p;
+    } else {
+        d.mode = MODE_FWD;
+        d.out.T_out = o.p;
+        d.out.fwd_iters = it.p;
+        std::vector<double> z(std::max(nr, 1), 0.0);
+        if ((rc = chk(tt.upload(z.data(), std::max(nr, 1), st))) ||
+            (rc = chk(ones.upload(z.data(), std::max(nr, 1), st))))
+            return done(rc);
+        d.ev.tt_obs = tt.p;
+        d.ev.weight = ones.p;
+    }
+    if ((rc = chk(cudaMemsetAsync(P->queue.p, 0, sizeof(unsigned int), st)))) return done(rc);
+    if ((rc = chk(precision == SA_FP64 ? launch_batch64(d, st) : launch_batch32(d, st))))
+        return done(rc);
+    int h_it = 0, h_st = 0;
+    if ((rc = chk(cudaMemcpyAsync(out, o.p, n * sizeof(double), cudaMemcpyDeviceToHost, st))) ||
+        (rc = chk(cudaMemcpyAsync(&h_it, it.p, sizeof(int), cudaMemcpyDeviceToHost, st))) ||
+        (rc = chk(cudaMemcpyAsync(&h_st, stt.p, sizeof(int), cudaMemcpyDeviceToHost, st))) ||
+        (rc = chk(cudaStreamSynchronize(st))))
+        return done(rc);
+    if (niter) *niter = h_it;
+    if (h_st == ST_NOCONV) return done(fail(ctx, SA_ERR_NOCONV, "iteration cap reached"));
+    if (h_st == ST_NONFINITE) return done(fail(ctx, SA_ERR_NONFINITE, "non-finite field"));
+    return done(SA_OK);
+}
+}  // namespace
+
+extern "C" int sa_eik_fwd_field(sa_ctx* ctx, int precision, int nx, int ny, const double* xx_deg,
+                                const double* yy_deg, const double* spha, const double* sphb,
+                                const double* sphc, const double* fun, double x0_deg,
+                                double y0_deg, double* T_out, int* niter) {
+    return single_solve(ctx, precision, nx, ny, xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg,
+                        y0_deg, 0, nullptr, nullptr, nullptr, false, T_out, niter);
+}
+
+extern "C" int sa_eik_adj_field(sa_ctx* ctx, int precision, int nx, int ny, const double* xx_deg,
+                                const double* yy_deg, const double* spha, const double* sphb,
+                                const double* sphc, const double* T, int nr,
+                                const double* xrec_deg, const double* yrec_deg,
+                                const double* source_adj, double* Ta_out, int* niter) {
+    return single_solve(ctx, precision, nx, ny, xx_deg, yy_deg, spha, sphb, sphc, T, 0.0, 0.0,
+                        nr, xrec_deg, yrec_deg, source_adj, true, Ta_out, niter);
+}

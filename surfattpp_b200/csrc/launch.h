@@ -1,0 +1,71 @@
+// Host-side launch descriptors shared by the C ABI (capi.cu) and the kernel
+// translation units (eik64.cu, eik32.cu, surfker.cu).
+#pragma once
+#include <algorithm>
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace sa {
+
+struct BatchDesc {
+    Grid g;
+    int nper;
+    int iso;
+    // FP64 media / geometry
+    const double* fun64;
+    const double* inv3;
+    const double* a_f_row64;
+    const double* a_a_row64;
+    double b_iso;
+    const double* a_f64;
+    const double* b_p64;
+    const double* c_f64;
+    const double* a_a64;
+    const double* c_a64;
+    const double* G64;
+    const double* Gx64;
+    const double* Gy64;
+    // FP32 media / geometry
+    const float* fun32;
+    const float* a_f_row32;
+    float b_iso32;
+    const float* a_f32;
+    const float* b_p32;
+    const float* c_f32;
+    const float* G32;
+    const float* Gx32;
+    const float* Gy32;
+    Events ev;
+    Outputs out;
+    Scratch sc;
+    int mode;
+};
+
+size_t batch64_slot_bytes(int nx, int ny);
+int batch64_max_slots(int device);
+size_t batch32_slot_bytes(int nx, int ny);
+int batch32_max_slots(int device);
+
+cudaError_t launch_media64(int nx, int ny, int nper, const double* svel, const double* m11,
+                           const double* m12, const double* m22, const double* cosy,
+                           double* fun, double* inv3, double* a_f, double* b_p, double* c_f,
+                           double* a_a, double* c_a, cudaStream_t st);
+cudaError_t launch_media32(int nx, int ny, int nper, const double* fun64, const double* a_f64,
+                           const double* b_p64, const double* c_f64, float* fun32, float* a_f32,
+                           float* b_p32, float* c_f32, cudaStream_t st);
+template <class T>
+cudaError_t launch_geometry(int nx, int ny, int nsrc, const double* siny, const double* cosy,
+                            const double* sy0, const double* cy0, const double* cdl,
+                            const double* sdl, T* G, T* Gx, T* Gy, double* G64,
+                            cudaStream_t st);
+cudaError_t launch_batch64(const BatchDesc& d, cudaStream_t st);
+cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st);
+
+}  // namespace sa
+
+namespace sa {
+cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStream_t st);
+cudaError_t launch_fold_status(int ne, const int* status, int* worst, cudaStream_t st);
+}  // namespace sa

@@ -1,0 +1,45 @@
+// Small device utilities: deterministic event-sum of the misfit and status
+// folding.
+#include "launch.h"
+
+namespace sa {
+
+// chi = sum over events of chi_ev (fixed-order tree: deterministic run to run).
+__global__ void sum_events_kernel(int ne, const double* __restrict__ chi_ev, double* chi) {
+    __shared__ double part[1024];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) s += chi_ev[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *chi = part[0];
+}
+
+// worst = max status over events (0 = all ok).
+__global__ void fold_status_kernel(int ne, const int* __restrict__ st, int* worst) {
+    __shared__ int part[1024];
+    int s = 0;
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) s = max(s, st[i]);
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] = max(part[threadIdx.x], part[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *worst = part[0];
+}
+
+cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStream_t st) {
+    sum_events_kernel<<<1, 1024, 0, st>>>(ne, chi_ev, chi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_status(int ne, const int* status, int* worst, cudaStream_t st) {
+    fold_status_kernel<<<1, 1024, 0, st>>>(ne, status, worst);
+    return cudaGetLastError();
+}
+
+}  // namespace sa

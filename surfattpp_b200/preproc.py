@@ -1,0 +1,121 @@
+"""preproc:: call surface (reference include/preproc.h) on the GPU.
+
+``forward_for_event`` is the drop-in for preproc::forward_for_event
+(src/preproc.cpp:71-148): every (source, period) event runs forward, receiver
+interpolation, residuals, adjoint, source mask and accumulation into adj_s.
+``ForwardAdjointPlan`` keeps the event set, per-source geometry and scratch
+resident on the device across misfit evaluations (one plan per inversion).
+Device memory is held in torch tensors (allocation only; all arithmetic runs
+in libsurfatt_gpu.so).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import SA_FP32, SA_FP64, default_context, ptr
+
+
+def _prec(p):
+    return {"fp64": SA_FP64, "fp32": SA_FP32, SA_FP64: SA_FP64, SA_FP32: SA_FP32}[p]
+
+
+def _c(a, dt=np.float64):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class ForwardAdjointPlan:
+    """sa_plan: grid + event set fixed; call ``run`` once per misfit evaluation."""
+
+    def __init__(self, xx_deg, yy_deg, nper, evlo, evla, iper, rec_ptr, rec_idx, stlo, stla,
+                 precision="fp64", ctx=None, graph=True):
+        self.ctx = ctx or default_context()
+        self.precision = _prec(precision)
+        self._keep = [_c(xx_deg), _c(yy_deg), _c(evlo), _c(evla), _c(iper, np.int32),
+                      _c(rec_ptr, np.int32), _c(rec_idx, np.int32), _c(stlo), _c(stla)]
+        xx, yy, elo, ela, ip, rp, ri, slo, sla = self._keep
+        self.nx, self.ny, self.nper = xx.size, yy.size, int(nper)
+        self.ne, self.nsta = elo.size, slo.size
+        self.npair = int(rp[-1]) if rp.size else 0
+        h = C.c_void_p()
+        addr = (lambda a: a.ctypes.data if a.size else None)
+        rc = _capi.lib().sa_plan_create(self.ctx.h, self.precision, self.nx, self.ny, self.nper,
+                                        xx, yy, self.ne, addr(elo), addr(ela), addr(ip), addr(rp),
+                                        addr(ri), self.nsta, addr(slo), addr(sla), C.byref(h))
+        _capi.check(self.ctx.h, rc)
+        self.h = h
+        _capi.lib().sa_plan_set_graph(self.h, int(bool(graph)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().sa_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def debug_fields(self, T_out=None, Ta_out=None):
+        _capi.lib().sa_plan_debug_fields(self.h, ptr(T_out), ptr(Ta_out))
+
+    def run(self, svel, tt_obs, weight, calc_adj=True, m11=None, m12=None, m22=None, out=None,
+            stream=None):
+        """Enqueue one evaluation on device tensors (float64, contiguous).
+
+        svel: (nper, ny, nx); tt_obs/weight: (npair,).  ``out`` is a dict of
+        preallocated device tensors (syn, adj_s, chi, fwd_iters, adj_iters,
+        status); missing ones are allocated.  Returns ``out``; synchronise the
+        stream before reading."""
+        import torch
+        dev = svel.device
+        out = {} if out is None else out
+        f64 = dict(dtype=torch.float64, device=dev)
+        i32 = dict(dtype=torch.int32, device=dev)
+        out.setdefault("syn", torch.empty(max(self.npair, 1), **f64))
+        out.setdefault("adj_s", torch.empty((self.nper, self.ny, self.nx), **f64))
+        out.setdefault("chi", torch.zeros(1, **f64))
+        out.setdefault("fwd_iters", torch.zeros(max(self.ne, 1), **i32))
+        out.setdefault("adj_iters", torch.zeros(max(self.ne, 1), **i32))
+        out.setdefault("status", torch.zeros(max(self.ne, 1), **i32))
+        rc = _capi.lib().sa_plan_forward_adjoint(
+            self.h, ptr(svel), ptr(m11), ptr(m12), ptr(m22), ptr(tt_obs), ptr(weight),
+            int(bool(calc_adj)), ptr(out["syn"]), ptr(out["adj_s"]), ptr(out["chi"]),
+            ptr(out["fwd_iters"]), ptr(out["adj_iters"]), ptr(out["status"]),
+            stream if stream is not None else None)
+        _capi.check(self.ctx.h, rc)
+        return out
+
+
+def forward_for_event(xx_deg, yy_deg, svel, events, calc_adj=True, m11=None, m12=None, m22=None,
+                      precision="fp64", ctx=None):
+    """Host-array drop-in for preproc::forward_for_event.
+
+    svel (nper, ny, nx); ``events`` holds evlo, evla, iper, rec_ptr, rec_idx,
+    stlo, stla, tt_obs, weight.  Returns dict(syn, adj_s, chi, fwd_iters,
+    adj_iters).  Raises NoConvergence if an event hit the iteration cap."""
+    ctx = ctx or default_context()
+    svel = _c(svel)
+    nper, ny, nx = svel.shape
+    ev = events
+    ne = len(ev["evlo"])
+    npair = int(ev["rec_ptr"][-1])
+    syn = np.zeros(max(npair, 1))
+    adj_s = np.zeros((nper, ny, nx))
+    chi = C.c_double(0.0)
+    fi = np.zeros(max(ne, 1), np.int32)
+    ai = np.zeros(max(ne, 1), np.int32)
+    addr = (lambda a: None if a is None else _c(a).ctypes.data)
+    keep = [_c(m) for m in (m11, m12, m22) if m is not None]
+    mp = [k.ctypes.data for k in keep] if keep else [None, None, None]
+    rc = _capi.lib().sa_forward_for_events(
+        ctx.h, _prec(precision), nx, ny, nper, _c(xx_deg), _c(yy_deg), svel, mp[0], mp[1], mp[2],
+        ne, _c(ev["evlo"]), _c(ev["evla"]), _c(ev["iper"], np.int32), _c(ev["rec_ptr"], np.int32),
+        _c(ev["rec_idx"], np.int32), len(ev["stlo"]), _c(ev["stlo"]), _c(ev["stla"]),
+        _c(ev["tt_obs"]), _c(ev["weight"]), int(bool(calc_adj)), syn, adj_s, C.byref(chi), fi, ai)
+    _capi.check(ctx.h, rc)
+    return dict(syn=syn[:npair], adj_s=adj_s, chi=chi.value, fwd_iters=fi[:ne],
+                adj_iters=ai[:ne])
