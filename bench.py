@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark: (source, period) forward + adjoint solves/s on one B200.
+
+Workload: the batched configuration -- 301x301 surface grid at 0.01 deg,
+400 stations as sources and receivers, 20 periods 2-50 s: 8000 forward +
+adjoint solves per step, FP32 sweeps with FP64 T0 / residuals / accumulation,
+one persistent launch replayed as a CUDA graph.  Inputs are seeded synthetic
+(no public dataset exists for this path).
+
+A step is one misfit evaluation of the whole event set: media preparation,
+the fused per-event forward FSM -> receivers -> residuals -> adjoint FSM ->
+mask -> FP64 kernel accumulation, and the misfit sum.  Inputs (>= 700 MB of
+per-event scratch traffic per step) are larger than L2, so no flush is needed.
+
+`value` is device-timed with CUDA events on the launching stream (max over
+ranks); `e2e` times the same step through the public plan API with pinned
+host buffers, host->device copies of the step's inputs and the device->host
+read of adj_s and the misfit inside the timed region.
+
+--impl reference times the CPU restatement of the reference (oracle/, all
+host threads) on a bounded sample of the same workload.
+Under torchrun each rank runs its own shard of (source, period) events
+(weak scaling); the only exchange is the FP64 all-reduce of adj_s and the
+misfit (the reference's MPI_Allreduce, src/preproc.cpp:146, :238).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "(src,period) fwd+adj solves/s, batched FP32 sweeps (FP64 T0/residual/accumulation)"
+UNIT = "solves/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    p.add_argument("--nsta", type=int, default=400)
+    p.add_argument("--nper", type=int, default=20)
+    p.add_argument("--n", type=int, default=301)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(a, world):
+    return {"workload": f"C3 batched fwd+adj: {a.n}x{a.n} grid at 0.01 deg, {a.nsta} stations "
+                        f"(sources and receivers), {a.nper} periods 2-50 s, "
+                        f"{a.nsta * a.nper} events per rank",
+            "grid": [a.n, a.n], "stations": a.nsta, "periods": a.nper,
+            "events_per_rank": a.nsta * a.nper, "ranks": world,
+            "l2_policy": "per-step working set > L2 (126 MB); no flush",
+            "graph": True, "precision": a.precision}
+
+
+def make_inputs(a, rank):
+    from surfattpp_b200 import workloads as W
+    w = W.config3(seed=1003 + rank, nsta=a.nsta, nper=a.nper, n=a.n)
+    X, Y = np.meshgrid(w.xx_deg, w.yy_deg)
+    # smooth synthetic phase-velocity planes per period (km/s)
+    svel = np.stack([3.0 + 0.9 * k / max(a.nper - 1, 1)
+                     + 0.1 * np.sin(X * 20 + k) * np.cos(Y * 17) for k in range(a.nper)])
+    return w, svel
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, dev):
+        self.dev, self.rows, self.stop, self.t = dev, [], False, None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self.stop:
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True,
+                                         text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                time.sleep(0.2)
+        self.t = threading.Thread(target=run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop = True
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(nx, ny, fwd_iters, adj_iters, bpu_fwd, bpu_adj):
+    """Algorithmic HBM bytes of the sweeps: per cell update, each stored
+    operand read once and the field written once (forward: T0, T0x, T0y, a,
+    b, c, fun, tau + tau write; adjoint: two face fluxes, delta, Ta + Ta
+    write), times cell updates = iterations x 4 sweeps x cells."""
+    fwd = float(np.sum(fwd_iters)) * 4 * nx * ny
+    adj = float(np.sum(adj_iters)) * 4 * (nx - 2) * (ny - 2)
+    return fwd * bpu_fwd + adj * bpu_adj, fwd, adj
+
+
+def cpu_baseline(a, w, svel, nev=16):
+    """The oracle (port of the reference) on a bounded sample of events with
+    every host thread."""
+    from oracle import oracle as O
+    from surfattpp_b200 import workloads as W
+    O.build()
+    rng = np.random.default_rng(7)
+    keep = np.sort(rng.choice(w.n_events, size=min(nev, w.n_events), replace=False))
+    sub = W.subset_events(w, keep)
+    m11, m12, m22 = sub.media()
+    nth = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.forward_for_events(sub.xx_deg, sub.yy_deg, svel, m11, m12, m22, sub.events(),
+                         calc_adj=True, nthreads=nth)
+    dt = time.perf_counter() - t0
+    return {"value": keep.size / dt, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": f"{keep.size} random events of the same workload, fwd+adj, FP64, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    w, svel = make_inputs(a, 0)
+    base = cpu_baseline(a, w, svel, nev=8)
+    vals = []
+    for _ in range(max(a.warmup, 0)):
+        pass   # the CPU sample has no warm-up state
+    for _ in range(a.steps):
+        vals.append(cpu_baseline(a, w, svel, nev=8)["value"])
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 8.0 / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": workload_config(a, world),
+            "cpu_baseline": {**base, "value": v},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    import torch
+    from surfattpp_b200 import preproc
+    from surfattpp_b200._capi import Context
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    ctx = Context(local)
+    w, svel = make_inputs(a, rank)
+    ev = w.events()
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    cs = stream.cuda_stream
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision=a.precision, ctx=ctx, graph=True)
+    t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=dev)
+    sv, tt, wt = t(svel), t(ev["tt_obs"]), t(ev["weight"])
+    out = plan.run(sv, tt, wt, stream=cs)
+
+    def step():
+        plan.run(sv, tt, wt, out=out, stream=cs)
+        if dist is not None:
+            dist.all_reduce(out["adj_s"])
+            dist.all_reduce(out["chi"])
+
+    for _ in range(max(a.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    fwd_iters = out["fwd_iters"].cpu().numpy()[:w.n_events]
+    adj_iters = out["adj_iters"].cpu().numpy()[:w.n_events]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    if dist is not None:
+        m = torch.tensor([ms], device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms = float(m)
+        dist.barrier()
+    status = int(out["status"][:w.n_events].max())
+
+    # end to end through the public API: pinned host inputs in, adj_s + misfit out
+    h_sv = torch.from_numpy(svel).pin_memory()
+    h_tt = torch.from_numpy(np.ascontiguousarray(ev["tt_obs"])).pin_memory()
+    h_wt = torch.from_numpy(np.ascontiguousarray(ev["weight"])).pin_memory()
+    h_adj = torch.empty(out["adj_s"].shape, dtype=torch.float64).pin_memory()
+    h_chi = torch.empty(1, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        sv.copy_(h_sv, non_blocking=True)
+        tt.copy_(h_tt, non_blocking=True)
+        wt.copy_(h_wt, non_blocking=True)
+        step()
+        h_adj.copy_(out["adj_s"], non_blocking=True)
+        h_chi.copy_(out["chi"], non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(a.steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1) / a.steps
+    if dist is not None:
+        m = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms_e2e = float(m)
+    h2d = h_sv.numel() * 8 + h_tt.numel() * 8 + h_wt.numel() * 8
+    d2h = h_adj.numel() * 8 + 8
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        bpu_f, bpu_a = (36, 20) if a.precision == "fp32" else (72, 40)
+        algo, nf, na = algorithmic_bytes(w.nx, w.ny, fwd_iters, adj_iters, bpu_f, bpu_a)
+        achieved = algo / (ms * 1e-3) / 1e9
+        total_events = w.n_events * world
+        line = {
+            "metric": METRIC, "value": total_events / (ms * 1e-3), "unit": UNIT,
+            "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if a.precision == "fp32" else "f64",
+            "data": "synthetic (seeded GRF model, straight-ray observed times)",
+            "config": workload_config(a, world),
+            "e2e": {"value": total_events / (ms_e2e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": (5 if a.precision == "fp32" else 4) * a.steps,
+            "cell_updates_per_s": (nf + na) / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "note": "algorithmic bytes: 36 B per forward / 20 B per adjoint "
+                                 "cell update (FP32), x2 for FP64"},
+            "clocks": clk.summary(),
+            "status": status,
+        }
+        if not a.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(a, w, svel)
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

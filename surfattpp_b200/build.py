@@ -26,7 +26,7 @@ UNITS = {
     "surfker.cu": ["-fmad=false"],
     "kernels.cu": ["-fmad=false"],
     "util.cu": [],
-    "capi.cu": [],
+    "capi.cu": ["-Xcompiler", "-ffp-contract=off"],
     "noalloc.cu": [],
 }
 

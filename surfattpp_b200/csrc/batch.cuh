@@ -27,9 +27,7 @@ struct BatchArgs {
     const double* a_a_row64;
     S b_iso;
     double b_iso64;
-    const S* a_f;
-    const S* b_p;
-    const S* c_f;
+    const Q4<S>* mt;       // general metric {a, b, c, 0} per period (or null)
     const double* b_p64;
     const double* a_a64;
     const double* c_a64;
@@ -40,55 +38,59 @@ struct BatchArgs {
     Events ev;
     Outputs out;
     Scratch sc;
+    int maxr;              // largest receiver count of any event
     int mode;
 };
 
-// Scratch slot layout (bytes, every plane 256-byte aligned).
+// Scratch slot layout (bytes, every plane 256-byte aligned).  The packed
+// forward operands (PK) and the packed adjoint coefficients share one region:
+// the forward planes are dead once T is formed.
 struct SlotLayout {
-    size_t tau, tst, T, A, B, D, delta, Ta, W, sadj, syn, total;
+    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, total;
 };
 template <class S>
-__host__ __device__ inline SlotLayout slot_layout(int nx, int ny) {
+__host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     const size_t n = (size_t)nx * ny;
-    SlotLayout L;
+    const size_t r = (size_t)(maxr > 0 ? maxr : 1);
+    SlotLayout L{};
     size_t o = 0;
     auto take = [&](size_t bytes) {
-        const size_t r = o;
+        const size_t at = o;
         o += align_up(bytes, 256);
-        return r;
+        return at;
     };
     L.tau = take(n * sizeof(S));
     L.tst = take(n * sizeof(S));
     L.T = take(n * sizeof(double));
     L.delta = take(n * sizeof(double));
-    L.sadj = take(n * sizeof(double));
-    L.syn = take(n * sizeof(double));
+    L.PK = take(n * 4 * sizeof(S));
+    L.AQ = L.PK;      // FP64: {a1p, a2m, b1p, b2m} (same size as PK)
+    L.W = L.PK;       // FP32: {wxm, wxp, wym, wyp} (same size as PK)
     if (sizeof(S) == sizeof(double)) {
-        L.A = take(n * sizeof(double));
-        L.B = take(n * sizeof(double));
-        L.D = take(n * sizeof(double));
-        L.Ta = take(n * sizeof(double));
-        L.W = 0;
+        L.DD = take(n * 2 * sizeof(double));
+        L.C0 = 0;
     } else {
-        L.A = L.B = L.D = 0;
-        L.W = take(5 * n * sizeof(float));
-        L.Ta = take(n * sizeof(float));
+        L.C0 = take(n * sizeof(float));
+        L.DD = 0;
     }
+    L.Ta = take(n * sizeof(S));
+    L.sadj = take(r * sizeof(double));
+    L.syn = take(r * sizeof(double));
     L.total = o;
     return L;
 }
 
-template <class S>
+template <class S, bool ISO>
 __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo& si, int ip,
-                                            int src, S* tau, S* tst, double* T, int& iters,
-                                            int& status) {
+                                            int src, S* tau, S* tst, Q4<S>* pk, double* T,
+                                            int& iters, int& status) {
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
     const size_t n = (size_t)nx * ny;
     const int lane = threadIdx.x & 31;
     const double fun0_64 = bilinear64(B.fun64 + (size_t)ip * n, nx, si.idx0, si.idy0, si.r1, si.r2);
-    using Pol = typename std::conditional<sizeof(S) == sizeof(double), FwdPolicy<double>,
-                                          FwdPolicyDelta32>::type;
+    using Pol = typename std::conditional<sizeof(S) == sizeof(double), FwdPolicy64<ISO>,
+                                          FwdPolicyDelta32<ISO>>::type;
     Pol P;
     P.nx = nx;
     P.ny = ny;
@@ -99,16 +101,21 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
         P.idx = (float)(1.0 / g.dx);
         P.idy = (float)(1.0 / g.dy);
     }
-    P.fun0 = (S)fun0_64;
-    P.G = B.G + (size_t)src * n;
-    P.Gx = B.Gx + (size_t)src * n;
-    P.Gy = B.Gy + (size_t)src * n;
-    P.fun = B.fun + (size_t)ip * n;
+    // packed per-cell operands {T0, T0x, T0y, fun}; T0 = G*fun0 etc. exactly
+    // as src/eikonal_solver.cpp:102-115 multiplies by fun0 last
+    const S fun0 = (S)fun0_64;
+    {
+        const S* G = B.G + (size_t)src * n;
+        const S* Gx = B.Gx + (size_t)src * n;
+        const S* Gy = B.Gy + (size_t)src * n;
+        const S* fn = B.fun + (size_t)ip * n;
+        for (size_t k = lane; k < n; k += 32)
+            st4(pk + k, G[k] * fun0, Gx[k] * fun0, Gy[k] * fun0, fn[k]);
+    }
+    P.pk = pk;
+    P.mt = ISO ? nullptr : B.mt + (size_t)ip * n;
     P.a_row = B.a_f_row;
     P.b_iso = B.b_iso;
-    P.a_pl = B.iso ? nullptr : B.a_f + (size_t)ip * n;
-    P.b_pl = B.iso ? nullptr : B.b_p + (size_t)ip * n;
-    P.c_pl = B.iso ? nullptr : B.c_f + (size_t)ip * n;
     P.tau = tau;
     P.tau_start = tst;
     P.fix_x0 = si.fix_x0;
@@ -130,10 +137,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     iters = 0;
     for (int iter = 0; iter < 2000; iter++) {
         double l1 = 0.0, linf = 0.0;
-        systolic_sweep(P, +1, +1, false, l1, linf);
-        systolic_sweep(P, +1, -1, false, l1, linf);
-        systolic_sweep(P, -1, +1, false, l1, linf);
-        systolic_sweep(P, -1, -1, true, l1, linf);
+        for (int sw = 0; sw < 4; sw++) systolic_sweep(P, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
         iters = iter + 1;
         const double L1 = warp_sum(l1) / (double)(nx * ny);
         const double Linf = warp_max(linf);
@@ -155,15 +159,15 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     return fun0_64;
 }
 
-template <class S>
-__global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
+template <class S, bool ISO>
+__global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batch_kernel(BatchArgs<S> B) {
     const int lane = threadIdx.x & 31;
     const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (slot >= B.sc.nslots) return;
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
     const size_t n = (size_t)nx * ny;
-    const SlotLayout L = slot_layout<S>(nx, ny);
+    const SlotLayout L = slot_layout<S>(nx, ny, B.maxr);
     unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
     S* P_tau = reinterpret_cast<S*>(base + L.tau);
     S* P_tst = reinterpret_cast<S*>(base + L.tst);
@@ -171,6 +175,7 @@ __global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
     double* P_delta = reinterpret_cast<double*>(base + L.delta);   // zero between events
     double* P_sadj = reinterpret_cast<double*>(base + L.sadj);
     double* P_syn = reinterpret_cast<double*>(base + L.syn);
+    Q4<S>* P_pk = reinterpret_cast<Q4<S>*>(base + L.PK);
 
     for (;;) {
         const unsigned int e = warp_next_event(B.sc.queue);
@@ -184,7 +189,7 @@ __global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
 
         if (B.mode != MODE_ADJ_ONLY) {
             int iters = 0;
-            fwd_solve<S>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_T, iters, status);
+            fwd_solve<S, ISO>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_T, iters, status);
             if (lane == 0 && B.out.fwd_iters) B.out.fwd_iters[e] = iters;
             if (B.out.T_out)
                 for (size_t k = lane; k < n; k += 32) B.out.T_out[(size_t)e * n + k] = P_T[k];
@@ -216,48 +221,48 @@ __global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
             // adjoint source (src/eikonal_solver.cpp:354-375), receivers in order
             if (lane == 0) spread_delta(g, B.ev, r0, nr, P_sadj, P_delta, false);
             __syncwarp();
-            const double* a_a = B.iso ? nullptr : B.a_a64 + (size_t)ip * n;
-            const double* b_p = B.iso ? nullptr : B.b_p64 + (size_t)ip * n;
-            const double* c_a = B.iso ? nullptr : B.c_a64 + (size_t)ip * n;
+            const double* a_a = ISO ? nullptr : B.a_a64 + (size_t)ip * n;
+            const double* b_p = ISO ? nullptr : B.b_p64 + (size_t)ip * n;
+            const double* c_a = ISO ? nullptr : B.c_a64 + (size_t)ip * n;
             auto faceA = [&](int ix, int iy) -> double {
-                return B.iso ? face_a1_iso(T, B.a_a_row64[iy], nx, ix, iy, g.dx, g.dy)
-                             : face_a1(T, a_a, c_a, nx, ix, iy, g.dx, g.dy);
+                if constexpr (ISO) return face_a1_iso(T, B.a_a_row64[iy], nx, ix, iy, g.dx, g.dy);
+                else return face_a1(T, a_a, c_a, nx, ix, iy, g.dx, g.dy);
             };
             auto faceB = [&](int ix, int iy) -> double {
-                return B.iso ? face_b1_iso(T, B.b_iso64, B.b_iso64, nx, ix, iy, g.dx, g.dy)
-                             : face_b1(T, b_p, c_a, nx, ix, iy, g.dx, g.dy);
+                if constexpr (ISO) return face_b1_iso(T, B.b_iso64, B.b_iso64, nx, ix, iy, g.dx, g.dy);
+                else return face_b1(T, b_p, c_a, nx, ix, iy, g.dx, g.dy);
             };
             int iters = 0;
             const bool big = nx >= 3 && ny >= 3;
             if constexpr (sizeof(S) == sizeof(double)) {
-                double* P_A = reinterpret_cast<double*>(base + L.A);
-                double* P_B = reinterpret_cast<double*>(base + L.B);
-                double* P_D = reinterpret_cast<double*>(base + L.D);
+                Q4<double>* P_AQ = reinterpret_cast<Q4<double>*>(base + L.AQ);
+                double2* P_DD = reinterpret_cast<double2*>(base + L.DD);
                 double* P_Ta = reinterpret_cast<double*>(base + L.Ta);
                 double* P_Tst = reinterpret_cast<double*>(P_tst);
-                // face fluxes (src/eikonal_solver.cpp:404-441)
+                // face fluxes (src/eikonal_solver.cpp:404-441): a2(ix) is a1(ix+1)
+                // and b2(iy) is b1(iy+1), identical expressions in the reference
                 for (size_t k = lane; k < n; k += 32) {
                     const int iy = (int)(k / nx), ix = (int)(k % nx);
-                    P_A[k] = (ix >= 1 && iy >= 1 && iy <= ny - 2) ? faceA(ix, iy) : 0.0;
-                    P_B[k] = (iy >= 1 && ix >= 1 && ix <= nx - 2) ? faceB(ix, iy) : 0.0;
                     const bool interior = ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2;
+                    double a1p = 0, a2m = 0, b1p = 0, b2m = 0, d = 0;
+                    if (interior) {
+                        const double a1 = faceA(ix, iy), a2 = faceA(ix + 1, iy);
+                        const double b1 = faceB(ix, iy), b2 = faceB(ix, iy + 1);
+                        const double a1m = (a1 - fabs(a1)) / 2.0;
+                        a1p = (a1 + fabs(a1)) / 2.0;
+                        a2m = (a2 - fabs(a2)) / 2.0;
+                        const double a2p = (a2 + fabs(a2)) / 2.0;
+                        const double b1m = (b1 - fabs(b1)) / 2.0;
+                        b1p = (b1 + fabs(b1)) / 2.0;
+                        b2m = (b2 - fabs(b2)) / 2.0;
+                        const double b2p = (b2 + fabs(b2)) / 2.0;
+                        d = (a2p - a1m) / g.dx + (b2p - b1m) / g.dy;   // :479-481
+                    }
+                    st4(P_AQ + k, a1p, a2m, b1p, b2m);
+                    P_DD[k] = make_double2(P_delta[k], d);
                     const double v0 = interior ? 100.0 : 0.0;   // :446-449
                     P_Ta[k] = v0;
                     P_Tst[k] = v0;
-                }
-                __syncwarp();
-                for (size_t k = lane; k < n; k += 32) {   // diagonal, :479-481
-                    const int iy = (int)(k / nx), ix = (int)(k % nx);
-                    double d = 0.0;
-                    if (ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2) {
-                        const double a1 = P_A[k], a2 = P_A[k + 1], b1 = P_B[k], b2 = P_B[k + nx];
-                        const double a1m = (a1 - fabs(a1)) / 2.0;
-                        const double a2p = (a2 + fabs(a2)) / 2.0;
-                        const double b1m = (b1 - fabs(b1)) / 2.0;
-                        const double b2p = (b2 + fabs(b2)) / 2.0;
-                        d = (a2p - a1m) / g.dx + (b2p - b1m) / g.dy;
-                    }
-                    P_D[k] = d;
                 }
                 __syncwarp();
                 AdjPolicyExact Q;
@@ -265,53 +270,65 @@ __global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
                 Q.ny = ny;
                 Q.dx = g.dx;
                 Q.dy = g.dy;
-                Q.A = P_A;
-                Q.B = P_B;
-                Q.D = P_D;
-                Q.delta = P_delta;
+                Q.aq = P_AQ;
+                Q.dd = P_DD;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_Tst;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
-                        systolic_sweep(Q, +1, +1, false, l1, linf);
-                        systolic_sweep(Q, +1, -1, false, l1, linf);
-                        systolic_sweep(Q, -1, +1, false, l1, linf);
-                        systolic_sweep(Q, -1, -1, true, l1, linf);
+                        for (int sw = 0; sw < 4; sw++)
+                            systolic_sweep(Q, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
                         iters = iter + 1;
                         const double L1 = warp_sum(l1) / (double)(nx * ny);
                         const double Linf = warp_max(linf);
                         if (L1 < 1e-9 && Linf < 1e-9) break;
                     }
             } else {
-                float* P_W = reinterpret_cast<float*>(base + L.W);
+                Q4<float>* P_W = reinterpret_cast<Q4<float>*>(base + L.W);
+                float* P_C0 = reinterpret_cast<float*>(base + L.C0);
                 float* P_Ta = reinterpret_cast<float*>(base + L.Ta);
                 // weights of the rewritten update, computed in FP64 from FP64 T
+                // (FP32 path: reciprocals instead of divisions)
+                const double idx = 1.0 / g.dx, idy = 1.0 / g.dy;
+                const double i4dx = 1.0 / (4.0 * g.dx), i4dy = 1.0 / (4.0 * g.dy);
+                auto fA = [&](int ix, int iy) -> double {
+                    const size_t k = (size_t)iy * nx + ix;
+                    const double av = ISO ? B.a_a_row64[iy] : 0.5 * (a_a[k] + a_a[k - 1]);
+                    const double cv = ISO ? 0.0 : 0.5 * (c_a[k] + c_a[k - 1]);
+                    return -(T[k] - T[k - 1]) * idx * av
+                           + (T[k + nx] - T[k - nx] + T[k - 1 + nx] - T[k - 1 - nx]) * i4dy * cv;
+                };
+                auto fB = [&](int ix, int iy) -> double {
+                    const size_t k = (size_t)iy * nx + ix;
+                    const double bv = ISO ? B.b_iso64 : 0.5 * (b_p[k] + b_p[k - nx]);
+                    const double cv = ISO ? 0.0 : 0.5 * (c_a[k] + c_a[k - nx]);
+                    return -(T[k] - T[k - nx]) * idy * bv
+                           + (T[k + 1] - T[k - 1] + T[k + 1 - nx] - T[k - 1 - nx]) * i4dx * cv;
+                };
                 for (size_t k = lane; k < n; k += 32) {
                     const int iy = (int)(k / nx), ix = (int)(k % nx);
                     const bool interior = ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2;
                     float c0 = 0.f, wxm = 0.f, wxp = 0.f, wym = 0.f, wyp = 0.f;
                     if (interior) {
-                        const double a1 = faceA(ix, iy), a2 = faceA(ix + 1, iy);
-                        const double b1 = faceB(ix, iy), b2 = faceB(ix, iy + 1);
-                        const double a1m = (a1 - fabs(a1)) / 2.0, a1p = (a1 + fabs(a1)) / 2.0;
-                        const double a2m = (a2 - fabs(a2)) / 2.0, a2p = (a2 + fabs(a2)) / 2.0;
-                        const double b1m = (b1 - fabs(b1)) / 2.0, b1p = (b1 + fabs(b1)) / 2.0;
-                        const double b2m = (b2 - fabs(b2)) / 2.0, b2p = (b2 + fabs(b2)) / 2.0;
-                        const double d = (a2p - a1m) / g.dx + (b2p - b1m) / g.dy;
+                        const double a1 = fA(ix, iy), a2 = fA(ix + 1, iy);
+                        const double b1 = fB(ix, iy), b2 = fB(ix, iy + 1);
+                        const double a1p = fmax(a1, 0.0), a1m = fmin(a1, 0.0);
+                        const double a2p = fmax(a2, 0.0), a2m = fmin(a2, 0.0);
+                        const double b1p = fmax(b1, 0.0), b1m = fmin(b1, 0.0);
+                        const double b2p = fmax(b2, 0.0), b2m = fmin(b2, 0.0);
+                        const double d = (a2p - a1m) * idx + (b2p - b1m) * idy;
                         if (!(fabs(d) < 1e-14)) {
-                            c0 = (float)(P_delta[k] / d);
-                            wxm = (float)(a1p / g.dx / d);
-                            wxp = (float)(-a2m / g.dx / d);
-                            wym = (float)(b1p / g.dy / d);
-                            wyp = (float)(-b2m / g.dy / d);
+                            const double id = 1.0 / d;
+                            c0 = (float)(P_delta[k] * id);
+                            wxm = (float)(a1p * idx * id);
+                            wxp = (float)(-a2m * idx * id);
+                            wym = (float)(b1p * idy * id);
+                            wyp = (float)(-b2m * idy * id);
                         }
                     }
-                    P_W[k] = c0;
-                    P_W[n + k] = wxm;
-                    P_W[2 * n + k] = wxp;
-                    P_W[3 * n + k] = wym;
-                    P_W[4 * n + k] = wyp;
+                    st4(P_W + k, wxm, wxp, wym, wyp);
+                    P_C0[k] = c0;
                     const float v0 = interior ? 100.f : 0.f;
                     P_Ta[k] = v0;
                     P_tst[k] = v0;
@@ -321,23 +338,22 @@ __global__ void __launch_bounds__(128) batch_kernel(BatchArgs<S> B) {
                 Q.nx = nx;
                 Q.ny = ny;
                 Q.W = P_W;
+                Q.C0 = P_C0;
+                Q.vmax = 0.0;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_tst;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
-                        systolic_sweep(Q, +1, +1, false, l1, linf);
-                        systolic_sweep(Q, +1, -1, false, l1, linf);
-                        systolic_sweep(Q, -1, +1, false, l1, linf);
-                        systolic_sweep(Q, -1, -1, true, l1, linf);
+                        for (int sw = 0; sw < 4; sw++)
+                            systolic_sweep(Q, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
                         iters = iter + 1;
                         const double L1 = warp_sum(l1) / (double)(nx * ny);
                         const double Linf = warp_max(linf);
                         if (L1 < 1e-9 && Linf < 1e-9) break;
                         // FP32 fixed point: no cell changed by more than a few ulps
-                        double vmax = 0.0;
-                        for (size_t k = lane; k < n; k += 32) vmax = fmax(vmax, fabs((double)P_Ta[k]));
-                        vmax = warp_max(vmax);
+                        const double vmax = warp_max(Q.vmax);
+                        Q.vmax = 0.0;
                         if (Linf <= 4.0 * 5.960464477539063e-08 * vmax) break;
                     }
             }
@@ -388,9 +404,7 @@ inline BatchArgs<double> make_batch_args<double>(const BatchDesc& d) {
     B.a_a_row64 = d.a_a_row64;
     B.b_iso = d.b_iso;
     B.b_iso64 = d.b_iso;
-    B.a_f = d.a_f64;
-    B.b_p = d.b_p64;
-    B.c_f = d.c_f64;
+    B.mt = reinterpret_cast<const Q4<double>*>(d.mt64);
     B.b_p64 = d.b_p64;
     B.a_a64 = d.a_a64;
     B.c_a64 = d.c_a64;
@@ -401,6 +415,7 @@ inline BatchArgs<double> make_batch_args<double>(const BatchDesc& d) {
     B.ev = d.ev;
     B.out = d.out;
     B.sc = d.sc;
+    B.maxr = d.maxr;
     B.mode = d.mode;
     return B;
 }
@@ -417,9 +432,7 @@ inline BatchArgs<float> make_batch_args<float>(const BatchDesc& d) {
     B.a_a_row64 = d.a_a_row64;
     B.b_iso = d.b_iso32;
     B.b_iso64 = d.b_iso;
-    B.a_f = d.a_f32;
-    B.b_p = d.b_p32;
-    B.c_f = d.c_f32;
+    B.mt = reinterpret_cast<const Q4<float>*>(d.mt32);
     B.b_p64 = d.b_p64;
     B.a_a64 = d.a_a64;
     B.c_a64 = d.c_a64;
@@ -430,6 +443,7 @@ inline BatchArgs<float> make_batch_args<float>(const BatchDesc& d) {
     B.ev = d.ev;
     B.out = d.out;
     B.sc = d.sc;
+    B.maxr = d.maxr;
     B.mode = d.mode;
     return B;
 }

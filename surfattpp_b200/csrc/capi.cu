@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -87,8 +88,9 @@ struct sa_plan {
     DArr<int> iper, src, rec_ptr, rec_idx;
     DArr<double> G64, Gx64, Gy64;
     DArr<float> G32, Gx32, Gy32;
-    DArr<double> fun64, inv3, a_f64, b_p64, c_f64, a_a64, c_a64;
-    DArr<float> fun32, a_f32, b_p32, c_f32;
+    DArr<double> fun64, inv3, mt64, b_p64, a_a64, c_a64;
+    DArr<float> fun32, mt32;
+    int maxr = 0;
     DArr<double> chi_ev;
     DArr<int> status_tmp, worst;
     DArr<unsigned char> scratch;
@@ -203,6 +205,7 @@ int plan_events(sa_plan* P, int ne, const double* evlo, const double* evla, cons
         const int nr = rec_ptr[e + 1] - rec_ptr[e];
         if (nr < 0) return fail(ctx, SA_ERR_ARG, "rec_ptr must be non-decreasing");
         if ((size_t)nr > n) return fail(ctx, SA_ERR_ARG, "more receivers than grid cells");
+        P->maxr = std::max(P->maxr, nr);
     }
     for (int i = 0; i < P->npair; i++)
         if (rec_idx[i] < 0 || rec_idx[i] >= nsta)
@@ -262,12 +265,45 @@ int plan_events(sa_plan* P, int ne, const double* evlo, const double* evla, cons
     const size_t ng = (size_t)std::max(nsrc, 1) * n;
     SA_CUDA(P->G64.alloc(ng));
     if (P->prec == SA_FP64) {
+        // FP64 parity path: great-circle geometry from the C library's acos,
+        // i.e. the very T0 a CPU evaluation of src/eikonal_solver.cpp:96-116
+        // produces.  It depends on the stations only and is built once per
+        // plan; T, residuals and adjoint fields are then bit-identical.
         SA_CUDA(P->Gx64.alloc(ng));
         SA_CUDA(P->Gy64.alloc(ng));
-        if (nsrc)
-            SA_CUDA(launch_geometry<double>(nx, ny, nsrc, P->siny.p, P->cosy.p, d_sy0.p, d_cy0.p,
-                                            d_cdl.p, d_sdl.p, P->G64.p, P->Gx64.p, P->Gy64.p,
-                                            nullptr, st));
+        std::vector<double> hG(ng), hGx(ng), hGy(ng), sy(ny), cy(ny);
+        SA_CUDA(cudaMemcpy(sy.data(), P->siny.p, ny * sizeof(double), cudaMemcpyDeviceToHost));
+        SA_CUDA(cudaMemcpy(cy.data(), P->cosy.p, ny * sizeof(double), cudaMemcpyDeviceToHost));
+        const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 64));
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nth; t++)
+            pool.emplace_back([&, t]() {
+                for (int s = t; s < nsrc; s += nth)
+                    for (int iy = 0; iy < ny; iy++)
+                        for (int ix = 0; ix < nx; ix++) {
+                            const size_t i = (size_t)s * n + (size_t)iy * nx + ix;
+                            const double cdlv = cdl[(size_t)s * nx + ix];
+                            const double sdlv = sdl[(size_t)s * nx + ix];
+                            const double tmp = sy[iy] * sy0[s] + cy[iy] * cy0[s] * cdlv;
+                            const double tmp_c = std::max(-1.0, std::min(1.0, tmp));
+                            hG[i] = std::acos(tmp_c) * R_EARTH;
+                            const double sin_d = std::sqrt(std::max(0.0, 1.0 - tmp_c * tmp_c));
+                            if (sin_d < 1e-14) {
+                                hGx[i] = 0.0;
+                                hGy[i] = 0.0;
+                            } else {
+                                hGx[i] = cy[iy] * cy0[s] * sdlv / sin_d * R_EARTH;
+                                hGy[i] = -(cy[iy] * sy0[s] - sy[iy] * cy0[s] * cdlv) / sin_d * R_EARTH;
+                            }
+                        }
+            });
+        for (auto& th : pool) th.join();
+        if (nsrc) {
+            SA_CUDA(cudaMemcpyAsync(P->G64.p, hG.data(), ng * sizeof(double), cudaMemcpyHostToDevice, st));
+            SA_CUDA(cudaMemcpyAsync(P->Gx64.p, hGx.data(), ng * sizeof(double), cudaMemcpyHostToDevice, st));
+            SA_CUDA(cudaMemcpyAsync(P->Gy64.p, hGy.data(), ng * sizeof(double), cudaMemcpyHostToDevice, st));
+            SA_CUDA(cudaStreamSynchronize(st));
+        }
     } else {
         SA_CUDA(P->G32.alloc(ng));
         SA_CUDA(P->Gx32.alloc(ng));
@@ -283,7 +319,8 @@ int plan_events(sa_plan* P, int ne, const double* evlo, const double* evla, cons
     SA_CUDA(P->queue.alloc(1));
     // scratch slots: one per resident warp, bounded by events and free memory
     const int maxs = P->prec == SA_FP64 ? batch64_max_slots(ctx->device) : batch32_max_slots(ctx->device);
-    P->slot_bytes = P->prec == SA_FP64 ? batch64_slot_bytes(nx, ny) : batch32_slot_bytes(nx, ny);
+    P->slot_bytes = P->prec == SA_FP64 ? batch64_slot_bytes(nx, ny, P->maxr)
+                                       : batch32_slot_bytes(nx, ny, P->maxr);
     size_t fr = 0, tot = 0;
     SA_CUDA(cudaMemGetInfo(&fr, &tot));
     const size_t budget = fr / 10 * 7;
@@ -304,25 +341,19 @@ int plan_media(sa_plan* P, const double* svel, const double* m11, const double* 
     SA_CUDA(P->fun64.alloc(np));
     SA_CUDA(P->inv3.alloc(np));
     if (general) {
-        SA_CUDA(P->a_f64.alloc(np));
+        SA_CUDA(P->mt64.alloc(4 * np));
         SA_CUDA(P->b_p64.alloc(np));
-        SA_CUDA(P->c_f64.alloc(np));
         SA_CUDA(P->a_a64.alloc(np));
         SA_CUDA(P->c_a64.alloc(np));
     }
     SA_CUDA(launch_media64(P->nx, P->ny, P->nper, svel, general ? m11 : nullptr, m12, m22,
-                           P->cosy.p, P->fun64.p, P->inv3.p, P->a_f64.p, P->b_p64.p, P->c_f64.p,
-                           P->a_a64.p, P->c_a64.p, st));
+                           P->cosy.p, P->fun64.p, P->inv3.p, P->mt64.p, P->b_p64.p, P->a_a64.p,
+                           P->c_a64.p, st));
     if (P->prec == SA_FP32) {
         SA_CUDA(P->fun32.alloc(np));
-        if (general) {
-            SA_CUDA(P->a_f32.alloc(np));
-            SA_CUDA(P->b_p32.alloc(np));
-            SA_CUDA(P->c_f32.alloc(np));
-        }
-        SA_CUDA(launch_media32(P->nx, P->ny, P->nper, P->fun64.p, general ? P->a_f64.p : nullptr,
-                               P->b_p64.p, P->c_f64.p, P->fun32.p, P->a_f32.p, P->b_p32.p,
-                               P->c_f32.p, st));
+        if (general) SA_CUDA(P->mt32.alloc(4 * np));
+        SA_CUDA(launch_media32(P->nx, P->ny, P->nper, P->fun64.p, general ? P->mt64.p : nullptr,
+                               P->fun32.p, P->mt32.p, st));
     }
     return SA_OK;
 }
@@ -346,9 +377,8 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
     d.a_f_row64 = P->a_f_row64.p;
     d.a_a_row64 = P->a_a_row64.p;
     d.b_iso = 1.0 / (R_EARTH * R_EARTH);
-    d.a_f64 = P->a_f64.p;
+    d.mt64 = P->mt64.p;
     d.b_p64 = P->b_p64.p;
-    d.c_f64 = P->c_f64.p;
     d.a_a64 = P->a_a64.p;
     d.c_a64 = P->c_a64.p;
     d.G64 = P->G64.p;
@@ -357,9 +387,7 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
     d.fun32 = P->fun32.p;
     d.a_f_row32 = P->a_f_row32.p;
     d.b_iso32 = (float)d.b_iso;
-    d.a_f32 = P->a_f32.p;
-    d.b_p32 = P->b_p32.p;
-    d.c_f32 = P->c_f32.p;
+    d.mt32 = P->mt32.p;
     d.G32 = P->G32.p;
     d.Gx32 = P->Gx32.p;
     d.Gy32 = P->Gy32.p;
@@ -377,6 +405,7 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
     d.sc.slot_bytes = P->slot_bytes;
     d.sc.base = P->scratch.p;
     d.sc.queue = P->queue.p;
+    d.maxr = P->maxr;
     return d;
 }
 
@@ -626,8 +655,7 @@ int single_solve(sa_ctx* ctx, int precision, int nx, int ny, const double* xx_de
     if ((rc = chk(cudaMemcpyAsync(P->fun64.p, fin.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st))))
         return done(rc);
     if (precision == SA_FP32 &&
-        (rc = chk(launch_media32(nx, ny, 1, P->fun64.p, P->a_f64.p, P->b_p64.p, P->c_f64.p,
-                                 P->fun32.p, P->a_f32.p, P->b_p32.p, P->c_f32.p, st))))
+        (rc = chk(launch_media32(nx, ny, 1, P->fun64.p, P->mt64.p, P->fun32.p, P->mt32.p, st))))
         return done(rc);
     BatchDesc d = plan_desc(P, true);
     d.ev.sadj = sa_.p;

@@ -19,8 +19,8 @@ namespace sa {
 __global__ void media64_kernel(int nx, int ny, int nper, const double* __restrict__ svel,
                                const double* __restrict__ m11, const double* __restrict__ m12,
                                const double* __restrict__ m22, const double* __restrict__ cosy,
-                               double* fun, double* inv3, double* a_f, double* b_p, double* c_f,
-                               double* a_a, double* c_a) {
+                               double* fun, double* inv3, double* mt, double* b_p, double* a_a,
+                               double* c_a) {
     const size_t n = (size_t)nx * ny;
     const size_t total = n * nper;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
@@ -34,9 +34,12 @@ __global__ void media64_kernel(int nx, int ny, int nper, const double* __restric
             const double cos2_y = cos_y * cos_y;
             const double R2 = R_EARTH * R_EARTH;
             const double spha = m11[i], sphb = m22[i], sphc = -m12[i];
-            a_f[i] = spha / (R2 * cos2_y);
-            b_p[i] = sphb / R2;
-            c_f[i] = sphc / (R_EARTH * R_EARTH * cos_y);
+            const double bv = sphb / R2;
+            mt[4 * i + 0] = spha / (R2 * cos2_y);
+            mt[4 * i + 1] = bv;
+            mt[4 * i + 2] = sphc / (R_EARTH * R_EARTH * cos_y);
+            mt[4 * i + 3] = 0.0;
+            b_p[i] = bv;
             a_a[i] = spha / (R2 * cos_y * cos_y);
             c_a[i] = sphc / (R2 * cos_y);
         }
@@ -86,25 +89,27 @@ __global__ void geometry_kernel(int nx, int ny, int nsrc, const double* __restri
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-size_t batch64_slot_bytes(int nx, int ny) { return slot_layout<double>(nx, ny).total; }
+size_t batch64_slot_bytes(int nx, int ny, int maxr) {
+    return slot_layout<double>(nx, ny, maxr).total;
+}
 
 int batch64_max_slots(int device) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<double>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<double, true>, 128, 0);
     if (per_sm < 1) per_sm = 1;
     return nsm * per_sm * 4;
 }
 
 cudaError_t launch_media64(int nx, int ny, int nper, const double* svel, const double* m11,
                            const double* m12, const double* m22, const double* cosy,
-                           double* fun, double* inv3, double* a_f, double* b_p, double* c_f,
-                           double* a_a, double* c_a, cudaStream_t st) {
+                           double* fun, double* inv3, double* mt, double* b_p, double* a_a,
+                           double* c_a, cudaStream_t st) {
     const size_t total = (size_t)nx * ny * nper;
     const int threads = 256;
     const int blocks = (int)std::min<size_t>((total + threads - 1) / threads, 148 * 16);
     media64_kernel<<<blocks, threads, 0, st>>>(nx, ny, nper, svel, m11, m12, m22, cosy, fun,
-                                                inv3, a_f, b_p, c_f, a_a, c_a);
+                                                inv3, mt, b_p, a_a, c_a);
     return cudaGetLastError();
 }
 
@@ -132,7 +137,8 @@ template cudaError_t launch_geometry<float>(int, int, int, const double*, const 
 cudaError_t launch_batch64(const BatchDesc& d, cudaStream_t st) {
     const BatchArgs<double> B = make_batch_args<double>(d);
     const int blocks = (d.sc.nslots + 3) / 4;
-    batch_kernel<double><<<blocks, 128, 0, st>>>(B);
+    if (d.iso) batch_kernel<double, true><<<blocks, 128, 0, st>>>(B);
+    else batch_kernel<double, false><<<blocks, 128, 0, st>>>(B);
     return cudaGetLastError();
 }
 

@@ -13,13 +13,40 @@ namespace sa {
 __device__ __forceinline__ double abs_(double x) { return fabs(x); }
 __device__ __forceinline__ float abs_(float x) { return fabsf(x); }
 
+// Four values of precision S loaded with 16-byte vector loads (one load for
+// FP32, two for FP64): the per-cell operands of a sweep are packed so that a
+// lane fetches its next cell with one or two instructions.
+template <class S>
+struct Q4 {
+    S x, y, z, w;
+};
+__device__ __forceinline__ Q4<float> ld4(const Q4<float>* p) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ Q4<double> ld4(const Q4<double>* p) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st4(Q4<float>* p, float x, float y, float z, float w) {
+    *reinterpret_cast<float4*>(p) = make_float4(x, y, z, w);
+}
+__device__ __forceinline__ void st4(Q4<double>* p, double x, double y, double z, double w) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(x, y);
+    reinterpret_cast<double2*>(p)[1] = make_double2(z, w);
+}
+
 // One cell update of eikonal::FSM_UW_PS_lonlat_2d (src/eikonal_solver.cpp:157-283).
 // xm/xp/ym/yp carry tau and T0 of the axis neighbours (ix-1, ix+1, iy-1, iy+1).
-template <class S>
+// ISO: flat isotropic surface, c == +0 exactly.  The c terms are then
+// signed zeros added to non-zero values and are dropped without changing any
+// rounded result or comparison.
+template <class S, bool ISO>
 __device__ __forceinline__ S fsm_update(S tau, S t0, S t0x, S t0y, S aij, S bij, S cij, S fij,
                                         S dx, S dy, const Nb<S, S>& xm, const Nb<S, S>& xp,
                                         const Nb<S, S>& ym, const Nb<S, S>& yp) {
-    const S det = aij * bij - cij * cij;
+    const S det = ISO ? aij * bij : aij * bij - cij * cij;
     const S tdx = t0 / dx;
     const S tdy = t0 / dy;
 #pragma unroll
@@ -33,9 +60,16 @@ __device__ __forceinline__ S fsm_update(S tau, S t0, S t0x, S t0y, S aij, S bij,
         const S qx = sx * tdx * nxn.v;
         const S py = t0y - sy * tdy;
         const S qy = sy * tdy * nyn.v;
-        const S eq_a = aij * px * px + bij * py * py - S(2.0) * cij * px * py;
-        const S eq_b = S(2.0) * (aij * px * qx + bij * py * qy - cij * (px * qy + py * qx));
-        const S eq_c = aij * qx * qx + bij * qy * qy - S(2.0) * cij * qx * qy - fij * fij;
+        S eq_a, eq_b, eq_c;
+        if (ISO) {
+            eq_a = aij * px * px + bij * py * py;
+            eq_b = S(2.0) * (aij * px * qx + bij * py * qy);
+            eq_c = aij * qx * qx + bij * qy * qy - fij * fij;
+        } else {
+            eq_a = aij * px * px + bij * py * py - S(2.0) * cij * px * py;
+            eq_b = S(2.0) * (aij * px * qx + bij * py * qy - cij * (px * qy + py * qx));
+            eq_c = aij * qx * qx + bij * qy * qy - S(2.0) * cij * qx * qy - fij * fij;
+        }
         const S Delta = eq_b * eq_b - S(4.0) * eq_a * eq_c;
         if (Delta < S(0) || abs_(eq_a) < S(1e-30)) continue;
         const S sq = sqrt(Delta);
@@ -45,8 +79,8 @@ __device__ __forceinline__ S fsm_update(S tau, S t0, S t0x, S t0y, S aij, S bij,
             const S tmp_tau = (-eq_b + (sgn == 0 ? sq : -sq)) / two_a;
             const S Tx = px * tmp_tau + qx;
             const S Ty = py * tmp_tau + qy;
-            const S char_x = aij * Tx - cij * Ty;
-            const S char_y = bij * Ty - cij * Tx;
+            const S char_x = ISO ? aij * Tx : aij * Tx - cij * Ty;
+            const S char_y = ISO ? bij * Ty : bij * Ty - cij * Tx;
             if (-sx * char_x >= S(0) && -sy * char_y >= S(0))
                 if (tmp_tau < tau) tau = tmp_tau;
         }
@@ -98,35 +132,39 @@ __device__ __forceinline__ S fsm_update(S tau, S t0, S t0x, S t0y, S aij, S bij,
     return tau;
 }
 
-// Forward sweep policy.  Field: tau (sweep precision S) in the warp's
-// scratch slot; tau_start holds the field at the start of the iteration for
-// the convergence test (src/eikonal_solver.cpp:147, :292-302).
+// Forward sweep policies.  Per cell the sweep reads one packed record
+// pk = {T0, T0x, T0y, fun} (built per event) and, for a general metric, one
+// record mt = {a, b, c, 0} (built per period); the evolving field is a
+// separate plane.  tau_start holds the field at the start of the iteration
+// for the convergence test (src/eikonal_solver.cpp:147, :292-302).
+template <class S, bool ISO>
+struct MetricCell {
+    S a, b, c;
+};
 template <class S>
-struct FwdPolicy {
+struct MetricCell<S, true> {};
+
+template <class S, bool ISO>
+struct FwdBase {
     using V = S;
     using X = S;
+    static constexpr int kLead = 1;
     struct Cell {
-        S v;    // tau before this update
+        S v;    // field before this update
         S x;    // T0 of the cell
-        S gx, gy, f, a, b, c, vs;
+        S gx, gy, f, vs;
+        MetricCell<S, ISO> m;
     };
     int nx, ny;
-    S dx, dy, fun0;
-    const S* G;
-    const S* Gx;
-    const S* Gy;
-    const S* fun;        // period plane
+    const Q4<S>* pk;     // per event
+    const Q4<S>* mt;     // per period (general metric) or null
     const S* a_row;      // iso: [ny]
     S b_iso;
-    const S* a_pl;       // general planes or null
-    const S* b_pl;
-    const S* c_pl;
     S* tau;
     S* tau_start;
     int fix_x0, fix_x1;  // fixed source columns [fix_x0, fix_x1]
     const double* yy;
     double y0, dy64;
-    // per-row state
     bool row_fixed;
     S row_a;
 
@@ -137,54 +175,72 @@ struct FwdPolicy {
     __device__ void begin_row(int iy, bool act) {
         if (!act) return;
         row_fixed = fabs((yy[iy] - y0) / dy64) <= 1.0;
-        row_a = a_pl ? S(0) : a_row[iy];
+        if (ISO) row_a = a_row[iy];
     }
     __device__ Cell load(int iy, int ix, bool last) const {
         const size_t k = (size_t)iy * nx + ix;
         Cell c;
         c.v = tau[k];
-        c.x = G[k] * fun0;
-        c.gx = Gx[k];
-        c.gy = Gy[k];
-        c.f = fun[k];
-        if (a_pl) {
-            c.a = a_pl[k];
-            c.b = b_pl[k];
-            c.c = c_pl[k];
-        } else {
-            c.a = row_a;
-            c.b = b_iso;
-            c.c = S(0);
+        const Q4<S> q = ld4(pk + k);
+        c.x = q.x;
+        c.gx = q.y;
+        c.gy = q.z;
+        c.f = q.w;
+        if constexpr (!ISO) {
+            const Q4<S> m = ld4(mt + k);
+            c.m.a = m.x;
+            c.m.b = m.y;
+            c.m.c = m.z;
         }
         c.vs = last ? tau_start[k] : S(0);
         return c;
+    }
+    __device__ S ca(const Cell& c) const {
+        if constexpr (ISO) return row_a; else return c.m.a;
+    }
+    __device__ S cb(const Cell& c) const {
+        if constexpr (ISO) return b_iso; else return c.m.b;
+    }
+    __device__ S cc(const Cell& c) const {
+        if constexpr (ISO) return S(0); else return c.m.c;
     }
     __device__ Cell load_nb(int iy, int ix) const {
         const size_t k = (size_t)iy * nx + ix;
         Cell c{};
         c.v = tau[k];
-        c.x = G[k] * fun0;
+        c.x = pk[k].x;
         return c;
-    }
-    __device__ S update(const Cell& cur, int iy, int ix, const Nb<S, S>& xm, const Nb<S, S>& xp,
-                        const Nb<S, S>& ym, const Nb<S, S>& yp, bool last, double& l1,
-                        double& linf) const {
-        if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;   // ischange == 0
-        const S t0x = cur.gx * fun0;
-        const S t0y = cur.gy * fun0;
-        const S nv = fsm_update<S>(cur.v, cur.x, t0x, t0y, cur.a, cur.b, cur.c, cur.f, dx, dy,
-                                   xm, xp, ym, yp);
-        if (last) {
-            const double d = fabs((double)nv - (double)cur.vs) * (double)cur.x;
-            l1 += d;
-            linf = fmax(linf, d);
-        }
-        return nv;
     }
     __device__ void store(int iy, int ix, S v, bool last) const {
         const size_t k = (size_t)iy * nx + ix;
         tau[k] = v;
         if (last) tau_start[k] = v;
+    }
+};
+
+// FP64 forward: field tau, exact reference update.
+template <bool ISO>
+struct FwdPolicy64 : FwdBase<double, ISO> {
+    using Base = FwdBase<double, ISO>;
+    using Cell = typename Base::Cell;
+    using Base::row_fixed;
+    using Base::fix_x0;
+    using Base::fix_x1;
+    double dx, dy;
+    __device__ double update(const Cell& cur, int iy, int ix, const Nb<double, double>& xm,
+                             const Nb<double, double>& xp, const Nb<double, double>& ym,
+                             const Nb<double, double>& yp, bool last, double& l1,
+                             double& linf) const {
+        if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;   // ischange == 0
+        const double nv = fsm_update<double, ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur),
+                                                  this->cb(cur), this->cc(cur), cur.f, dx, dy, xm,
+                                                  xp, ym, yp);
+        if (last) {
+            const double d = fabs(nv - cur.vs) * cur.x;
+            l1 += d;
+            linf = fmax(linf, d);
+        }
+        return nv;
     }
 };
 
@@ -198,6 +254,7 @@ struct FwdPolicy {
 //   A0 = t0x*(1+u_x), A1 = t0x - sx*t0/dx,
 //   B0 = t0y*(1+u_x) - sy*(t0/dy)*(u_x - u_y), B1 = t0y - sy*t0/dy,
 // solved with the cancellation-free quadratic formula.
+template <bool ISO>
 __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, float t0y,
                                                   float aij, float bij, float cij, float fij,
                                                   float idx, float idy,
@@ -205,7 +262,7 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
                                                   const Nb<float, float>& xp,
                                                   const Nb<float, float>& ym,
                                                   const Nb<float, float>& yp) {
-    const float det = aij * bij - cij * cij;
+    const float det = ISO ? aij * bij : aij * bij - cij * cij;
     const float k = t0 * idx;
     const float m = t0 * idy;
     const float f2 = fij * fij;
@@ -222,9 +279,16 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
         const float A1 = t0x - sx * k;
         const float B0 = fmaf(t0y, ux, t0y) - sy * m * (ux - uy);
         const float B1 = t0y - sy * m;
-        const float al = aij * A1 * A1 + bij * B1 * B1 - 2.f * cij * A1 * B1;
-        const float be = 2.f * (aij * A0 * A1 + bij * B0 * B1 - cij * (A0 * B1 + A1 * B0));
-        const float ga = aij * A0 * A0 + bij * B0 * B0 - 2.f * cij * A0 * B0 - f2;
+        float al, be, ga;
+        if (ISO) {
+            al = aij * A1 * A1 + bij * B1 * B1;
+            be = 2.f * (aij * A0 * A1 + bij * B0 * B1);
+            ga = aij * A0 * A0 + bij * B0 * B0 - f2;
+        } else {
+            al = aij * A1 * A1 + bij * B1 * B1 - 2.f * cij * A1 * B1;
+            be = 2.f * (aij * A0 * A1 + bij * B0 * B1 - cij * (A0 * B1 + A1 * B0));
+            ga = aij * A0 * A0 + bij * B0 * B0 - 2.f * cij * A0 * B0 - f2;
+        }
         const float disc = be * be - 4.f * al * ga;
         if (disc < 0.f || fabsf(al) < 1e-30f) continue;
         const float sq = sqrtf(disc);
@@ -237,8 +301,8 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
             const float D = Dr[r];
             const float Tx = fmaf(A1, D, A0);
             const float Ty = fmaf(B1, D, B0);
-            const float char_x = aij * Tx - cij * Ty;
-            const float char_y = bij * Ty - cij * Tx;
+            const float char_x = ISO ? aij * Tx : aij * Tx - cij * Ty;
+            const float char_y = ISO ? bij * Ty : bij * Ty - cij * Tx;
             if (-sx * char_x >= 0.f && -sy * char_y >= 0.f) {
                 const float c = ux + D;
                 if (c < u) u = c;
@@ -270,77 +334,23 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
     return u;
 }
 
-// FP32 forward policy: field u = tau - 1.
-struct FwdPolicyDelta32 {
-    using V = float;
-    using X = float;
-    struct Cell {
-        float v;    // u before this update
-        float x;    // T0 of the cell
-        float gx, gy, f, a, b, c, vs;
-    };
-    int nx, ny;
-    float idx, idy, fun0;
-    const float* G;
-    const float* Gx;
-    const float* Gy;
-    const float* fun;
-    const float* a_row;
-    float b_iso;
-    const float* a_pl;
-    const float* b_pl;
-    const float* c_pl;
-    float* tau;         // holds u
-    float* tau_start;
-    int fix_x0, fix_x1;
-    const double* yy;
-    double y0, dy64;
-    bool row_fixed;
-    float row_a;
-
-    __device__ int nrows() const { return ny; }
-    __device__ int ncols() const { return nx; }
-    __device__ int row(int rp, int yd) const { return yd > 0 ? rp : ny - 1 - rp; }
-    __device__ int col(int cp, int xd) const { return xd > 0 ? cp : nx - 1 - cp; }
-    __device__ void begin_row(int iy, bool act) {
-        if (!act) return;
-        row_fixed = fabs((yy[iy] - y0) / dy64) <= 1.0;
-        row_a = a_pl ? 0.f : a_row[iy];
-    }
-    __device__ Cell load(int iy, int ix, bool last) const {
-        const size_t k = (size_t)iy * nx + ix;
-        Cell c;
-        c.v = tau[k];
-        c.x = G[k] * fun0;
-        c.gx = Gx[k];
-        c.gy = Gy[k];
-        c.f = fun[k];
-        if (a_pl) {
-            c.a = a_pl[k];
-            c.b = b_pl[k];
-            c.c = c_pl[k];
-        } else {
-            c.a = row_a;
-            c.b = b_iso;
-            c.c = 0.f;
-        }
-        c.vs = last ? tau_start[k] : 0.f;
-        return c;
-    }
-    __device__ Cell load_nb(int iy, int ix) const {
-        const size_t k = (size_t)iy * nx + ix;
-        Cell c{};
-        c.v = tau[k];
-        c.x = G[k] * fun0;
-        return c;
-    }
+// FP32 forward: field u = tau - 1, increment-form update.
+template <bool ISO>
+struct FwdPolicyDelta32 : FwdBase<float, ISO> {
+    using Base = FwdBase<float, ISO>;
+    using Cell = typename Base::Cell;
+    using Base::row_fixed;
+    using Base::fix_x0;
+    using Base::fix_x1;
+    float idx, idy;
     __device__ float update(const Cell& cur, int iy, int ix, const Nb<float, float>& xm,
                             const Nb<float, float>& xp, const Nb<float, float>& ym,
                             const Nb<float, float>& yp, bool last, double& l1,
                             double& linf) const {
         if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;
-        const float nv = fsm_update_delta(cur.v, cur.x, cur.gx * fun0, cur.gy * fun0, cur.a,
-                                          cur.b, cur.c, cur.f, idx, idy, xm, xp, ym, yp);
+        const float nv = fsm_update_delta<ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur),
+                                               this->cb(cur), this->cc(cur), cur.f, idx, idy, xm,
+                                               xp, ym, yp);
         if (last) {
             const double d = fabs((double)nv - (double)cur.vs) * (double)cur.x;
             l1 += d;
@@ -348,31 +358,27 @@ struct FwdPolicyDelta32 {
         }
         return nv;
     }
-    __device__ void store(int iy, int ix, float v, bool last) const {
-        const size_t k = (size_t)iy * nx + ix;
-        tau[k] = v;
-        if (last) tau_start[k] = v;
-    }
 };
 
 // Adjoint sweep policy, exact FP64 form (src/eikonal_solver.cpp:471-509),
-// over the interior.  A(ix,iy) = a1 (left-face flux) for ix in [1,nx-1] and
-// a2(ix) == A(ix+1); B(ix,iy) = b1 (bottom-face flux) for iy in [1,ny-1] and
-// b2(iy) == B(iy+1) (identical expressions in the reference).  D = diagonal.
+// over the interior.  Per cell: aq = {a1p, a2m, b1p, b2m} (the positive /
+// negative parts of the left/right/bottom/top face fluxes, :404-441) and
+// dd = {delta, d} with d = (a2p - a1m)/dx + (b2p - b1m)/dy (:479-481).
 struct AdjPolicyExact {
     using V = double;
     using X = float;      // no auxiliary neighbour data
+    static constexpr int kLead = 2;
     struct Cell {
         double v;
         float x;
+        Q4<double> q;
+        double2 de;
         double vs;
     };
     int nx, ny;
     double dx, dy;
-    const double* A;
-    const double* B;
-    const double* D;
-    const double* delta;
+    const Q4<double>* aq;
+    const double2* dd;
     double* Ta;
     double* Ta_start;
 
@@ -386,6 +392,8 @@ struct AdjPolicyExact {
         Cell c;
         c.v = Ta[k];
         c.x = 0.f;
+        c.q = ld4(aq + k);
+        c.de = dd[k];
         c.vs = last ? Ta_start[k] : 0.0;
         return c;
     }
@@ -398,29 +406,23 @@ struct AdjPolicyExact {
                              const Nb<double, float>& xp, const Nb<double, float>& ym,
                              const Nb<double, float>& yp, bool last, double& l1,
                              double& linf) const {
-        const size_t k = (size_t)iy * nx + ix;
-        const double d = D[k];
+        const double2 de = cur.de;
         double nv;
-        if (fabs(d) < 1e-14) {
+        if (fabs(de.y) < 1e-14) {
             nv = 0.0;
         } else {
-            const double a1 = A[k], a2 = A[k + 1];
-            const double b1 = B[k], b2 = B[k + nx];
-            const double a1p = (a1 + fabs(a1)) / 2.0;
-            const double a2m = (a2 - fabs(a2)) / 2.0;
-            const double b1p = (b1 + fabs(b1)) / 2.0;
-            const double b2m = (b2 - fabs(b2)) / 2.0;
+            const Q4<double>& q = cur.q;
             const double txm = xm.has ? xm.v : 0.0;
             const double txp = xp.has ? xp.v : 0.0;
             const double tym = ym.has ? ym.v : 0.0;
             const double typ = yp.has ? yp.v : 0.0;
-            const double e = (txm * a1p - txp * a2m) / dx + (tym * b1p - typ * b2m) / dy;
-            nv = (delta[k] + e) / d;
+            const double e = (txm * q.x - txp * q.y) / dx + (tym * q.z - typ * q.w) / dy;
+            nv = (de.x + e) / de.y;
         }
         if (last) {
-            const double dd = fabs(nv - cur.vs);
-            l1 += dd;
-            linf = fmax(linf, dd);
+            const double dv = fabs(nv - cur.vs);
+            l1 += dv;
+            linf = fmax(linf, dv);
         }
         return nv;
     }
@@ -433,21 +435,24 @@ struct AdjPolicyExact {
 
 // Adjoint sweep policy, FP32 weight form: the same Gauss-Seidel update
 // rewritten as Ta = c0 + wxm*Ta(ix-1) + wxp*Ta(ix+1) + wym*Ta(iy-1) + wyp*Ta(iy+1)
-// with FP32 weights precomputed in FP64 (W plane = 5 floats per cell).
+// with FP32 weights computed in FP64 (w = {wxm, wxp, wym, wyp}, c0 separate).
 struct AdjPolicyW32 {
     using V = float;
     using X = float;
+    static constexpr int kLead = 4;
     struct Cell {
         float v;
         float x;
-        float c0, wxm, wxp, wym, wyp;
+        Q4<float> w;
+        float c0;
         float vs;
     };
     int nx, ny;
-    const float* W;     // [5][ny][nx]
+    const Q4<float>* W;
+    const float* C0;
     float* Ta;
     float* Ta_start;
-    float* vmax;        // unused placeholder
+    double vmax;        // max |Ta| seen in the last sweep of an iteration
 
     __device__ int nrows() const { return ny - 2; }
     __device__ int ncols() const { return nx - 2; }
@@ -455,16 +460,12 @@ struct AdjPolicyW32 {
     __device__ int col(int cp, int xd) const { return xd > 0 ? 1 + cp : nx - 2 - cp; }
     __device__ void begin_row(int, bool) {}
     __device__ Cell load(int iy, int ix, bool last) const {
-        const size_t n = (size_t)nx * ny;
         const size_t k = (size_t)iy * nx + ix;
         Cell c;
         c.v = Ta[k];
         c.x = 0.f;
-        c.c0 = W[k];
-        c.wxm = W[n + k];
-        c.wxp = W[2 * n + k];
-        c.wym = W[3 * n + k];
-        c.wyp = W[4 * n + k];
+        c.w = ld4(W + k);
+        c.c0 = C0[k];
         c.vs = last ? Ta_start[k] : 0.f;
         return c;
     }
@@ -481,11 +482,12 @@ struct AdjPolicyW32 {
         const float txp = xp.has ? xp.v : 0.f;
         const float tym = ym.has ? ym.v : 0.f;
         const float typ = yp.has ? yp.v : 0.f;
-        const float nv = cur.c0 + cur.wxm * txm + cur.wxp * txp + cur.wym * tym + cur.wyp * typ;
+        const float nv = cur.c0 + cur.w.x * txm + cur.w.y * txp + cur.w.z * tym + cur.w.w * typ;
         if (last) {
-            const double dd = fabs((double)nv - (double)cur.vs);
-            l1 += dd;
-            linf = fmax(linf, dd);
+            const double dv = fabs((double)nv - (double)cur.vs);
+            l1 += dv;
+            linf = fmax(linf, dv);
+            const_cast<AdjPolicyW32*>(this)->vmax = fmax(vmax, fabs((double)nv));
         }
         return nv;
     }

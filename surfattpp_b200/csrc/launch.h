@@ -19,9 +19,8 @@ struct BatchDesc {
     const double* a_f_row64;
     const double* a_a_row64;
     double b_iso;
-    const double* a_f64;
+    const double* mt64;     // packed {a, b, c, 0} forward metric per period (general)
     const double* b_p64;
-    const double* c_f64;
     const double* a_a64;
     const double* c_a64;
     const double* G64;
@@ -31,30 +30,28 @@ struct BatchDesc {
     const float* fun32;
     const float* a_f_row32;
     float b_iso32;
-    const float* a_f32;
-    const float* b_p32;
-    const float* c_f32;
+    const float* mt32;
     const float* G32;
     const float* Gx32;
     const float* Gy32;
     Events ev;
     Outputs out;
     Scratch sc;
+    int maxr;
     int mode;
 };
 
-size_t batch64_slot_bytes(int nx, int ny);
+size_t batch64_slot_bytes(int nx, int ny, int maxr);
 int batch64_max_slots(int device);
-size_t batch32_slot_bytes(int nx, int ny);
+size_t batch32_slot_bytes(int nx, int ny, int maxr);
 int batch32_max_slots(int device);
 
 cudaError_t launch_media64(int nx, int ny, int nper, const double* svel, const double* m11,
                            const double* m12, const double* m22, const double* cosy,
-                           double* fun, double* inv3, double* a_f, double* b_p, double* c_f,
-                           double* a_a, double* c_a, cudaStream_t st);
-cudaError_t launch_media32(int nx, int ny, int nper, const double* fun64, const double* a_f64,
-                           const double* b_p64, const double* c_f64, float* fun32, float* a_f32,
-                           float* b_p32, float* c_f32, cudaStream_t st);
+                           double* fun, double* inv3, double* mt, double* b_p, double* a_a,
+                           double* c_a, cudaStream_t st);
+cudaError_t launch_media32(int nx, int ny, int nper, const double* fun64, const double* mt64,
+                           float* fun32, float* mt32, cudaStream_t st);
 template <class T>
 cudaError_t launch_geometry(int nx, int ny, int nsrc, const double* siny, const double* cosy,
                             const double* sy0, const double* cy0, const double* cdl,

@@ -15,9 +15,10 @@
 //   upwind-y   (r'-1, c')    = lane j-1's result of step t-1   (__shfl_up)
 //   downwind-x (r',   c'+1)  = this lane's prefetch, loaded in step t
 //   downwind-y (r'+1, c')    = lane j+1's prefetch of step t  (__shfl_down)
-// Lane 0 reads its upwind row from memory (previous strip, final for this
-// sweep); the strip's last lane reads its downwind row from memory (next
-// strip, still old).  Every access is row-contiguous per lane.
+// Lane 0 streams its upwind row from memory (previous strip, final for this
+// sweep); the strip's last lane streams its downwind row (next strip, still
+// old).  Every access is row-contiguous per lane and issued one step before
+// its use.
 #pragma once
 #include "common.cuh"
 
@@ -37,12 +38,67 @@ struct Nb {
 //   load(iy, ix, last) -> Cell, load_nb(iy, ix) -> Cell,
 //   update(cur, iy, ix, xm, xp, ym, yp, last, l1, linf) -> V,
 //   store(iy, ix, v, last).
+// One step of the march.  cur = column c, nx1 = column c+1, ld = target of the
+// load of column c+1+LEAD.  Loads are issued LEAD steps before their first
+// use (as downwind-x / downwind-y neighbour) and buffer roles rotate
+// statically (the caller unrolls by LEAD+2), so no register copy ever waits
+// on a load in flight.
+template <int LEAD, class P, class Cell, class V, class X>
+__device__ __forceinline__ void systolic_step(P& p, const int t, const int lane, const int NR,
+                                              const int NC, const int rp, const bool act,
+                                              const int iy, const bool edge_up,
+                                              const bool edge_dn, const int iy_up,
+                                              const int iy_dn, const int xd, const int yd,
+                                              const bool last, Cell& cur, Cell& nx1, Cell& ld,
+                                              Cell& ucur, Cell& uld, Cell& dcur, Cell& dld,
+                                              V& prev_v, X& prev_x, double& l1, double& linf) {
+    const int c = t - lane;
+    const bool valid = act && c >= 0 && c < NC;
+    const int c2 = c + 1 + LEAD;
+    if (act && c2 >= 0 && c2 < NC) {
+        const int ix2 = p.col(c2, xd);
+        ld = p.load(iy, ix2, last);
+        if (edge_up) uld = p.load_nb(iy_up, ix2);
+        if (edge_dn) dld = p.load_nb(iy_dn, ix2);
+    }
+    V up_v = __shfl_up_sync(FULL_MASK, prev_v, 1);
+    X up_x = __shfl_up_sync(FULL_MASK, prev_x, 1);
+    V dn_v = __shfl_down_sync(FULL_MASK, nx1.v, 1);
+    X dn_x = __shfl_down_sync(FULL_MASK, nx1.x, 1);
+    if (valid) {
+        const int ix = p.col(c, xd);
+        const bool has_up = rp > 0;
+        const bool has_dn = rp + 1 < NR;
+        if (edge_up) {
+            up_v = ucur.v;
+            up_x = ucur.x;
+        }
+        if (edge_dn) {
+            dn_v = dcur.v;
+            dn_x = dcur.x;
+        }
+        const Nb<V, X> upw_x{c > 0, prev_v, prev_x};
+        const Nb<V, X> dnw_x{c + 1 < NC, nx1.v, nx1.x};
+        const Nb<V, X> upw_y{has_up, up_v, up_x};
+        const Nb<V, X> dnw_y{has_dn, dn_v, dn_x};
+        const V nv = p.update(cur, iy, ix, xd > 0 ? upw_x : dnw_x, xd > 0 ? dnw_x : upw_x,
+                              yd > 0 ? upw_y : dnw_y, yd > 0 ? dnw_y : upw_y, last, l1, linf);
+        p.store(iy, ix, nv, last);
+        prev_v = nv;
+        prev_x = cur.x;
+    }
+}
+
+// P::kLead = how many steps ahead a lane loads its row (1 for the long
+// forward update, more for the short adjoint update).
 template <class P>
 __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd, const bool last,
                                                double& l1, double& linf) {
     using V = typename P::V;
     using X = typename P::X;
     using Cell = typename P::Cell;
+    constexpr int LEAD = P::kLead;
+    constexpr int NB = LEAD + 2;
     const int lane = threadIdx.x & 31;
     const int NR = p.nrows();
     const int NC = p.ncols();
@@ -51,52 +107,49 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         const bool act = rp < NR;
         const int nr_strip = min(32, NR - k0);
         const int iy = act ? p.row(rp, yd) : 0;
+        // strip-edge lanes also stream the neighbouring row of the adjacent
+        // strip, with the same lead as their own row
+        const bool edge_up = act && lane == 0 && rp > 0;
+        const bool edge_dn = act && lane == nr_strip - 1 && rp + 1 < NR;
+        const int iy_up = edge_up ? p.row(rp - 1, yd) : 0;
+        const int iy_dn = edge_dn ? p.row(rp + 1, yd) : 0;
         p.begin_row(iy, act);
-        Cell cur{}, nxt{};
-        if (act && lane == 0) cur = p.load(iy, p.col(0, xd), last);
+        Cell buf[NB], ub[NB], db[NB];
+        // columns c .. c+LEAD of step 0 (what earlier steps would have loaded)
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+            buf[q] = Cell{};
+            ub[q] = Cell{};
+            db[q] = Cell{};
+            const int cq = q - lane;
+            if (q <= LEAD && act && cq >= 0 && cq < NC) {
+                const int ixq = p.col(cq, xd);
+                buf[q] = p.load(iy, ixq, last);
+                if (edge_up) ub[q] = p.load_nb(iy_up, ixq);
+                if (edge_dn) db[q] = p.load_nb(iy_dn, ixq);
+            }
+        }
         V prev_v = V(0);
         X prev_x = X(0);
         const int nsteps = NC + nr_strip - 1;
-        for (int t = 0; t < nsteps; ++t) {
-            const int c = t - lane;
-            const bool valid = act && c >= 0 && c < NC;
-            const int cn = c + 1;
-            if (act && cn >= 0 && cn < NC) nxt = p.load(iy, p.col(cn, xd), last);
-            V up_v = __shfl_up_sync(FULL_MASK, prev_v, 1);
-            X up_x = __shfl_up_sync(FULL_MASK, prev_x, 1);
-            V dn_v = __shfl_down_sync(FULL_MASK, nxt.v, 1);
-            X dn_x = __shfl_down_sync(FULL_MASK, nxt.x, 1);
-            if (valid) {
-                const int ix = p.col(c, xd);
-                const bool has_up = rp > 0;
-                const bool has_dn = rp + 1 < NR;
-                if (lane == 0 && has_up) {
-                    const Cell nb = p.load_nb(p.row(rp - 1, yd), ix);
-                    up_v = nb.v;
-                    up_x = nb.x;
-                }
-                if (lane == nr_strip - 1 && has_dn) {
-                    const Cell nb = p.load_nb(p.row(rp + 1, yd), ix);
-                    dn_v = nb.v;
-                    dn_x = nb.x;
-                }
-                const Nb<V, X> upw_x{c > 0, prev_v, prev_x};
-                const Nb<V, X> dnw_x{c + 1 < NC, nxt.v, nxt.x};
-                const Nb<V, X> upw_y{has_up, up_v, up_x};
-                const Nb<V, X> dnw_y{has_dn, dn_v, dn_x};
-                const V nv = p.update(cur, iy, ix,
-                                      xd > 0 ? upw_x : dnw_x, xd > 0 ? dnw_x : upw_x,
-                                      yd > 0 ? upw_y : dnw_y, yd > 0 ? dnw_y : upw_y,
-                                      last, l1, linf);
-                p.store(iy, ix, nv, last);
-                prev_v = nv;
-                prev_x = cur.x;
+        for (int t = 0; t < nsteps; t += NB) {
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+                if (t + i < nsteps)
+                    systolic_step<LEAD>(p, t + i, lane, NR, NC, rp, act, iy, edge_up, edge_dn,
+                                        iy_up, iy_dn, xd, yd, last, buf[i % NB],
+                                        buf[(i + 1) % NB], buf[(i + 1 + LEAD) % NB], ub[i % NB],
+                                        ub[(i + 1 + LEAD) % NB], db[i % NB],
+                                        db[(i + 1 + LEAD) % NB], prev_v, prev_x, l1, linf);
             }
-            cur = nxt;
         }
         __syncwarp();
     }
 }
+
+// The four sweep directions of src/eikonal_solver.cpp:137-140 (and :466-469).
+__device__ __forceinline__ int sweep_xd(int s) { return s < 2 ? 1 : -1; }
+__device__ __forceinline__ int sweep_yd(int s) { return (s & 1) ? -1 : 1; }
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
