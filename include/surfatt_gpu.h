@@ -124,6 +124,42 @@ int sa_forward_for_events(sa_ctx* ctx, int precision, int nx, int ny, int nper,
  * forward T and the masked adjoint field of the next sa_plan_forward_adjoint. */
 int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out);
 
+
+/* ---- surfker:: and preproc::combine_kernels (device arrays) --------------- */
+
+/* Replaces the column loop of SurfGrid::fwdsurf (reference
+ * src/surf_grid.cpp:194-245), i.e. build_disp_req (src/surfdisp.cpp:60-108)
+ * with the Brocher Vp/rho relations and surfker::surfdisp -> surfdisp96_c
+ * (src/surfdisp.cpp:428-462, src/surfker/surfdisp96.f:57-373), spherical
+ * earth (IFLSPH = 1), fundamental mode.  One thread per column.
+ *   zgrid [nz] (host), periods [nper] (host, nper <= 64), nz + 1 <= 64
+ *   vs3d  (nx, ny, nz) row-major (device)
+ *   svel  [nper][ny][nx] (device out); status [ny][nx] (device, may be NULL):
+ *         1 where the root search failed (the Fortran's `stop`). */
+int sa_surfdisp_columns(sa_ctx* ctx, int nx, int ny, int nz, const double* zgrid,
+                        const double* vs3d, int nper, const double* periods, int iwave, int igr,
+                        double* svel, int* status, void* stream);
+
+/* Replaces the column loop of SurfGrid::compute_dispersion_kernel for phase
+ * velocity (src/surf_grid.cpp:247-305) through surfker::depthkernelHTI1d
+ * (src/surfdisp.cpp:481-547) and sregn96_hti_c (src/surfker/sregn96.f90:1745-1849).
+ * One thread per (column, period).
+ *   cp [nper][ny][nx] Rayleigh phase velocities from sa_surfdisp_columns(igr = 0)
+ *   sen_vs, sen_vp, sen_rho (nx, ny, nz, nper) row-major (device out). */
+int sa_depthkernel_columns(sa_ctx* ctx, int nx, int ny, int nz, const double* zgrid,
+                           const double* vs3d, int nper, const double* periods,
+                           const double* cp, double* sen_vs, double* sen_vp, double* sen_rho,
+                           void* stream);
+
+/* Replaces preproc::combine_kernels, vs-only parametrisation
+ * (src/preproc.cpp:276-304): ker_vs(ix,iy,k) = -sum_iper adj_s(iper,ix,iy) *
+ * (sen_vs + sen_vp*dVp/dVs + sen_rho*drho/dVp*dVp/dVs), periods in order.
+ *   adj_s [nper][ny][nx]; vs3d, vp3d, ker_vs (nx, ny, nz); sen_* (nx, ny, nz, nper). */
+int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper, const double* adj_s,
+                          const double* vs3d, const double* vp3d, const double* sen_vs,
+                          const double* sen_vp, const double* sen_rho, double* ker_vs,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

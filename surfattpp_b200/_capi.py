@@ -24,6 +24,7 @@ EXPORTED = (
     "sa_eik_fwd_field", "sa_eik_adj_field", "sa_mask_uniform_grid",
     "sa_plan_create", "sa_plan_destroy", "sa_plan_set_graph", "sa_plan_forward_adjoint",
     "sa_forward_for_events", "sa_plan_debug_fields",
+    "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
 )
 
 
@@ -72,10 +73,9 @@ def lib():
     L.sa_forward_for_events.argtypes = [_vp, i, i, i, i, _dp, _dp, _dp, _vp, _vp, _vp, i, _dp,
                                         _dp, _ip, _ip, _ip, i, _dp, _dp, _dp, _dp, i, _dp, _dp,
                                         C.POINTER(d), _ip, _ip]
-    if hasattr(L, "sa_surfdisp_batch"):
-        L.sa_surfdisp_batch.argtypes = [_vp] * 2 + [i] * 4 + [_vp] * 4 + [i] * 4 + [_vp] * 3
-        L.sa_depthkernel_batch.argtypes = [_vp] * 2 + [i] * 3 + [_vp] * 7 + [_vp]
-        L.sa_combine_kernels_vs.argtypes = [_vp] + [i] * 4 + [_vp] * 7 + [_vp]
+    L.sa_surfdisp_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, i, i, _vp, _vp, _vp]
+    L.sa_depthkernel_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, _vp, _vp, _vp, _vp, _vp]
+    L.sa_combine_kernels_vs.argtypes = [_vp, i, i, i, i] + [_vp] * 7 + [_vp]
     _lib = L
     return L
 

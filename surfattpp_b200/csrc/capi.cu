@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -707,4 +708,107 @@ extern "C" int sa_eik_adj_field(sa_ctx* ctx, int precision, int nx, int ny, cons
                                 const double* source_adj, double* Ta_out, int* niter) {
     return single_solve(ctx, precision, nx, ny, xx_deg, yy_deg, spha, sphb, sphc, T, 0.0, 0.0,
                         nr, xrec_deg, yrec_deg, source_adj, true, Ta_out, niter);
+}
+
+// ---------------------------------------------------------------------------
+// Dispersion, depth kernels and kernel combination
+// ---------------------------------------------------------------------------
+namespace {
+struct LayerConstCache {
+    int nz = -1;
+    std::vector<double> z;
+    DArr<unsigned char> dev;
+};
+thread_local LayerConstCache g_lc;
+
+const void* layer_const_dev(sa_ctx* ctx, int nz, const double* zgrid, int* rc) {
+    *rc = SA_OK;
+    if (g_lc.nz == nz && std::equal(g_lc.z.begin(), g_lc.z.end(), zgrid)) return g_lc.dev.p;
+    std::vector<unsigned char> h(layer_const_bytes());
+    if (build_layer_const(nz, zgrid, h.data()) != 0) {
+        *rc = fail(ctx, SA_ERR_ARG, "nz + 1 exceeds the supported layer count (64)");
+        return nullptr;
+    }
+    cudaError_t e = g_lc.dev.upload(h.data(), h.size(), ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        *rc = fail(ctx, SA_ERR_CUDA, cudaGetErrorString(e));
+        return nullptr;
+    }
+    g_lc.nz = nz;
+    g_lc.z.assign(zgrid, zgrid + nz);
+    return g_lc.dev.p;
+}
+
+struct PeriodCache {
+    std::vector<double> p;
+    DArr<double> dev;
+};
+thread_local PeriodCache g_pc;
+
+const double* periods_dev(sa_ctx* ctx, int nper, const double* periods, int* rc) {
+    *rc = SA_OK;
+    if ((int)g_pc.p.size() == nper && std::equal(g_pc.p.begin(), g_pc.p.end(), periods))
+        return g_pc.dev.p;
+    cudaError_t e = g_pc.dev.upload(periods, nper, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        *rc = fail(ctx, SA_ERR_CUDA, cudaGetErrorString(e));
+        return nullptr;
+    }
+    g_pc.p.assign(periods, periods + nper);
+    return g_pc.dev.p;
+}
+}  // namespace
+
+extern "C" int sa_surfdisp_columns(sa_ctx* ctx, int nx, int ny, int nz, const double* zgrid,
+                                   const double* vs3d, int nper, const double* periods,
+                                   int iwave, int igr, double* svel, int* status, void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 1 || ny < 1 || nz < 2 || nper < 1 || nper > 64 || !zgrid || !periods || !vs3d || !svel)
+        return fail(ctx, SA_ERR_ARG, "sa_surfdisp_columns: bad sizes or null pointers");
+    if (iwave != 1 && iwave != 2)
+        return fail(ctx, SA_ERR_ARG, "iwave must be 1 (Love) or 2 (Rayleigh)");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    const void* L = layer_const_dev(ctx, nz, zgrid, &rc);
+    if (rc) return rc;
+    const double* p = periods_dev(ctx, nper, periods, &rc);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, p, 1, iwave, igr, L, svel, status, st));
+    return SA_OK;
+}
+
+extern "C" int sa_depthkernel_columns(sa_ctx* ctx, int nx, int ny, int nz, const double* zgrid,
+                                      const double* vs3d, int nper, const double* periods,
+                                      const double* cp, double* sen_vs, double* sen_vp,
+                                      double* sen_rho, void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 1 || ny < 1 || nz < 2 || nper < 1 || nper > 64 || !zgrid || !periods || !vs3d ||
+        !cp || !sen_vs || !sen_vp || !sen_rho)
+        return fail(ctx, SA_ERR_ARG, "sa_depthkernel_columns: bad sizes or null pointers");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    const void* L = layer_const_dev(ctx, nz, zgrid, &rc);
+    if (rc) return rc;
+    const double* p = periods_dev(ctx, nper, periods, &rc);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, p, cp, L, sen_vs, sen_vp, sen_rho, st));
+    return SA_OK;
+}
+
+extern "C" int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper,
+                                     const double* adj_s, const double* vs3d, const double* vp3d,
+                                     const double* sen_vs, const double* sen_vp,
+                                     const double* sen_rho, double* ker_vs, void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 1 || ny < 1 || nz < 1 || nper < 1 || !adj_s || !vs3d || !vp3d || !sen_vs ||
+        !sen_vp || !sen_rho || !ker_vs)
+        return fail(ctx, SA_ERR_ARG, "sa_combine_kernels_vs: bad sizes or null pointers");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    SA_CUDA(launch_combine_vs(nx, ny, nz, nper, adj_s, vs3d, vp3d, sen_vs, sen_vp, sen_rho, ker_vs, st));
+    return SA_OK;
 }

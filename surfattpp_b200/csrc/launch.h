@@ -66,3 +66,20 @@ namespace sa {
 cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStream_t st);
 cudaError_t launch_fold_status(int ne, const int* status, int* worst, cudaStream_t st);
 }  // namespace sa
+
+namespace sa {
+// surfker.cu
+size_t layer_const_bytes();
+int build_layer_const(int nz, const double* zgrid, void* out);
+cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, int nper,
+                                    const double* periods, int iflsph, int iwave, int igr,
+                                    const void* layer_const, double* svel, int* status,
+                                    cudaStream_t st);
+cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int nper,
+                               const double* periods, const double* cp, const void* layer_const,
+                               double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st);
+cudaError_t launch_combine_vs(int nx, int ny, int nz, int nper, const double* adj_s,
+                              const double* vs3d, const double* vp3d, const double* sen_vs,
+                              const double* sen_vp, const double* sen_rho, double* ker_vs,
+                              cudaStream_t st);
+}  // namespace sa
