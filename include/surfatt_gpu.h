@@ -160,6 +160,26 @@ int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper, const d
                           const double* sen_vp, const double* sen_rho, double* ker_vs,
                           void* stream);
 
+/* ---- allocation-free entry point ------------------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they call in (inside another framework's allocator or memory
+ * pool, hosts that forbid cudaMalloc after start-up, fully reserved device
+ * memory): one eikonal::FSM_UW_PS_lonlat_2d solve in FP64 with every
+ * intermediate in a fixed 64 MiB device array that each GPU loading this
+ * library keeps until exit (grids up to ~460,000 cells; larger ones return
+ * SA_ERR_ARG with a message on stderr).  All array arguments are DEVICE
+ * pointers: xx_deg [nx], yy_deg [ny], spha/sphb/sphc/fun/T_out [nx*ny];
+ * niter and status (may be NULL) are single device ints.  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy stream) after a small synchronous
+ * read of the first two grid coordinates.  Calls share the array: calls that
+ * overlap on the GPU race and must be serialised.  The first call on a device
+ * looks up the array's address; make it before any stream capture. */
+int sa_eik_fwd_field_noalloc(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                             const double* spha, const double* sphb, const double* sphc,
+                             const double* fun, double x0_deg, double y0_deg, double* T_out,
+                             int* niter, int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

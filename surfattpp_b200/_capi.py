@@ -25,6 +25,7 @@ EXPORTED = (
     "sa_plan_create", "sa_plan_destroy", "sa_plan_set_graph", "sa_plan_forward_adjoint",
     "sa_forward_for_events", "sa_plan_debug_fields",
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
+    "sa_eik_fwd_field_noalloc",
 )
 
 
@@ -76,6 +77,7 @@ def lib():
     L.sa_surfdisp_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, i, i, _vp, _vp, _vp]
     L.sa_depthkernel_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, _vp, _vp, _vp, _vp, _vp]
     L.sa_combine_kernels_vs.argtypes = [_vp, i, i, i, i] + [_vp] * 7 + [_vp]
+    L.sa_eik_fwd_field_noalloc.argtypes = [i, i] + [_vp] * 6 + [d, d] + [_vp] * 4
     _lib = L
     return L
 
