@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--nper", type=int, default=20)
     p.add_argument("--n", type=int, default=301)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the misfit-gradient and plain-FP64 side measurements")
     return p.parse_args()
 
 
@@ -118,6 +120,14 @@ class Clocks:
                 "samples": len(self.rows)}
 
 
+# DRAM bytes moved per algorithmic byte by batch_kernel<float>, from
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the same
+# kernel on the 151x151 / 3000-event case (82.504 GB moved for 73.420 GB of
+# algorithmic bytes; profiles/batch_kernel_fp32_c3_151x151_full.md).  Traffic
+# scales with cell updates, so a full launch moves algorithmic x this ratio.
+TRAFFIC_PER_ALGO_BYTE = {"fp32": 82.503724e9 / 73.419606e9}
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -180,6 +190,72 @@ def run_reference(a):
     return 0
 
 
+def _event_ms(stream, fn, steps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def misfit_gradient_timing(a, w, plan, tt, wt, dev, stream):
+    """One misfit-gradient evaluation (Inversion::run_forward_adjoint up to
+    combine_kernels) on the workload's 3-D model: wall time on the device per
+    iteration, plus each stage run alone on the same stream."""
+    import torch
+    from surfattpp_b200 import inversion, surfker
+    cs = stream.cuda_stream
+    g = inversion.MisfitGradient(plan, w.zgrid, w.periods)
+    vs = torch.as_tensor(np.ascontiguousarray(w.vs3d), device=dev)
+    out = g.run(vs, tt, wt, stream=cs)
+    for _ in range(2):
+        g.run(vs, tt, wt, out=out, stream=cs)
+    torch.cuda.synchronize()
+    steps = max(1, min(a.steps, 3))
+    ms = _event_ms(stream, lambda: g.run(vs, tt, wt, out=out, stream=cs), steps)
+    status = int(out["status"][0])
+    sv = out["svel"]
+    t_disp = _event_ms(stream, lambda: surfker.fwdsurf(w.zgrid, vs, w.periods, stream=cs,
+                                                        check=False), steps)
+    t_sen = _event_ms(stream, lambda: surfker.depthkernel_hti(w.zgrid, vs, w.periods, sv,
+                                                              stream=cs), steps)
+    sen = g.sen(stream=cs)
+    t_comb = _event_ms(stream, lambda: surfker.combine_kernels_vs(out["adj_s"], vs, None, *sen,
+                                                                 stream=cs), steps)
+    o2 = plan.run(sv, tt, wt, stream=cs)
+    t_batch = _event_ms(stream, lambda: plan.run(sv, tt, wt, out=o2, stream=cs), steps)
+    g.close()
+    del sen
+    return {"s_per_iter": ms * 1e-3, "unit": "s/iter", "steps": steps, "status": status,
+            "model": f"{w.nx}x{w.ny}x{w.nz} vs3d, {w.nper} Rayleigh phase periods, "
+                     f"{w.n_events} events",
+            "stages_ms_alone": {"fwdsurf": t_disp, "depthkernel": t_sen,
+                                "forward_adjoint": t_batch, "combine": t_comb},
+            "note": "depth kernels run on a second stream concurrently with the event batch"}
+
+
+def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx):
+    """The same solves with the FP64 parity path (the reference's arithmetic)."""
+    from surfattpp_b200 import preproc
+    cs = stream.cuda_stream
+    ev = w.events()
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision="fp64", ctx=ctx, graph=True)
+    out = plan.run(sv, tt, wt, stream=cs)
+    plan.run(sv, tt, wt, out=out, stream=cs)
+    import torch
+    torch.cuda.synchronize()
+    steps = max(1, min(a.steps, 2))
+    ms = _event_ms(stream, lambda: plan.run(sv, tt, wt, out=out, stream=cs), steps)
+    plan.close()
+    return {"value": w.n_events / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "dtype": "f64"}
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -240,6 +316,17 @@ def main():
         dist.barrier()
     status = int(out["status"][:w.n_events].max())
 
+    # the dominant kernel alone: CUDA events around each batch launch (same
+    # stream, launched without the graph), one step at a time
+    plan.kernel_timing(True)
+    kms = []
+    for _ in range(a.steps):
+        step()
+        kms.append(plan.kernel_ms())
+    plan.kernel_timing(False)
+    torch.cuda.synchronize()
+    kernel_ms = float(np.mean(kms))
+
     # end to end through the public API: pinned host inputs in, adj_s + misfit out
     h_sv = torch.from_numpy(svel).pin_memory()
     h_tt = torch.from_numpy(np.ascontiguousarray(ev["tt_obs"])).pin_memory()
@@ -274,11 +361,16 @@ def main():
     h2d = h_sv.numel() * 8 + h_tt.numel() * 8 + h_wt.numel() * 8
     d2h = h_adj.numel() * 8 + 8
 
+    extra = {}
+    if world == 1 and not a.no_extras:
+        extra["misfit_gradient"] = misfit_gradient_timing(a, w, plan, tt, wt, dev, stream)
+        extra["fp64_plain"] = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx)
+
     if rank == 0:
         peak, peak_kind = peaks()
         bpu_f, bpu_a = (36, 20) if a.precision == "fp32" else (72, 40)
         algo, nf, na = algorithmic_bytes(w.nx, w.ny, fwd_iters, adj_iters, bpu_f, bpu_a)
-        achieved = algo / (ms * 1e-3) / 1e9
+        achieved = algo / (kernel_ms * 1e-3) / 1e9
         total_events = w.n_events * world
         line = {
             "metric": METRIC, "value": total_events / (ms * 1e-3), "unit": UNIT,
@@ -292,13 +384,21 @@ def main():
             "gpu_launches": (5 if a.precision == "fp32" else 4) * a.steps,
             "cell_updates_per_s": (nf + na) / (ms * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": (algo * TRAFFIC_PER_ALGO_BYTE[a.precision]
+                                     if a.precision in TRAFFIC_PER_ALGO_BYTE else None),
+                         "traffic_source": "ncu dram bytes of the 151x151 capture, scaled "
+                                           "by cell updates",
+                         "kernel": "batch_kernel<%s>" % ("float" if a.precision == "fp32"
+                                                         else "double"),
+                         "kernel_ms": kernel_ms, "algorithmic_bytes": algo,
                          "peak_kind": peak_kind,
                          "note": "algorithmic bytes: 36 B per forward / 20 B per adjoint "
                                  "cell update (FP32), x2 for FP64"},
             "clocks": clk.summary(),
             "status": status,
         }
+        line.update(extra)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a, w, svel)
         print(json.dumps(line), flush=True)

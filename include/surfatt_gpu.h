@@ -120,6 +120,13 @@ int sa_forward_for_events(sa_ctx* ctx, int precision, int nx, int ny, int nper,
                           int calc_adj, double* syn, double* adj_s, double* chi, int* fwd_iters,
                           int* adj_iters);
 
+/* Timing of the batch kernel (no counterpart in the reference).  While
+ * enabled, sa_plan_forward_adjoint launches without the graph and records CUDA
+ * events on its stream around the batched forward/adjoint kernel;
+ * sa_plan_kernel_ms waits for the last of them and returns its duration. */
+int sa_plan_kernel_timing(sa_plan* plan, int enable);
+int sa_plan_kernel_ms(sa_plan* plan, float* ms);
+
 /* Full-field outputs for testing (device arrays [ne][ny][nx], may be NULL):
  * forward T and the masked adjoint field of the next sa_plan_forward_adjoint. */
 int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out);
@@ -154,11 +161,45 @@ int sa_depthkernel_columns(sa_ctx* ctx, int nx, int ny, int nz, const double* zg
 /* Replaces preproc::combine_kernels, vs-only parametrisation
  * (src/preproc.cpp:276-304): ker_vs(ix,iy,k) = -sum_iper adj_s(iper,ix,iy) *
  * (sen_vs + sen_vp*dVp/dVs + sen_rho*drho/dVp*dVp/dVs), periods in order.
- *   adj_s [nper][ny][nx]; vs3d, vp3d, ker_vs (nx, ny, nz); sen_* (nx, ny, nz, nper). */
+ *   adj_s [nper][ny][nx]; vs3d, vp3d, ker_vs (nx, ny, nz); sen_* (nx, ny, nz, nper).
+ *   vp3d may be NULL: vp = vs2vp(vs3d) (Brocher, include/utils.h:237-245). */
 int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper, const double* adj_s,
                           const double* vs3d, const double* vp3d, const double* sen_vs,
                           const double* sen_vp, const double* sen_rho, double* ker_vs,
                           void* stream);
+
+/* ---- one misfit-gradient evaluation ---------------------------------------- */
+
+/* Replaces one data type's pass of Inversion::run_forward_adjoint(true)
+ * (reference src/inversion.cpp:245-276) up to and including combine_kernels,
+ * for Rayleigh phase-velocity data and the vs-only parametrisation:
+ * SurfGrid::fwdsurf (src/surf_grid.cpp:194-245), compute_dispersion_kernel
+ * (:247-305), preproc::forward_for_event (src/preproc.cpp:71-148) over the
+ * plan's events, combine_kernels (:276-304).  Kernel preconditioning and
+ * smoothing (src/postproc.cpp) are not part of it.
+ * sa_grad_create binds an existing plan (its grid, events and precision) to a
+ * depth grid zgrid[nz] and the plan's nper periods[] (host arrays) and keeps
+ * the depth-kernel arrays (3 x nx*ny*nz*nper doubles) on the device. */
+typedef struct sa_grad sa_grad;
+int sa_grad_create(sa_plan* plan, int nz, const double* zgrid, const double* periods,
+                   sa_grad** out);
+void sa_grad_destroy(sa_grad* grad);
+
+/* Device arrays: vs3d, vp3d (NULL = Brocher vs2vp(vs3d), as the model keeps it
+ * for vs-only inversions), ker_vs: (nx, ny, nz) row-major; tt_obs, weight:
+ * [npair]; chi: 1 double.  svel_out and adj_s_out ([nper][ny][nx], may be
+ * NULL) receive the phase velocities and the accumulated adjoint kernels;
+ * status (1 device int, may be NULL) receives SA_ERR_NOROOT when a column's
+ * root search failed, else the worst event status.  Enqueued on `stream`
+ * (NULL = the context's stream); the depth kernels run on an internal stream
+ * concurrently with the event batch. */
+int sa_grad_run(sa_grad* grad, const double* vs3d, const double* vp3d, const double* tt_obs,
+                const double* weight, double* ker_vs, double* chi, double* svel_out,
+                double* adj_s_out, int* status, void* stream);
+
+/* Copies the last run's depth kernels into device arrays sen_vs, sen_vp,
+ * sen_rho ((nx, ny, nz, nper) row-major; any may be NULL), on `stream`. */
+int sa_grad_sen(sa_grad* grad, double* sen_vs, double* sen_vp, double* sen_rho, void* stream);
 
 /* ---- allocation-free entry point ------------------------------------------ */
 

@@ -23,9 +23,10 @@ EXPORTED = (
     "sa_ctx_create", "sa_ctx_destroy", "sa_ctx_error", "sa_version",
     "sa_eik_fwd_field", "sa_eik_adj_field", "sa_mask_uniform_grid",
     "sa_plan_create", "sa_plan_destroy", "sa_plan_set_graph", "sa_plan_forward_adjoint",
-    "sa_forward_for_events", "sa_plan_debug_fields",
+    "sa_forward_for_events", "sa_plan_debug_fields", "sa_plan_kernel_timing", "sa_plan_kernel_ms",
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
     "sa_eik_fwd_field_noalloc",
+    "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen",
 )
 
 
@@ -71,6 +72,8 @@ def lib():
     L.sa_plan_set_graph.argtypes = [_vp, i]
     L.sa_plan_forward_adjoint.argtypes = [_vp] + [_vp] * 6 + [i] + [_vp] * 6 + [_vp]
     L.sa_plan_debug_fields.argtypes = [_vp, _vp, _vp]
+    L.sa_plan_kernel_timing.argtypes = [_vp, i]
+    L.sa_plan_kernel_ms.argtypes = [_vp, C.POINTER(C.c_float)]
     L.sa_forward_for_events.argtypes = [_vp, i, i, i, i, _dp, _dp, _dp, _vp, _vp, _vp, i, _dp,
                                         _dp, _ip, _ip, _ip, i, _dp, _dp, _dp, _dp, i, _dp, _dp,
                                         C.POINTER(d), _ip, _ip]
@@ -78,6 +81,10 @@ def lib():
     L.sa_depthkernel_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, _vp, _vp, _vp, _vp, _vp]
     L.sa_combine_kernels_vs.argtypes = [_vp, i, i, i, i] + [_vp] * 7 + [_vp]
     L.sa_eik_fwd_field_noalloc.argtypes = [i, i] + [_vp] * 6 + [d, d] + [_vp] * 4
+    L.sa_grad_create.argtypes = [_vp, i, _dp, _dp, C.POINTER(_vp)]
+    L.sa_grad_destroy.argtypes = [_vp]
+    L.sa_grad_run.argtypes = [_vp] + [_vp] * 9 + [_vp]
+    L.sa_grad_sen.argtypes = [_vp] * 5
     _lib = L
     return L
 

@@ -20,18 +20,11 @@
 
 using namespace sa;
 
-struct sa_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-};
+struct sa_ctx;
 
 namespace {
 
-int fail(sa_ctx* ctx, int code, const std::string& msg) {
-    if (ctx) ctx->err = msg;
-    return code;
-}
+int fail(sa_ctx* ctx, int code, const std::string& msg);
 
 #define SA_CUDA(call)                                                                      \
     do {                                                                                   \
@@ -67,6 +60,33 @@ struct DArr {
         return e;
     }
 };
+
+// Device copies of the per-layer flattening constants and of the period list,
+// rebuilt when the depth grid or the periods change.
+struct LayerConstCache {
+    int nz = -1;
+    std::vector<double> z;
+    DArr<unsigned char> dev;
+};
+struct PeriodCache {
+    std::vector<double> p;
+    DArr<double> dev;
+};
+}  // namespace
+
+struct sa_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    LayerConstCache lc;
+    PeriodCache pc;
+};
+
+namespace {
+int fail(sa_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
 
 struct GraphKey {
     const void* ptr[17];
@@ -104,8 +124,12 @@ struct sa_plan {
     bool have_graph = false;
     GraphKey key{};
     cudaGraphExec_t gexec = nullptr;
+    bool timing = false;                    // events around the batch launch (no graph)
+    cudaEvent_t tk0 = nullptr, tk1 = nullptr;
     ~sa_plan() {
         if (gexec) cudaGraphExecDestroy(gexec);
+        if (tk0) cudaEventDestroy(tk0);
+        if (tk1) cudaEventDestroy(tk1);
     }
 };
 
@@ -435,7 +459,9 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
     if (calc_adj && adj_s)
         SA_CUDA(cudaMemsetAsync(adj_s, 0, (size_t)P->nx * P->ny * P->nper * sizeof(double), st));
     if (P->ne > 0) {
+        if (P->timing) SA_CUDA(cudaEventRecord(P->tk0, st));
         SA_CUDA(P->prec == SA_FP64 ? launch_batch64(d, st) : launch_batch32(d, st));
+        if (P->timing) SA_CUDA(cudaEventRecord(P->tk1, st));
         if (calc_adj && chi) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi, st));
         SA_CUDA(launch_fold_status(P->ne, d.out.status, P->worst.p, st));
     } else {
@@ -484,6 +510,27 @@ extern "C" int sa_plan_set_graph(sa_plan* plan, int enable) {
     return SA_OK;
 }
 
+extern "C" int sa_plan_kernel_timing(sa_plan* P, int enable) {
+    if (!P) return SA_ERR_ARG;
+    sa_ctx* ctx = P->ctx;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    if (enable && !P->tk0) {
+        SA_CUDA(cudaEventCreate(&P->tk0));
+        SA_CUDA(cudaEventCreate(&P->tk1));
+    }
+    P->timing = enable != 0;
+    return SA_OK;
+}
+
+extern "C" int sa_plan_kernel_ms(sa_plan* P, float* ms) {
+    if (!P || !ms) return SA_ERR_ARG;
+    sa_ctx* ctx = P->ctx;
+    if (!P->tk0) return fail(ctx, SA_ERR_ARG, "kernel timing is not enabled");
+    SA_CUDA(cudaEventSynchronize(P->tk1));
+    SA_CUDA(cudaEventElapsedTime(ms, P->tk0, P->tk1));
+    return SA_OK;
+}
+
 extern "C" int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out) {
     if (!plan) return SA_ERR_ARG;
     plan->dbg_T = T_out;
@@ -505,7 +552,7 @@ extern "C" int sa_plan_forward_adjoint(sa_plan* P, const double* svel, const dou
     if (P->npair > 0 && (!tt_obs || !weight)) return fail(ctx, SA_ERR_ARG, "tt_obs/weight");
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-    if (!P->use_graph)
+    if (!P->use_graph || P->timing)
         return plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj, syn, adj_s, chi,
                             fwd_iters, adj_iters, status, st);
     GraphKey k{};
@@ -714,15 +761,9 @@ extern "C" int sa_eik_adj_field(sa_ctx* ctx, int precision, int nx, int ny, cons
 // Dispersion, depth kernels and kernel combination
 // ---------------------------------------------------------------------------
 namespace {
-struct LayerConstCache {
-    int nz = -1;
-    std::vector<double> z;
-    DArr<unsigned char> dev;
-};
-thread_local LayerConstCache g_lc;
-
 const void* layer_const_dev(sa_ctx* ctx, int nz, const double* zgrid, int* rc) {
     *rc = SA_OK;
+    LayerConstCache& g_lc = ctx->lc;
     if (g_lc.nz == nz && std::equal(g_lc.z.begin(), g_lc.z.end(), zgrid)) return g_lc.dev.p;
     std::vector<unsigned char> h(layer_const_bytes());
     if (build_layer_const(nz, zgrid, h.data()) != 0) {
@@ -740,14 +781,9 @@ const void* layer_const_dev(sa_ctx* ctx, int nz, const double* zgrid, int* rc) {
     return g_lc.dev.p;
 }
 
-struct PeriodCache {
-    std::vector<double> p;
-    DArr<double> dev;
-};
-thread_local PeriodCache g_pc;
-
 const double* periods_dev(sa_ctx* ctx, int nper, const double* periods, int* rc) {
     *rc = SA_OK;
+    PeriodCache& g_pc = ctx->pc;
     if ((int)g_pc.p.size() == nper && std::equal(g_pc.p.begin(), g_pc.p.end(), periods))
         return g_pc.dev.p;
     cudaError_t e = g_pc.dev.upload(periods, nper, ctx->stream);
@@ -804,11 +840,121 @@ extern "C" int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int np
                                      const double* sen_vs, const double* sen_vp,
                                      const double* sen_rho, double* ker_vs, void* stream) {
     if (!ctx) return SA_ERR_ARG;
-    if (nx < 1 || ny < 1 || nz < 1 || nper < 1 || !adj_s || !vs3d || !vp3d || !sen_vs ||
+    if (nx < 1 || ny < 1 || nz < 1 || nper < 1 || !adj_s || !vs3d || !sen_vs ||
         !sen_vp || !sen_rho || !ker_vs)
         return fail(ctx, SA_ERR_ARG, "sa_combine_kernels_vs: bad sizes or null pointers");
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     SA_CUDA(launch_combine_vs(nx, ny, nz, nper, adj_s, vs3d, vp3d, sen_vs, sen_vp, sen_rho, ker_vs, st));
+    return SA_OK;
+}
+
+// ---- one misfit-gradient evaluation ------------------------------------------
+
+struct sa_grad {
+    sa_plan* plan = nullptr;
+    int nz = 0;
+    DArr<unsigned char> lc;
+    DArr<double> periods, svel, adj_s, sen_vs, sen_vp, sen_rho;
+    DArr<int> colst, worst;
+    cudaStream_t side = nullptr;
+    cudaEvent_t e_disp = nullptr, e_sen = nullptr;
+    ~sa_grad() {
+        if (e_disp) cudaEventDestroy(e_disp);
+        if (e_sen) cudaEventDestroy(e_sen);
+        if (side) cudaStreamDestroy(side);
+    }
+};
+
+extern "C" int sa_grad_create(sa_plan* plan, int nz, const double* zgrid, const double* periods,
+                              sa_grad** out) {
+    if (!plan || !out) return SA_ERR_ARG;
+    *out = nullptr;
+    sa_ctx* ctx = plan->ctx;
+    const int nper = plan->nper;
+    if (nz < 2 || nper > 64 || !zgrid || !periods)
+        return fail(ctx, SA_ERR_ARG, "sa_grad_create: nz >= 2, nper <= 64, zgrid and periods");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    std::vector<unsigned char> h(layer_const_bytes());
+    if (build_layer_const(nz, zgrid, h.data()) != 0)
+        return fail(ctx, SA_ERR_ARG, "nz + 1 exceeds the supported layer count (64)");
+    sa_grad* g = new sa_grad();
+    g->plan = plan;
+    g->nz = nz;
+    const size_t ncol = (size_t)plan->nx * plan->ny, n4 = ncol * nz * nper;
+    cudaError_t e = g->lc.upload(h.data(), h.size(), ctx->stream);
+    if (e == cudaSuccess) e = g->periods.upload(periods, nper, ctx->stream);
+    if (e == cudaSuccess) e = g->svel.alloc(ncol * nper);
+    if (e == cudaSuccess) e = g->adj_s.alloc(ncol * nper);
+    if (e == cudaSuccess) e = g->sen_vs.alloc(n4);
+    if (e == cudaSuccess) e = g->sen_vp.alloc(n4);
+    if (e == cudaSuccess) e = g->sen_rho.alloc(n4);
+    if (e == cudaSuccess) e = g->colst.alloc(ncol);
+    if (e == cudaSuccess) e = g->worst.alloc(1);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->e_disp, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->e_sen, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete g;
+        return fail(ctx, e == cudaErrorMemoryAllocation ? SA_ERR_NOMEM : SA_ERR_CUDA,
+                    std::string("sa_grad_create: ") + cudaGetErrorString(e));
+    }
+    *out = g;
+    return SA_OK;
+}
+
+extern "C" void sa_grad_destroy(sa_grad* g) {
+    if (!g) return;
+    cudaSetDevice(g->plan->ctx->device);
+    delete g;
+}
+
+extern "C" int sa_grad_run(sa_grad* g, const double* vs3d, const double* vp3d,
+                           const double* tt_obs, const double* weight, double* ker_vs,
+                           double* chi, double* svel_out, double* adj_s_out, int* status,
+                           void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (!vs3d || !ker_vs || !chi) return fail(ctx, SA_ERR_ARG, "vs3d, ker_vs and chi are required");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
+    double* svel = svel_out ? svel_out : g->svel.p;
+    double* adj_s = adj_s_out ? adj_s_out : g->adj_s.p;
+    // SurfGrid::fwdsurf (phase, Rayleigh, spherical earth)
+    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->periods.p, 1, 2, 0, g->lc.p, svel,
+                                    g->colst.p, st));
+    SA_CUDA(cudaEventRecord(g->e_disp, st));
+    // forward_for_event over every event (accumulates adj_s and the misfit)
+    int rc = sa_plan_forward_adjoint(P, svel, nullptr, nullptr, nullptr, tt_obs, weight, 1,
+                                     nullptr, adj_s, chi, nullptr, nullptr, nullptr, st);
+    if (rc) return rc;
+    // compute_dispersion_kernel on a second stream: it needs only vs3d and the
+    // phase velocities, so it runs while the event batch drains
+    SA_CUDA(cudaStreamWaitEvent(g->side, g->e_disp, 0));
+    SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p, g->sen_vs.p,
+                               g->sen_vp.p, g->sen_rho.p, g->side));
+    SA_CUDA(cudaEventRecord(g->e_sen, g->side));
+    SA_CUDA(cudaStreamWaitEvent(st, g->e_sen, 0));
+    // combine_kernels (vs-only parametrisation)
+    SA_CUDA(launch_combine_vs(nx, ny, nz, nper, adj_s, vs3d, vp3d, g->sen_vs.p, g->sen_vp.p,
+                              g->sen_rho.p, ker_vs, st));
+    SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
+    return SA_OK;
+}
+
+extern "C" int sa_grad_sen(sa_grad* g, double* sen_vs, double* sen_vp, double* sen_rho,
+                           void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_ctx* ctx = g->plan->ctx;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const size_t bytes = (size_t)g->plan->nx * g->plan->ny * g->nz * g->plan->nper * sizeof(double);
+    double* dst[3] = {sen_vs, sen_vp, sen_rho};
+    const double* src[3] = {g->sen_vs.p, g->sen_vp.p, g->sen_rho.p};
+    for (int i = 0; i < 3; ++i)
+        if (dst[i]) SA_CUDA(cudaMemcpyAsync(dst[i], src[i], bytes, cudaMemcpyDeviceToDevice, st));
     return SA_OK;
 }

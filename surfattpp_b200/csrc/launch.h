@@ -78,6 +78,8 @@ cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, 
 cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int nper,
                                const double* periods, const double* cp, const void* layer_const,
                                double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st);
+cudaError_t launch_grad_status(int ncol, const int* colst, const int* ev_worst, int* out,
+                               cudaStream_t st);
 cudaError_t launch_combine_vs(int nx, int ny, int nz, int nper, const double* adj_s,
                               const double* vs3d, const double* vp3d, const double* sen_vs,
                               const double* sen_vp, const double* sen_rho, double* ker_vs,

@@ -1327,7 +1327,9 @@ __global__ void combine_vs_kernel(int nx, int ny, int nz, int nper, const double
     const int col = (int)(i3 / nz);
     const int ix = col / ny, iy = col % ny;
     const double vs = vs3d[i3];
-    const double vp = vp3d[i3];
+    // vp3d NULL: vp = vs2vp(vs), as ModelGrid keeps it for vs-only
+    // parametrisations (src/model_grid.cpp:594-596)
+    const double vp = vp3d ? vp3d[i3] : sk::vs2vp(vs);
     const double dab = sk::dalpha_dbeta(vs);
     const double dra = sk::drho_dalpha(vp);
     double k = 0.0;

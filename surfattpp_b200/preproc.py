@@ -59,6 +59,16 @@ class ForwardAdjointPlan:
         except Exception:
             pass
 
+    def kernel_timing(self, enable=True):
+        """Record CUDA events around the batch kernel (runs without the graph)."""
+        _capi.check(self.ctx.h, _capi.lib().sa_plan_kernel_timing(self.h, int(bool(enable))))
+
+    def kernel_ms(self):
+        """Duration of the last batch kernel launch (waits for it)."""
+        ms = C.c_float(0.0)
+        _capi.check(self.ctx.h, _capi.lib().sa_plan_kernel_ms(self.h, C.byref(ms)))
+        return ms.value
+
     def debug_fields(self, T_out=None, Ta_out=None):
         _capi.lib().sa_plan_debug_fields(self.h, ptr(T_out), ptr(Ta_out))
 
