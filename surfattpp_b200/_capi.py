@@ -11,7 +11,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libsurfatt_gpu.so")
+# SURFATT_GPU_LIB selects another build of the same library (same C ABI).
+LIB_PATH = os.environ.get("SURFATT_GPU_LIB") or os.path.join(_HERE, "libsurfatt_gpu.so")
 
 SA_OK, SA_ERR_ARG, SA_ERR_CUDA, SA_ERR_NOCONV, SA_ERR_NOROOT, SA_ERR_NONFINITE, SA_ERR_NOMEM = range(7)
 SA_FP64, SA_FP32 = 0, 1

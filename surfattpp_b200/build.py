@@ -45,8 +45,14 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, force: bool = False, defines: list[str] | None = None,
+          out: str | None = None, build_dir: str | None = None) -> str:
+    """Compile every unit and link the library.  ``defines`` (``NAME=VALUE``
+    strings), ``out`` and ``build_dir`` build a variant next to the default."""
+    lib = out or LIB
+    bdir = build_dir or BUILD
+    dflags = [f"-D{d}" for d in (defines or [])]
+    os.makedirs(bdir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(INCLUDE, "surfatt_gpu.h"))
     objs = []
@@ -54,18 +60,18 @@ def build(verbose: bool = False, force: bool = False) -> str:
         src = os.path.join(CSRC, unit)
         if not os.path.exists(src):
             continue
-        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        obj = os.path.join(bdir, unit.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
+            cmd = [nvcc()] + ARCH + COMMON + dflags + flags + ["-c", src, "-o", obj]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd), file=sys.stderr)
             subprocess.run(cmd, check=True)
-    if force or _stale(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if force or _stale(lib, objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"]
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

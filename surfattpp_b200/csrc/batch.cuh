@@ -14,6 +14,14 @@
 
 #include <type_traits>
 
+// Resident 128-thread blocks per SM the register allocation is sized for.
+#ifndef SA_MINB64
+#define SA_MINB64 3
+#endif
+#ifndef SA_MINB32
+#define SA_MINB32 4
+#endif
+
 namespace sa {
 
 template <class S>
@@ -46,7 +54,7 @@ struct BatchArgs {
 // forward operands (PK) and the packed adjoint coefficients share one region:
 // the forward planes are dead once T is formed.
 struct SlotLayout {
-    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, total;
+    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, flags, total;
 };
 template <class S>
 __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
@@ -76,14 +84,16 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     L.Ta = take(n * sizeof(S));
     L.sadj = take(r * sizeof(double));
     L.syn = take(r * sizeof(double));
+    L.flags = take(n);   // sweep flags (systolic.cuh), forward then adjoint
     L.total = o;
     return L;
 }
 
 template <class S, bool ISO>
 __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo& si, int ip,
-                                            int src, S* tau, S* tst, Q4<S>* pk, double* T,
-                                            int& iters, int& status) {
+                                            int src, S* tau, S* tst, Q4<S>* pk,
+                                            unsigned char* flags, double* T, int& iters,
+                                            int& status) {
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
     const size_t n = (size_t)nx * ny;
@@ -118,6 +128,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     P.b_iso = B.b_iso;
     P.tau = tau;
     P.tau_start = tst;
+    P.flags = flags;
     P.fix_x0 = si.fix_x0;
     P.fix_x1 = si.fix_x1;
     P.yy = g.yy;
@@ -132,6 +143,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
         const S v = (fixed ? S(1) : S(10)) - off;
         tau[k] = v;
         tst[k] = v;
+        flags[k] = 1;
     }
     __syncwarp();
     iters = 0;
@@ -160,7 +172,8 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
 }
 
 template <class S, bool ISO>
-__global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batch_kernel(BatchArgs<S> B) {
+__global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? SA_MINB64 : SA_MINB32)
+batch_kernel(BatchArgs<S> B) {
     const int lane = threadIdx.x & 31;
     const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (slot >= B.sc.nslots) return;
@@ -176,10 +189,12 @@ __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batc
     double* P_sadj = reinterpret_cast<double*>(base + L.sadj);
     double* P_syn = reinterpret_cast<double*>(base + L.syn);
     Q4<S>* P_pk = reinterpret_cast<Q4<S>*>(base + L.PK);
+    unsigned char* P_fl = base + L.flags;
 
     for (;;) {
-        const unsigned int e = warp_next_event(B.sc.queue);
-        if (e >= (unsigned)B.ev.ne) break;
+        const unsigned int qi = warp_next_event(B.sc.queue);
+        if (qi >= (unsigned)B.ev.ne) break;
+        const unsigned int e = B.sc.order ? (unsigned)B.sc.order[qi] : qi;
         const int ip = B.ev.iper[e];
         const int r0 = B.ev.rec_ptr[e];
         const int nr = B.ev.rec_ptr[e + 1] - r0;
@@ -189,7 +204,8 @@ __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batc
 
         if (B.mode != MODE_ADJ_ONLY) {
             int iters = 0;
-            fwd_solve<S, ISO>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_T, iters, status);
+            fwd_solve<S, ISO>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_fl, P_T, iters,
+                              status);
             if (lane == 0 && B.out.fwd_iters) B.out.fwd_iters[e] = iters;
             if (B.out.T_out)
                 for (size_t k = lane; k < n; k += 32) B.out.T_out[(size_t)e * n + k] = P_T[k];
@@ -263,6 +279,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batc
                     const double v0 = interior ? 100.0 : 0.0;   // :446-449
                     P_Ta[k] = v0;
                     P_Tst[k] = v0;
+                    P_fl[k] = 1;
                 }
                 __syncwarp();
                 AdjPolicyExact Q;
@@ -274,6 +291,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batc
                 Q.dd = P_DD;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_Tst;
+                Q.flags = P_fl;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
@@ -332,6 +350,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batc
                     const float v0 = interior ? 100.f : 0.f;
                     P_Ta[k] = v0;
                     P_tst[k] = v0;
+                    P_fl[k] = 1;
                 }
                 __syncwarp();
                 AdjPolicyW32 Q;
@@ -342,6 +361,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? 3 : 4) batc
                 Q.vmax = 0.0;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_tst;
+                Q.flags = P_fl;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;

@@ -116,6 +116,12 @@ struct sa_plan {
     DArr<int> status_tmp, worst;
     DArr<unsigned char> scratch;
     DArr<unsigned int> queue;
+    // cost-ordered work queue: events sorted by the previous evaluation's
+    // sweep counts, longest first, so the persistent kernel's tail is short
+    DArr<int> fit, ait, order, ord_idx;
+    DArr<unsigned int> key_a, key_b;
+    DArr<unsigned char> sort_tmp;
+    size_t sort_bytes = 0;
     int nslots = 0;
     size_t slot_bytes = 0;
     double* dbg_T = nullptr;
@@ -342,6 +348,21 @@ int plan_events(sa_plan* P, int ne, const double* evlo, const double* evla, cons
     SA_CUDA(P->status_tmp.alloc(std::max(ne, 1)));
     SA_CUDA(P->worst.alloc(1));
     SA_CUDA(P->queue.alloc(1));
+    {
+        const size_t ne1 = (size_t)std::max(ne, 1);
+        SA_CUDA(P->fit.alloc(ne1));
+        SA_CUDA(P->ait.alloc(ne1));
+        SA_CUDA(cudaMemsetAsync(P->fit.p, 0, ne1 * sizeof(int), st));
+        SA_CUDA(cudaMemsetAsync(P->ait.p, 0, ne1 * sizeof(int), st));
+        std::vector<int> iota(ne1);
+        for (size_t i = 0; i < ne1; i++) iota[i] = (int)i;
+        SA_CUDA(P->order.upload(iota.data(), ne1, st));
+        SA_CUDA(P->ord_idx.alloc(ne1));
+        SA_CUDA(P->key_a.alloc(ne1));
+        SA_CUDA(P->key_b.alloc(ne1));
+        P->sort_bytes = ne > 0 ? sort_events_temp_bytes(ne) : 0;
+        SA_CUDA(P->sort_tmp.alloc(std::max<size_t>(P->sort_bytes, 1)));
+    }
     // scratch slots: one per resident warp, bounded by events and free memory
     const int maxs = P->prec == SA_FP64 ? batch64_max_slots(ctx->device) : batch32_max_slots(ctx->device);
     P->slot_bytes = P->prec == SA_FP64 ? batch64_slot_bytes(nx, ny, P->maxr)
@@ -449,8 +470,9 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
     d.out.syn = syn;
     d.out.chi_ev = (calc_adj && chi) ? P->chi_ev.p : nullptr;
     d.out.adj_s = calc_adj ? adj_s : nullptr;
-    d.out.fwd_iters = fwd_iters;
-    d.out.adj_iters = adj_iters;
+    d.out.fwd_iters = P->fit.p;
+    d.out.adj_iters = P->ait.p;
+    d.sc.order = P->order.p;
     d.out.status = status ? status : P->status_tmp.p;
     d.out.T_out = P->dbg_T;
     d.out.Ta_out = P->dbg_Ta;
@@ -464,6 +486,14 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
         if (P->timing) SA_CUDA(cudaEventRecord(P->tk1, st));
         if (calc_adj && chi) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi, st));
         SA_CUDA(launch_fold_status(P->ne, d.out.status, P->worst.p, st));
+        const size_t ib = (size_t)P->ne * sizeof(int);
+        if (fwd_iters)
+            SA_CUDA(cudaMemcpyAsync(fwd_iters, P->fit.p, ib, cudaMemcpyDeviceToDevice, st));
+        if (calc_adj && adj_iters)
+            SA_CUDA(cudaMemcpyAsync(adj_iters, P->ait.p, ib, cudaMemcpyDeviceToDevice, st));
+        SA_CUDA(launch_event_cost(P->ne, P->fit.p, P->ait.p, P->key_a.p, P->ord_idx.p, st));
+        SA_CUDA(launch_sort_events(P->ne, P->key_a.p, P->key_b.p, P->ord_idx.p, P->order.p,
+                                   P->sort_tmp.p, P->sort_bytes, st));
     } else {
         if (calc_adj && chi) SA_CUDA(cudaMemsetAsync(chi, 0, sizeof(double), st));
         SA_CUDA(cudaMemsetAsync(P->worst.p, 0, sizeof(int), st));

@@ -98,6 +98,7 @@ struct Scratch {
     size_t slot_bytes;
     unsigned char* base;
     unsigned int* queue;   // work-queue counter (reset to 0 before each launch)
+    const int* order;      // queue position -> event (NULL: identity)
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }

@@ -153,9 +153,11 @@ struct FwdBase {
         S v;    // field before this update
         S x;    // T0 of the cell
         S gx, gy, f, vs;
+        unsigned fl;     // sweep flags (systolic.cuh)
         MetricCell<S, ISO> m;
     };
     int nx, ny;
+    unsigned char* flags;  // per event
     const Q4<S>* pk;     // per event
     const Q4<S>* mt;     // per period (general metric) or null
     const S* a_row;      // iso: [ny]
@@ -193,6 +195,7 @@ struct FwdBase {
             c.m.c = m.z;
         }
         c.vs = last ? tau_start[k] : S(0);
+        c.fl = flags[k];
         return c;
     }
     __device__ S ca(const Cell& c) const {
@@ -209,12 +212,16 @@ struct FwdBase {
         Cell c{};
         c.v = tau[k];
         c.x = pk[k].x;
+        c.fl = flags[k];
         return c;
     }
-    __device__ void store(int iy, int ix, S v, bool last) const {
+    __device__ void store(int iy, int ix, S v, bool write_v, bool write_start) const {
         const size_t k = (size_t)iy * nx + ix;
-        tau[k] = v;
-        if (last) tau_start[k] = v;
+        if (write_v) tau[k] = v;
+        if (write_start) tau_start[k] = v;
+    }
+    __device__ void store_flag(int iy, int ix, unsigned f) const {
+        flags[(size_t)iy * nx + ix] = (unsigned char)f;
     }
 };
 
@@ -229,18 +236,17 @@ struct FwdPolicy64 : FwdBase<double, ISO> {
     double dx, dy;
     __device__ double update(const Cell& cur, int iy, int ix, const Nb<double, double>& xm,
                              const Nb<double, double>& xp, const Nb<double, double>& ym,
-                             const Nb<double, double>& yp, bool last, double& l1,
-                             double& linf) const {
+                             const Nb<double, double>& yp) const {
         if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;   // ischange == 0
-        const double nv = fsm_update<double, ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur),
-                                                  this->cb(cur), this->cc(cur), cur.f, dx, dy, xm,
-                                                  xp, ym, yp);
-        if (last) {
-            const double d = fabs(nv - cur.vs) * cur.x;
-            l1 += d;
-            linf = fmax(linf, d);
-        }
-        return nv;
+        return fsm_update<double, ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur),
+                                       this->cb(cur), this->cc(cur), cur.f, dx, dy, xm, xp, ym,
+                                       yp);
+    }
+    // convergence sums of src/eikonal_solver.cpp:292-302, last sweep only
+    __device__ void account(const Cell& cur, double nv, double& l1, double& linf) const {
+        const double d = fabs(nv - cur.vs) * cur.x;
+        l1 += d;
+        linf = fmax(linf, d);
     }
 };
 
@@ -345,18 +351,15 @@ struct FwdPolicyDelta32 : FwdBase<float, ISO> {
     float idx, idy;
     __device__ float update(const Cell& cur, int iy, int ix, const Nb<float, float>& xm,
                             const Nb<float, float>& xp, const Nb<float, float>& ym,
-                            const Nb<float, float>& yp, bool last, double& l1,
-                            double& linf) const {
+                            const Nb<float, float>& yp) const {
         if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;
-        const float nv = fsm_update_delta<ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur),
-                                               this->cb(cur), this->cc(cur), cur.f, idx, idy, xm,
-                                               xp, ym, yp);
-        if (last) {
-            const double d = fabs((double)nv - (double)cur.vs) * (double)cur.x;
-            l1 += d;
-            linf = fmax(linf, d);
-        }
-        return nv;
+        return fsm_update_delta<ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur), this->cb(cur),
+                                     this->cc(cur), cur.f, idx, idy, xm, xp, ym, yp);
+    }
+    __device__ void account(const Cell& cur, float nv, double& l1, double& linf) const {
+        const double d = fabs((double)nv - (double)cur.vs) * (double)cur.x;
+        l1 += d;
+        linf = fmax(linf, d);
     }
 };
 
@@ -374,9 +377,11 @@ struct AdjPolicyExact {
         Q4<double> q;
         double2 de;
         double vs;
+        unsigned fl;
     };
     int nx, ny;
     double dx, dy;
+    unsigned char* flags;
     const Q4<double>* aq;
     const double2* dd;
     double* Ta;
@@ -395,17 +400,19 @@ struct AdjPolicyExact {
         c.q = ld4(aq + k);
         c.de = dd[k];
         c.vs = last ? Ta_start[k] : 0.0;
+        c.fl = flags[k];
         return c;
     }
     __device__ Cell load_nb(int iy, int ix) const {
         Cell c{};
-        c.v = Ta[(size_t)iy * nx + ix];
+        const size_t k = (size_t)iy * nx + ix;
+        c.v = Ta[k];
+        c.fl = flags[k];
         return c;
     }
     __device__ double update(const Cell& cur, int iy, int ix, const Nb<double, float>& xm,
                              const Nb<double, float>& xp, const Nb<double, float>& ym,
-                             const Nb<double, float>& yp, bool last, double& l1,
-                             double& linf) const {
+                             const Nb<double, float>& yp) const {
         const double2 de = cur.de;
         double nv;
         if (fabs(de.y) < 1e-14) {
@@ -419,17 +426,21 @@ struct AdjPolicyExact {
             const double e = (txm * q.x - txp * q.y) / dx + (tym * q.z - typ * q.w) / dy;
             nv = (de.x + e) / de.y;
         }
-        if (last) {
-            const double dv = fabs(nv - cur.vs);
-            l1 += dv;
-            linf = fmax(linf, dv);
-        }
         return nv;
     }
-    __device__ void store(int iy, int ix, double v, bool last) const {
+    // src/eikonal_solver.cpp:498-507
+    __device__ void account(const Cell& cur, double nv, double& l1, double& linf) const {
+        const double dv = fabs(nv - cur.vs);
+        l1 += dv;
+        linf = fmax(linf, dv);
+    }
+    __device__ void store(int iy, int ix, double v, bool write_v, bool write_start) const {
         const size_t k = (size_t)iy * nx + ix;
-        Ta[k] = v;
-        if (last) Ta_start[k] = v;
+        if (write_v) Ta[k] = v;
+        if (write_start) Ta_start[k] = v;
+    }
+    __device__ void store_flag(int iy, int ix, unsigned f) const {
+        flags[(size_t)iy * nx + ix] = (unsigned char)f;
     }
 };
 
@@ -446,8 +457,10 @@ struct AdjPolicyW32 {
         Q4<float> w;
         float c0;
         float vs;
+        unsigned fl;
     };
     int nx, ny;
+    unsigned char* flags;
     const Q4<float>* W;
     const float* C0;
     float* Ta;
@@ -467,34 +480,38 @@ struct AdjPolicyW32 {
         c.w = ld4(W + k);
         c.c0 = C0[k];
         c.vs = last ? Ta_start[k] : 0.f;
+        c.fl = flags[k];
         return c;
     }
     __device__ Cell load_nb(int iy, int ix) const {
         Cell c{};
-        c.v = Ta[(size_t)iy * nx + ix];
+        const size_t k = (size_t)iy * nx + ix;
+        c.v = Ta[k];
+        c.fl = flags[k];
         return c;
     }
     __device__ float update(const Cell& cur, int, int, const Nb<float, float>& xm,
                             const Nb<float, float>& xp, const Nb<float, float>& ym,
-                            const Nb<float, float>& yp, bool last, double& l1,
-                            double& linf) const {
+                            const Nb<float, float>& yp) const {
         const float txm = xm.has ? xm.v : 0.f;
         const float txp = xp.has ? xp.v : 0.f;
         const float tym = ym.has ? ym.v : 0.f;
         const float typ = yp.has ? yp.v : 0.f;
-        const float nv = cur.c0 + cur.w.x * txm + cur.w.y * txp + cur.w.z * tym + cur.w.w * typ;
-        if (last) {
-            const double dv = fabs((double)nv - (double)cur.vs);
-            l1 += dv;
-            linf = fmax(linf, dv);
-            const_cast<AdjPolicyW32*>(this)->vmax = fmax(vmax, fabs((double)nv));
-        }
-        return nv;
+        return cur.c0 + cur.w.x * txm + cur.w.y * txp + cur.w.z * tym + cur.w.w * typ;
     }
-    __device__ void store(int iy, int ix, float v, bool last) const {
+    __device__ void account(const Cell& cur, float nv, double& l1, double& linf) {
+        const double dv = fabs((double)nv - (double)cur.vs);
+        l1 += dv;
+        linf = fmax(linf, dv);
+        vmax = fmax(vmax, fabs((double)nv));
+    }
+    __device__ void store(int iy, int ix, float v, bool write_v, bool write_start) const {
         const size_t k = (size_t)iy * nx + ix;
-        Ta[k] = v;
-        if (last) Ta_start[k] = v;
+        if (write_v) Ta[k] = v;
+        if (write_start) Ta_start[k] = v;
+    }
+    __device__ void store_flag(int iy, int ix, unsigned f) const {
+        flags[(size_t)iy * nx + ix] = (unsigned char)f;
     }
 };
 

@@ -78,6 +78,12 @@ cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, 
 cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int nper,
                                const double* periods, const double* cp, const void* layer_const,
                                double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st);
+cudaError_t launch_event_cost(int ne, const int* fwd_it, const int* adj_it, unsigned int* key,
+                              int* idx, cudaStream_t st);
+size_t sort_events_temp_bytes(int ne);
+cudaError_t launch_sort_events(int ne, const unsigned int* key_in, unsigned int* key_out,
+                               const int* idx_in, int* order, void* temp, size_t temp_bytes,
+                               cudaStream_t st);
 cudaError_t launch_grad_status(int ncol, const int* colst, const int* ev_worst, int* out,
                                cudaStream_t st);
 cudaError_t launch_combine_vs(int nx, int ny, int nz, int nper, const double* adj_s,

@@ -1,5 +1,6 @@
 // Small device utilities: deterministic event-sum of the misfit and status
 // folding.
+#include <cub/cub.cuh>
 #include "launch.h"
 
 namespace sa {
@@ -52,6 +53,23 @@ cudaError_t launch_grad_status(int ncol, const int* colst, const int* ev_worst, 
     return cudaGetLastError();
 }
 
+// Sort key of each event for the next evaluation's queue: the previous
+// evaluation's sweep work, forward sweeps weighted 3x (a forward cell update
+// costs about three adjoint ones).
+__global__ void event_cost_kernel(int ne, const int* __restrict__ fwd_it,
+                                  const int* __restrict__ adj_it, unsigned int* key, int* idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ne) return;
+    key[i] = 3u * (unsigned)fwd_it[i] + (unsigned)adj_it[i];
+    idx[i] = i;
+}
+
+cudaError_t launch_event_cost(int ne, const int* fwd_it, const int* adj_it, unsigned int* key,
+                              int* idx, cudaStream_t st) {
+    event_cost_kernel<<<(ne + 255) / 256, 256, 0, st>>>(ne, fwd_it, adj_it, key, idx);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStream_t st) {
     sum_events_kernel<<<1, 1024, 0, st>>>(ne, chi_ev, chi);
     return cudaGetLastError();
@@ -60,6 +78,22 @@ cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStr
 cudaError_t launch_fold_status(int ne, const int* status, int* worst, cudaStream_t st) {
     fold_status_kernel<<<1, 1024, 0, st>>>(ne, status, worst);
     return cudaGetLastError();
+}
+
+size_t sort_events_temp_bytes(int ne) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const unsigned int*)nullptr,
+                                              (unsigned int*)nullptr, (const int*)nullptr,
+                                              (int*)nullptr, ne);
+    return bytes;
+}
+
+// order = events by descending key (stable: equal keys keep event order).
+cudaError_t launch_sort_events(int ne, const unsigned int* key_in, unsigned int* key_out,
+                               const int* idx_in, int* order, void* temp, size_t temp_bytes,
+                               cudaStream_t st) {
+    return cub::DeviceRadixSort::SortPairsDescending(temp, temp_bytes, key_in, key_out, idx_in,
+                                                     order, ne, 0, 32, st);
 }
 
 }  // namespace sa
