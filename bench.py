@@ -122,10 +122,10 @@ class Clocks:
 
 # DRAM bytes moved per algorithmic byte by batch_kernel<float>, from
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the same
-# kernel on the 151x151 / 3000-event case (82.504 GB moved for 73.420 GB of
+# kernel on the 151x151 / 3000-event case (78.991 GB moved for 73.420 GB of
 # algorithmic bytes; profiles/batch_kernel_fp32_c3_151x151_full.md).  Traffic
 # scales with cell updates, so a full launch moves algorithmic x this ratio.
-TRAFFIC_PER_ALGO_BYTE = {"fp32": 82.503724e9 / 73.419606e9}
+TRAFFIC_PER_ALGO_BYTE = {"fp32": 78.990824e9 / 73.419606e9}
 
 
 def peaks():
@@ -235,6 +235,41 @@ def misfit_gradient_timing(a, w, plan, tt, wt, dev, stream):
             "stages_ms_alone": {"fwdsurf": t_disp, "depthkernel": t_sen,
                                 "forward_adjoint": t_batch, "combine": t_comb},
             "note": "depth kernels run on a second stream concurrently with the event batch"}
+
+
+def pde_smooth_timing(a, w, dev, stream, peak):
+    """PostProc::pde_smooth of a kernel on the workload's 3-D grid: device time
+    per Euler step and HBM throughput (16 B algorithmic per cell per step: one
+    read, one write)."""
+    import torch
+    from surfattpp_b200 import postproc
+    from surfattpp_b200 import workloads as W
+    cs = stream.cuda_stream
+    # the largest model grid (601 x 601 x 50 at 0.005 deg, 2 km): 144 MB > L2
+    xx, yy = W._grid(102.0, 24.0, (601, 601), 0.005)
+    zg = np.arange(0.0, 98.0 + 1e-9, 2.0)
+    w = type("G", (), dict(nx=601, ny=601, nz=zg.size, xx_deg=xx, yy_deg=yy, zgrid=zg))
+    shape = (w.nx, w.ny, w.nz)
+    g = torch.Generator(device=dev).manual_seed(11)
+    f = torch.rand(shape, dtype=torch.float64, device=dev, generator=g)
+    work = torch.empty_like(f)
+    d = float(w.xx_deg[1] - w.xx_deg[0])
+    dz = float(w.zgrid[1] - w.zgrid[0])
+    sig = (5.0 * d, 3.0 * dz)
+    postproc.pde_smooth(f, w.yy_deg, w.zgrid, d, d, dz, *sig, work=work, stream=cs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, ns = postproc.pde_smooth(f, w.yy_deg, w.zgrid, d, d, dz, *sig, work=work, stream=cs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    per = ms / ns
+    gbs = 16.0 * f.numel() / (per * 1e-3) / 1e9
+    return {"grid": list(shape), "sigma": [sig[0], sig[1]], "nstep": ns, "ms_total": ms,
+            "ms_per_step": per, "achieved_gbs": gbs, "frac_of_hbm": gbs / peak,
+            "note": "per step one read and one write of the field (16 B per cell); "
+                    "field %.0f MB" % (f.numel() * 8 / 1e6)}
 
 
 def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx):
@@ -365,6 +400,7 @@ def main():
     if world == 1 and not a.no_extras:
         extra["misfit_gradient"] = misfit_gradient_timing(a, w, plan, tt, wt, dev, stream)
         extra["fp64_plain"] = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx)
+        extra["pde_smooth"] = pde_smooth_timing(a, w, dev, stream, peaks()[0])
 
     if rank == 0:
         peak, peak_kind = peaks()
@@ -381,7 +417,9 @@ def main():
             "config": workload_config(a, world),
             "e2e": {"value": total_events / (ms_e2e * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": (5 if a.precision == "fp32" else 4) * a.steps,
+            # per step: media64, [media32], batch, sum_events, fold_status,
+            # event_cost (the queue-order sort is CUB, not counted)
+            "gpu_launches": (6 if a.precision == "fp32" else 5) * a.steps,
             "cell_updates_per_s": (nf + na) / (ms * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,

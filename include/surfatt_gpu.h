@@ -168,6 +168,28 @@ int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper, const d
                           const double* sen_vp, const double* sen_rho, double* ker_vs,
                           void* stream);
 
+/* ---- PostProc::pde_smooth ------------------------------------------------- */
+
+/* Step count and per-step diffusion coefficients of PostProc::pde_smooth
+ * (reference src/postproc.cpp:394-434): nstep, ch (deg^2), cv (km^2).
+ * ygrid[ny] latitudes in degrees (only the first and last are used).
+ * Host arithmetic only.  SA_ERR_ARG for non-positive sigma or too fine a grid
+ * (the reference logs an error and aborts). */
+int sa_pde_smooth_nstep(int ny, double dx_deg, double dy_deg, double dz_km, const double* ygrid,
+                        double sigma_h, double sigma_v, int* nstep, double* ch, double* cv);
+
+/* Replaces PostProc::pde_smooth (src/postproc.cpp:388-463) on one rank:
+ * nstep explicit Euler steps of the spherical Laplacian (:35-128) with the
+ * Neumann boundary copies (:130-158).  field (device, in/out): (nx, ny, nz)
+ * row-major, depth fastest (Tensor3r); work: device scratch of nx*ny*nz
+ * doubles, or NULL to allocate one for the call.  ygrid[ny] (degrees) and
+ * zgrid[nz] (km) are host arrays; dx_deg, dy_deg, dz_km the grid intervals.
+ * nstep_out (host, may be NULL) receives the step count.  Returns after the
+ * smoothing has completed on `stream` (NULL = the context's stream). */
+int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg, double dy_deg,
+                  double dz_km, const double* ygrid, const double* zgrid, double sigma_h,
+                  double sigma_v, double* field, double* work, int* nstep_out, void* stream);
+
 /* ---- one misfit-gradient evaluation ---------------------------------------- */
 
 /* Replaces one data type's pass of Inversion::run_forward_adjoint(true)

@@ -120,6 +120,18 @@ int orc_depthkernel_hti(int nx, int ny, int nz, const double* zgrid,
                         double* sen_vs, double* sen_vp, double* sen_rho,
                         int* status, int nthreads);
 
+/* PostProc::pde_smooth (src/postproc.cpp:388-463), one rank.  field (nx, ny, nz)
+ * row-major, depth fastest, smoothed in place.  dx, dy in degrees, dz in km;
+ * ygrid[ny] latitudes (degrees), zgrid[nz] depths (km).  Returns 0, or < 0 for
+ * invalid sigma (-1), too fine a grid (-2) or a grid below 3x3x3 (-3).
+ * orc_pde_smooth_nstep returns the step count and the per-step diffusion
+ * coefficients ch (deg^2) and cv (km^2) (:407-434). */
+int orc_pde_smooth_nstep(int ny, double dx, double dy, double dz, double y_first,
+                         double y_last, double sigma_h, double sigma_v, double* ch, double* cv);
+int orc_pde_smooth(int nx, int ny, int nz, double dx, double dy, double dz, const double* ygrid,
+                   const double* zgrid, double sigma_h, double sigma_v, double* field,
+                   int* nstep_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,10 @@ def lib():
     L.orc_sregn96.argtypes = [_fp, _fp, _fp, _fp, i, _dp, _dp, _dp] + [_dp] * 8 + [i]
     L.orc_fwdsurf.argtypes = [i, i, i, _dp, _dp, i, _dp, i, i, _dp, _ip, i]
     L.orc_depthkernel_hti.argtypes = [i, i, i, _dp, _dp, i, _dp, _dp, _dp, _dp, _ip, i]
+    L.orc_pde_smooth_nstep.argtypes = [i, d, d, d, d, d, d, d, C.POINTER(d), C.POINTER(d)]
+    L.orc_pde_smooth_nstep.restype = i
+    L.orc_pde_smooth.argtypes = [i, i, i, d, d, d, _dp, _dp, d, d, _dp, C.POINTER(i)]
+    L.orc_pde_smooth.restype = i
     _lib = L
     return L
 
@@ -199,3 +203,23 @@ def depthkernel_hti(zgrid, vs3d, periods, nthreads=1):
     lib().orc_depthkernel_hti(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
                               int(nthreads))
     return sv, sp, sr, st
+
+
+def pde_smooth_nstep(ny, dx, dy, dz, y_first, y_last, sigma_h, sigma_v):
+    """(nstep, ch, cv) of PostProc::pde_smooth (src/postproc.cpp:407-434)."""
+    ch, cv = C.c_double(), C.c_double()
+    n = lib().orc_pde_smooth_nstep(ny, dx, dy, dz, y_first, y_last, sigma_h, sigma_v,
+                                   C.byref(ch), C.byref(cv))
+    return n, ch.value, cv.value
+
+
+def pde_smooth(field, dx, dy, dz, ygrid, zgrid, sigma_h, sigma_v):
+    """PostProc::pde_smooth on one rank: returns (smoothed copy, nstep)."""
+    f = _c(field).copy()
+    nx, ny, nz = f.shape
+    ns = C.c_int(0)
+    rc = lib().orc_pde_smooth(nx, ny, nz, dx, dy, dz, _c(ygrid), _c(zgrid), sigma_h, sigma_v, f,
+                              C.byref(ns))
+    if rc != 0:
+        raise ValueError(f"orc_pde_smooth failed ({rc})")
+    return f, ns.value

@@ -28,6 +28,7 @@ EXPORTED = (
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
     "sa_eik_fwd_field_noalloc",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen",
+    "sa_pde_smooth_nstep", "sa_pde_smooth",
 )
 
 
@@ -86,6 +87,10 @@ def lib():
     L.sa_grad_destroy.argtypes = [_vp]
     L.sa_grad_run.argtypes = [_vp] + [_vp] * 9 + [_vp]
     L.sa_grad_sen.argtypes = [_vp] * 5
+    L.sa_pde_smooth_nstep.argtypes = [i, d, d, d, _dp, d, d, C.POINTER(i), C.POINTER(d),
+                                      C.POINTER(d)]
+    L.sa_pde_smooth.argtypes = [_vp, i, i, i, d, d, d, _dp, _dp, d, d, _vp, _vp, C.POINTER(i),
+                                _vp]
     _lib = L
     return L
 

@@ -3,6 +3,7 @@
 Each translation unit gets the flags its arithmetic contract needs:
   eik64.cu   -fmad=false: FP64 parity path, every operation rounds as written
   eik32.cu   fast FP32 division/sqrt, FTZ: the FP32 sweep path
+  postproc.cu -fmad=false: PDE smoothing rounds as the reference's FP64
   others     default IEEE flags
 """
 from __future__ import annotations
@@ -28,6 +29,7 @@ UNITS = {
     "util.cu": [],
     "capi.cu": ["-Xcompiler", "-ffp-contract=off"],
     "noalloc.cu": [],
+    "postproc.cu": ["-fmad=false"],
 }
 
 

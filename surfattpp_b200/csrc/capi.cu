@@ -988,3 +988,83 @@ extern "C" int sa_grad_sen(sa_grad* g, double* sen_vs, double* sen_vp, double* s
         if (dst[i]) SA_CUDA(cudaMemcpyAsync(dst[i], src[i], bytes, cudaMemcpyDeviceToDevice, st));
     return SA_OK;
 }
+
+// ---- PostProc::pde_smooth ------------------------------------------------------
+
+namespace {
+constexpr double PI_D = 3.14159265358979323846264338327950288;   // include/config.h:54
+constexpr double DEG2RAD_D = PI_D / 180.0;                         // include/config.h:68
+}  // namespace
+
+// Step count and diffusion coefficients of src/postproc.cpp:394-434.
+extern "C" int sa_pde_smooth_nstep(int ny, double dx_deg, double dy_deg, double dz_km,
+                                   const double* ygrid, double sigma_h, double sigma_v,
+                                   int* nstep, double* ch_out, double* cv_out) {
+    if (ny < 1 || !ygrid || !nstep) return SA_ERR_ARG;
+    if (!(sigma_h > 0.0) || !(sigma_v > 0.0)) return SA_ERR_ARG;   // :397-400
+    double lat_max = std::max(std::abs(ygrid[0]), std::abs(ygrid[ny - 1]));
+    lat_max = std::min(lat_max, 89.0);
+    const double cos2_lat_max = std::pow(std::cos(lat_max * DEG2RAD_D), 2);
+    const double cmax_h = std::min(dx_deg * dx_deg * cos2_lat_max, dy_deg * dy_deg) / 6.0;
+    const double cmax_v = dz_km * dz_km / 6.0;
+    if (cmax_h <= 1e-12 || cmax_v <= 1e-12) return SA_ERR_ARG;   // :414-417
+    const double dt = 1.0;
+    const double nh = std::ceil(sigma_h * sigma_h / (2.0 * cmax_h * dt));
+    const double nv = std::ceil(sigma_v * sigma_v / (2.0 * cmax_v * dt));
+    if (!(nh < 2e9) || !(nv < 2e9)) return SA_ERR_ARG;
+    const int ns = std::max({(int)nh, (int)nv, 1});
+    *nstep = ns;
+    if (ch_out) *ch_out = sigma_h * sigma_h / (2.0 * ns * dt);
+    if (cv_out) *cv_out = sigma_v * sigma_v / (2.0 * ns * dt);
+    return SA_OK;
+}
+
+extern "C" int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg, double dy_deg,
+                             double dz_km, const double* ygrid, const double* zgrid,
+                             double sigma_h, double sigma_v, double* field, double* work,
+                             int* nstep_out, void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 3 || ny < 3 || nz < 3 || !ygrid || !zgrid || !field)
+        return fail(ctx, SA_ERR_ARG, "sa_pde_smooth: grid must be at least 3x3x3");
+    int ns = 0;
+    double ch = 0, cv = 0;
+    if (sa_pde_smooth_nstep(ny, dx_deg, dy_deg, dz_km, ygrid, sigma_h, sigma_v, &ns, &ch, &cv))
+        return fail(ctx, SA_ERR_ARG,
+                    "Invalid sigma values or grid spacing for PDE-based smoothing");
+    if (nstep_out) *nstep_out = ns;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    // per-row and per-depth factors in the reference's evaluation order (:74-123)
+    const double dx2_inv = 1.0 / (dx_deg * dx_deg);
+    const double dy2_inv = 1.0 / (dy_deg * dy_deg);
+    const double dz2_inv = 1.0 / (dz_km * dz_km);
+    const double dy_inv_half = 1.0 / (2.0 * dy_deg);
+    const double dz_inv_half = 1.0 / (2.0 * dz_km);
+    std::vector<double> rowX(ny, 0.0), rowY(ny, 0.0), depE(nz, 0.0);
+    for (int iy = 1; iy < ny - 1; ++iy) {
+        const double lat_rad = (ygrid[0] + iy * dy_deg) * DEG2RAD_D;   // src/decomposer.cpp:116-118
+        const double cos_lat = std::cos(lat_rad);
+        const double dy2_corr_inv = 1.0 / (cos_lat * cos_lat);
+        const double tan_lat = std::tan(lat_rad);
+        rowX[iy] = ch * dx2_inv * dy2_corr_inv;
+        rowY[iy] = ch * DEG2RAD_D * tan_lat * dy_inv_half;
+    }
+    for (int k = 0; k < nz; ++k) {
+        const double r_inv = 2.0 / (R_EARTH - zgrid[k]);
+        depE[k] = cv * r_inv * dz_inv_half;
+    }
+    DArr<double> d_rx, d_ry, d_de, d_work;
+    SA_CUDA(d_rx.upload(rowX.data(), ny, st));
+    SA_CUDA(d_ry.upload(rowY.data(), ny, st));
+    SA_CUDA(d_de.upload(depE.data(), nz, st));
+    double* w = work;
+    if (!w) {
+        SA_CUDA(d_work.alloc((size_t)nx * ny * nz));
+        w = d_work.p;
+    }
+    SA_CUDA(launch_pde_smooth(nx, ny, nz, ch * dy2_inv, cv * dz2_inv, d_rx.p, d_ry.p, d_de.p, ns,
+                              field, w, st));
+    // the factor arrays (and an internal work array) are released on return
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}

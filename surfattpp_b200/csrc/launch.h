@@ -86,6 +86,10 @@ cudaError_t launch_sort_events(int ne, const unsigned int* key_in, unsigned int*
                                cudaStream_t st);
 cudaError_t launch_grad_status(int ncol, const int* colst, const int* ev_worst, int* out,
                                cudaStream_t st);
+// postproc.cu
+cudaError_t launch_pde_smooth(int nx, int ny, int nz, double B, double D, const double* rowX,
+                              const double* rowY, const double* depE, int nstep, double* field,
+                              double* work, cudaStream_t st);
 cudaError_t launch_combine_vs(int nx, int ny, int nz, int nper, const double* adj_s,
                               const double* vs3d, const double* vp3d, const double* sen_vs,
                               const double* sen_vp, const double* sen_rho, double* ker_vs,

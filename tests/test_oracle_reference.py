@@ -185,3 +185,35 @@ def test_sregn96_vs_kernel_matches_fd(orc):
         cm, _ = orc.surfdisp96(thk, vp, vsm, rho, np.array([T]), iflsph=0)
         fd = vs[layer] * (cp[0] - cm[0]) / (2 * h)
         assert abs(fd - o["dc2db"][layer]) < 2e-4 + 1e-3 * abs(fd)
+
+
+def test_pde_smooth_oracle_properties(orc):
+    """PostProc::pde_smooth restatement: step count formula (src/postproc.cpp:
+    407-434), constants preserved exactly, extrema not exceeded."""
+    y = 24.0 + 0.05 * np.arange(23)
+    z = 2.0 * np.arange(12)
+    n, ch, cv = orc.pde_smooth_nstep(23, 0.05, 0.05, 2.0, y[0], y[-1], 0.1, 4.0)
+    lat = max(abs(y[0]), abs(y[-1]))
+    cmax_h = min(0.05 * 0.05 * np.cos(np.deg2rad(lat)) ** 2, 0.05 * 0.05) / 6.0
+    cmax_v = 4.0 / 6.0
+    assert n == max(int(np.ceil(0.01 / (2 * cmax_h))), int(np.ceil(16.0 / (2 * cmax_v))), 1)
+    assert abs(ch - 0.01 / (2.0 * n)) < 1e-18 and abs(cv - 16.0 / (2.0 * n)) < 1e-15
+    c = np.full((21, 23, 12), -1.5)
+    out, _ = orc.pde_smooth(c, 0.05, 0.05, 2.0, y, z, 0.1, 4.0)
+    assert np.all(out == -1.5)
+    rng = np.random.default_rng(1)
+    f = rng.random((21, 23, 12))
+    out, _ = orc.pde_smooth(f, 0.05, 0.05, 2.0, y, z, 0.1, 4.0)
+    assert out.min() >= f.min() and out.max() <= f.max() and out.std() < f.std()
+
+
+def test_pde_smooth_nstep_library_matches_oracle(orc):
+    """The library's host-side step count (no GPU involved) equals the oracle's."""
+    from surfattpp_b200 import postproc
+    for (d, sh, sv) in ((0.05, 0.1, 4.0), (0.005, 0.02, 6.0), (0.01, 0.3, 1.0)):
+        y = 24.0 + d * np.arange(50)
+        ref = orc.pde_smooth_nstep(50, d, d, 2.0, y[0], y[-1], sh, sv)
+        got = postproc.pde_smooth_nstep(y, d, d, 2.0, sh, sv)
+        assert got == ref
+    with pytest.raises(ValueError):
+        postproc.pde_smooth_nstep(y, 0.05, 0.05, 2.0, -1.0, 4.0)
