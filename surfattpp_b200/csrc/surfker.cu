@@ -36,6 +36,12 @@ struct LayerConst {
     float thk[MMAX];         // unflattened float thickness (build_disp_req)
 };
 
+// The column kernels are large; functions reached from several call sites
+// are kept out of line so the hot loop fits the instruction cache.
+#ifndef SK_NOINLINE
+#define SK_NOINLINE __noinline__
+#endif
+
 __device__ __forceinline__ double dsign1(double x) { return copysign(1.0, x); }
 
 // Brocher relations, scalar forms (include/utils.h:185-187, :223-225)
@@ -207,7 +213,7 @@ __device__ __forceinline__ void normc(double* ee, int n) {
 }
 
 // surfdisp96.f:801-901
-__device__ inline double dltar4(const SDModel& M, double wvno, double omga) {
+__device__ SK_NOINLINE double dltar4(const SDModel& M, double wvno, double omga) {
     const int mmax = M.mmax;
     double omega = omga;
     if (omega < 1.0e-4) omega = 1.0e-4;
@@ -269,7 +275,7 @@ __device__ inline double dltar4(const SDModel& M, double wvno, double omga) {
 }
 
 // surfdisp96.f:737-797
-__device__ inline double dltar1(const SDModel& M, double wvno, double omega) {
+__device__ SK_NOINLINE double dltar1(const SDModel& M, double wvno, double omega) {
     const int mmax = M.mmax;
     double beta1 = (double)M.b[mmax - 1];
     double rho1 = (double)M.rho[mmax - 1];
@@ -323,7 +329,7 @@ __device__ __forceinline__ double dltar(const SDModel& M, double wvno, double om
 }
 
 // surfdisp96.f:578-711 (nevill with half inlined)
-__device__ inline double nevill(const SDModel& M, double t, double c1, double c2, double del1,
+__device__ SK_NOINLINE double nevill(const SDModel& M, double t, double c1, double c2, double del1,
                                 double del2, int ifunc, double twopi) {
     double x[20], y[20];
     const double omega = twopi / t;
@@ -400,7 +406,7 @@ __device__ inline double nevill(const SDModel& M, double t, double c1, double c2
 }
 
 // surfdisp96.f:403-498
-__device__ inline int getsol(SDModel& M, double t1, double& c1, double clow, double dc, double cm,
+__device__ SK_NOINLINE int getsol(SDModel& M, double t1, double& c1, double clow, double dc, double cm,
                              float betmx, int ifunc, int ifirst) {
     const double twopi = 2.0 * 3.141592653589793;
     double omega = twopi / t1;
@@ -655,7 +661,7 @@ struct VarSv {
     double cosp, cosq, rsinp, rsinq, sinpr, sinqr, pex, svex;
 };
 // sregn96.f90:827-911
-__device__ inline VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
+__device__ SK_NOINLINE VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
     VarSv o;
     const double lim = (double)1.0e-5f;
     o.svex = 0.0;
@@ -688,7 +694,7 @@ __device__ inline VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
 }
 
 // sregn96.f90:491-647 fused with the product ee(i) = sum_j cd(m+1,j)*ca(j,i)
-__device__ inline void dnka_rg(double ca[5][5], double cosp, double rsinp, double sinpr,
+__device__ SK_NOINLINE void dnka_rg(double ca[5][5], double cosp, double rsinp, double sinpr,
                                double cossv, double rsinsv, double sinsvr, float rho, float b,
                                int iwat, double ex, double exa, double wvno, double wvno2,
                                double om2) {
@@ -767,7 +773,7 @@ __device__ inline void dnka_rg(double ca[5][5], double cosp, double rsinp, doubl
 }
 
 // sregn96.f90:649-825 (jbdry = 0, inp = 1)
-__device__ inline void evalg(RW& W, int m, cx* gbr, double wvno, double om, double om2,
+__device__ SK_NOINLINE void evalg(RW& W, int m, cx* gbr, double wvno, double om, double om2,
                              double wvno2) {
     const double xka = om / W.za[m - 1];
     const double xkb = (W.zb[m - 1] > 0.0) ? om / W.zb[m - 1] : 0.0;
@@ -1045,7 +1051,7 @@ __device__ inline cx h2func(cx nua, cx nub, double dm) {
 // The six energy integrals of one layer (sregn96.f90:1205-1324 called with
 // (1,1),(1,3),(2,2),(2,4),(3,3),(4,4)); evalg is evaluated once per layer
 // (its outputs are the same for every (i, j)).
-__device__ inline void layer_integrals(RW& W, int m, int typelyr, double om, double om2,
+__device__ SK_NOINLINE void layer_integrals(RW& W, int m, int typelyr, double om, double om2,
                                        double wvno, double wvno2, double* I) {
     evalg(W, m, nullptr, wvno, om, om2, wvno2);
     const cx ra = W.ra, rb = W.rb;
