@@ -23,6 +23,8 @@
 #ifndef SURFATT_GPU_H
 #define SURFATT_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -189,6 +191,41 @@ int sa_pde_smooth_nstep(int ny, double dx_deg, double dy_deg, double dz_km, cons
 int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg, double dy_deg,
                   double dz_km, const double* ygrid, const double* zgrid, double sigma_h,
                   double sigma_v, double* field, double* work, int* nstep_out, void* stream);
+
+/* ---- optimizer: L-BFGS, strong Wolfe, model update (vs-only) --------------- */
+
+/* History of the last 6 iterates (model vs and gradient, n values each, kept
+ * on the device) for optimize::lbfgs_direction (reference
+ * src/optimize.cpp:150-255), replacing the model_vs_NNN / grad_vs_NNN
+ * datasets that Inversion::store_model / store_gradient write to HDF5
+ * (src/inversion.cpp:326-373).  sa_lbfgs_store copies device arrays into the
+ * slot of `iter`; sa_lbfgs_direction(iter) returns H_k g_k of the two-loop
+ * recursion (5 pairs at most, log-space model differences) in dir (device). */
+typedef struct sa_lbfgs sa_lbfgs;
+int sa_lbfgs_create(sa_ctx* ctx, size_t n, sa_lbfgs** out);
+void sa_lbfgs_destroy(sa_lbfgs* lbfgs);
+int sa_lbfgs_store(sa_lbfgs* lbfgs, int iter, const double* model, const double* grad);
+int sa_lbfgs_direction(sa_lbfgs* lbfgs, int iter, double* dir);
+
+/* Inner product of two device arrays (FP64, fixed reduction order), result on
+ * the host (optimize::field_dot + MPI sum, src/optimize.cpp:18-27, :62-68). */
+int sa_dot(sa_ctx* ctx, size_t n, const double* a, const double* b, double* out);
+/* Inversion::grad_normalization (src/inversion.cpp:302-323): g /= max|g|
+ * unless max|g| < DBL_EPSILON; max_out (host, may be NULL) receives max|g|. */
+int sa_grad_normalization(sa_ctx* ctx, size_t n, double* g, double* max_out);
+/* optimize::calc_descent_angle (src/optimize.cpp:33-57), degrees, on the host. */
+int sa_descent_angle(sa_ctx* ctx, size_t n, const double* dir, const double* grad, double* deg);
+/* optimize::wolfe_condition (src/optimize.cpp:74-145) from gd = grad.dir and
+ * kd = ker_next.dir (host arithmetic).  Returns 0 ACCEPT, 1 TRY, 2 FAIL (-1
+ * for NULL pointers); updates the bracket and next_alpha as the reference. */
+int sa_wolfe_condition(double gd, double kd, double alpha, double* alpha_L, double* alpha_R,
+                       double f0, double f1, int subiter, double c1, double c2,
+                       int max_sub_niter, double alpha_init, double* next_alpha);
+/* Inversion::model_update, vs-only (src/inversion.cpp:465-490):
+ * vs_out = vs*(1 - alpha*dir), vp_out = vs2vp(vs_out), rho_out = vp2rho(vp_out)
+ * (vp_out, rho_out may be NULL; vs_out may alias vs).  Device arrays. */
+int sa_model_update_vs(sa_ctx* ctx, size_t n, const double* vs, const double* dir, double alpha,
+                       double* vs_out, double* vp_out, double* rho_out, void* stream);
 
 /* ---- one misfit-gradient evaluation ---------------------------------------- */
 

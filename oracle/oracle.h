@@ -20,6 +20,8 @@
 #ifndef SURFATT_ORACLE_H
 #define SURFATT_ORACLE_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -131,6 +133,21 @@ int orc_pde_smooth_nstep(int ny, double dx, double dy, double dz, double y_first
 int orc_pde_smooth(int nx, int ny, int nz, double dx, double dy, double dz, const double* ygrid,
                    const double* zgrid, double sigma_h, double sigma_v, double* field,
                    int* nstep_out);
+
+/* Optimizer (vs-only parametrisation, src/optimize.cpp, src/inversion.cpp).
+ * orc_lbfgs_direction: models/grads are nhist + 1 consecutive iterates (oldest
+ * first, the current one last), n values each; dir receives H g. */
+void orc_lbfgs_direction(size_t n, int nhist, const double* const* models,
+                         const double* const* grads, double* dir);
+double orc_grad_normalization(size_t n, double* g);
+double orc_descent_angle(size_t n, const double* dir, const double* grad);
+int orc_wolfe_condition(double gd, double kd, double alpha, double* alpha_L, double* alpha_R,
+                        double f0, double f1, int subiter, double c1, double c2,
+                        int max_sub_niter, double alpha_init, double* next_alpha);
+void orc_model_update_vs(size_t n, const double* vs, const double* dir, double alpha,
+                         double* vs_out, double* vp_out, double* rho_out);
+double orc_vs2vp(double vs);
+double orc_vp2rho(double vp);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,16 @@ def lib():
     L.orc_pde_smooth_nstep.restype = i
     L.orc_pde_smooth.argtypes = [i, i, i, d, d, d, _dp, _dp, d, d, _dp, C.POINTER(i)]
     L.orc_pde_smooth.restype = i
+    z = C.c_size_t
+    L.orc_lbfgs_direction.argtypes = [z, i, C.POINTER(C.POINTER(d)), C.POINTER(C.POINTER(d)), _dp]
+    L.orc_grad_normalization.argtypes = [z, _dp]
+    L.orc_grad_normalization.restype = d
+    L.orc_descent_angle.argtypes = [z, _dp, _dp]
+    L.orc_descent_angle.restype = d
+    L.orc_wolfe_condition.argtypes = [d, d, d, C.POINTER(d), C.POINTER(d), d, d, i, d, d, i, d,
+                                      C.POINTER(d)]
+    L.orc_wolfe_condition.restype = i
+    L.orc_model_update_vs.argtypes = [z, _dp, _dp, d, _dp, _dp, _dp]
     _lib = L
     return L
 
@@ -223,3 +233,42 @@ def pde_smooth(field, dx, dy, dz, ygrid, zgrid, sigma_h, sigma_v):
     if rc != 0:
         raise ValueError(f"orc_pde_smooth failed ({rc})")
     return f, ns.value
+
+
+def lbfgs_direction(models, grads):
+    """optimize::lbfgs_direction over consecutive iterates (oldest first, the
+    current one last): returns H g."""
+    ms = [_c(m).ravel() for m in models]
+    gs = [_c(g).ravel() for g in grads]
+    n = ms[-1].size
+    P = C.POINTER(C.c_double)
+    mp = (P * len(ms))(*[m.ctypes.data_as(P) for m in ms])
+    gp = (P * len(gs))(*[g.ctypes.data_as(P) for g in gs])
+    out = np.zeros(n)
+    lib().orc_lbfgs_direction(n, len(ms) - 1, mp, gp, out)
+    return out
+
+
+def grad_normalization(g):
+    g = _c(g).ravel().copy()
+    m = lib().orc_grad_normalization(g.size, g)
+    return g, m
+
+
+def descent_angle(direction, grad):
+    return lib().orc_descent_angle(_c(direction).size, _c(direction).ravel(), _c(grad).ravel())
+
+
+def wolfe_condition(gd, kd, alpha, alpha_L, alpha_R, f0, f1, subiter, c1, c2, max_sub, alpha_init):
+    aL, aR, nxt = C.c_double(alpha_L), C.c_double(alpha_R), C.c_double()
+    st = lib().orc_wolfe_condition(gd, kd, alpha, C.byref(aL), C.byref(aR), f0, f1, subiter, c1,
+                                   c2, max_sub, alpha_init, C.byref(nxt))
+    return st, nxt.value, aL.value, aR.value
+
+
+def model_update_vs(vs, direction, alpha):
+    v = _c(vs).ravel()
+    n = v.size
+    o1, o2, o3 = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().orc_model_update_vs(n, v, _c(direction).ravel(), alpha, o1, o2, o3)
+    return o1, o2, o3

@@ -29,6 +29,8 @@ EXPORTED = (
     "sa_eik_fwd_field_noalloc",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
+    "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
+    "sa_grad_normalization", "sa_descent_angle", "sa_wolfe_condition", "sa_model_update_vs",
 )
 
 
@@ -89,6 +91,17 @@ def lib():
     L.sa_grad_sen.argtypes = [_vp] * 5
     L.sa_pde_smooth_nstep.argtypes = [i, d, d, d, _dp, d, d, C.POINTER(i), C.POINTER(d),
                                       C.POINTER(d)]
+    z = C.c_size_t
+    L.sa_lbfgs_create.argtypes = [_vp, z, C.POINTER(_vp)]
+    L.sa_lbfgs_destroy.argtypes = [_vp]
+    L.sa_lbfgs_store.argtypes = [_vp, i, _vp, _vp]
+    L.sa_lbfgs_direction.argtypes = [_vp, i, _vp]
+    L.sa_dot.argtypes = [_vp, z, _vp, _vp, C.POINTER(d)]
+    L.sa_grad_normalization.argtypes = [_vp, z, _vp, C.POINTER(d)]
+    L.sa_descent_angle.argtypes = [_vp, z, _vp, _vp, C.POINTER(d)]
+    L.sa_wolfe_condition.argtypes = [d, d, d, C.POINTER(d), C.POINTER(d), d, d, i, d, d, i, d,
+                                     C.POINTER(d)]
+    L.sa_model_update_vs.argtypes = [_vp, z, _vp, _vp, d, _vp, _vp, _vp, _vp]
     L.sa_pde_smooth.argtypes = [_vp, i, i, i, d, d, d, _dp, _dp, d, d, _vp, _vp, C.POINTER(i),
                                 _vp]
     _lib = L

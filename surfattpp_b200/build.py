@@ -30,6 +30,7 @@ UNITS = {
     "capi.cu": ["-Xcompiler", "-ffp-contract=off"],
     "noalloc.cu": [],
     "postproc.cu": ["-fmad=false"],
+    "optimize.cu": ["-fmad=false"],
 }
 
 

@@ -80,6 +80,7 @@ struct sa_ctx {
     std::string err;
     LayerConstCache lc;
     PeriodCache pc;
+    DArr<double> red;   // reduction scratch of the optimizer entry points
 };
 
 namespace {
@@ -1066,5 +1067,228 @@ extern "C" int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg,
                               field, w, st));
     // the factor arrays (and an internal work array) are released on return
     SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+
+// ---- optimizer (src/optimize.cpp, src/inversion.cpp:302-323, :465-490) -----------
+
+namespace {
+constexpr int LBFGS_STORE = 5;   // MAX_LBFGS_STORE, include/config.h:90
+
+// Reduction helper: runs on `st`, waits, returns the scalar.
+int reduce_to_host(sa_ctx* ctx, cudaError_t launched, double* scratch, double* out,
+                   cudaStream_t st) {
+    SA_CUDA(launched);
+    SA_CUDA(cudaMemcpyAsync(out, scratch + reduce_scratch_doubles() - 1, sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+}  // namespace
+
+struct sa_lbfgs {
+    sa_ctx* ctx = nullptr;
+    size_t n = 0;
+    // ring of the last LBFGS_STORE + 1 iterates: model (vs) and gradient
+    DArr<double> model[LBFGS_STORE + 1], grad[LBFGS_STORE + 1];
+    int stored_iter[LBFGS_STORE + 1];
+    DArr<double> s[LBFGS_STORE], y[LBFGS_STORE], red;
+};
+
+extern "C" int sa_lbfgs_create(sa_ctx* ctx, size_t n, sa_lbfgs** out) {
+    if (!ctx || !out || n == 0) return SA_ERR_ARG;
+    *out = nullptr;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    sa_lbfgs* L = new sa_lbfgs();
+    L->ctx = ctx;
+    L->n = n;
+    for (int i = 0; i <= LBFGS_STORE; i++) L->stored_iter[i] = -1;
+    cudaError_t e = L->red.alloc(reduce_scratch_doubles());
+    if (e != cudaSuccess) {
+        delete L;
+        return fail(ctx, SA_ERR_NOMEM, "sa_lbfgs_create: device allocation failed");
+    }
+    *out = L;
+    return SA_OK;
+}
+
+extern "C" void sa_lbfgs_destroy(sa_lbfgs* L) {
+    if (!L) return;
+    cudaSetDevice(L->ctx->device);
+    delete L;
+}
+
+extern "C" int sa_lbfgs_store(sa_lbfgs* L, int iter, const double* model, const double* grad) {
+    if (!L) return SA_ERR_ARG;
+    sa_ctx* ctx = L->ctx;
+    if (iter < 0 || !model || !grad) return fail(ctx, SA_ERR_ARG, "sa_lbfgs_store: arguments");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    const int slot = iter % (LBFGS_STORE + 1);
+    SA_CUDA(L->model[slot].alloc(L->n));
+    SA_CUDA(L->grad[slot].alloc(L->n));
+    SA_CUDA(cudaMemcpyAsync(L->model[slot].p, model, L->n * sizeof(double),
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+    SA_CUDA(cudaMemcpyAsync(L->grad[slot].p, grad, L->n * sizeof(double),
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+    SA_CUDA(cudaStreamSynchronize(ctx->stream));
+    L->stored_iter[slot] = iter;
+    return SA_OK;
+}
+
+extern "C" int sa_lbfgs_direction(sa_lbfgs* L, int iter, double* dir) {
+    if (!L) return SA_ERR_ARG;
+    sa_ctx* ctx = L->ctx;
+    if (iter < 0 || !dir) return fail(ctx, SA_ERR_ARG, "sa_lbfgs_direction: arguments");
+    const int nh = std::min(iter, LBFGS_STORE);   // src/optimize.cpp:153-154
+    const int h0 = iter - nh;
+    for (int k = h0; k <= iter; k++)
+        if (L->stored_iter[k % (LBFGS_STORE + 1)] != k)
+            return fail(ctx, SA_ERR_ARG, "sa_lbfgs_direction: iterate " + std::to_string(k) +
+                                             " was not stored");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t n = L->n;
+    auto M = [&](int k) { return L->model[k % (LBFGS_STORE + 1)].p; };
+    auto G = [&](int k) { return L->grad[k % (LBFGS_STORE + 1)].p; };
+    double rho[LBFGS_STORE] = {0}, alpha[LBFGS_STORE] = {0};
+    int rc;
+    for (int h = 0; h < nh; h++) {
+        SA_CUDA(L->s[h].alloc(n));
+        SA_CUDA(L->y[h].alloc(n));
+        SA_CUDA(launch_lbfgs_pair(n, M(h0 + h), M(h0 + h + 1), G(h0 + h), G(h0 + h + 1),
+                                  L->s[h].p, L->y[h].p, st));
+        double sy = 0;
+        if ((rc = reduce_to_host(ctx, launch_dot(n, L->s[h].p, L->y[h].p, L->red.p, st), L->red.p,
+                                 &sy, st)))
+            return rc;
+        rho[h] = (sy > 0.0) ? (1.0 / sy) : 0.0;   // :203
+    }
+    // q <- g_iter
+    SA_CUDA(cudaMemcpyAsync(dir, G(iter), n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    for (int h = nh - 1; h >= 0; --h) {   // :209-214
+        double sq = 0;
+        if ((rc = reduce_to_host(ctx, launch_dot(n, L->s[h].p, dir, L->red.p, st), L->red.p, &sq,
+                                 st)))
+            return rc;
+        alpha[h] = rho[h] * sq;
+        SA_CUDA(launch_axpy(n, 0, alpha[h], L->y[h].p, dir, st));
+    }
+    if (nh > 0) {   // :219-228
+        double yy = 0, sy = 0;
+        const int last = nh - 1;
+        if ((rc = reduce_to_host(ctx, launch_dot(n, L->y[last].p, L->y[last].p, L->red.p, st),
+                                 L->red.p, &yy, st)))
+            return rc;
+        if ((rc = reduce_to_host(ctx, launch_dot(n, L->s[last].p, L->y[last].p, L->red.p, st),
+                                 L->red.p, &sy, st)))
+            return rc;
+        const double gamma = (sy > 0.0 && yy > 0.0) ? (sy / yy) : 1.0;
+        SA_CUDA(launch_axpy(n, 1, gamma, nullptr, dir, st));
+    }
+    for (int h = 0; h < nh; ++h) {   // :231-236
+        double yr = 0;
+        if ((rc = reduce_to_host(ctx, launch_dot(n, L->y[h].p, dir, L->red.p, st), L->red.p, &yr,
+                                 st)))
+            return rc;
+        const double beta = rho[h] * yr;
+        SA_CUDA(launch_axpy(n, 2, alpha[h] - beta, L->s[h].p, dir, st));
+    }
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+
+namespace {
+double* ctx_red(sa_ctx* ctx, int* rc) {
+    cudaError_t e = ctx->red.alloc(reduce_scratch_doubles());
+    *rc = e == cudaSuccess ? SA_OK : fail(ctx, SA_ERR_NOMEM, "reduction scratch");
+    return ctx->red.p;
+}
+}  // namespace
+
+extern "C" int sa_dot(sa_ctx* ctx, size_t n, const double* a, const double* b, double* out) {
+    if (!ctx || !a || !b || !out) return SA_ERR_ARG;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    double* red = ctx_red(ctx, &rc);
+    if (rc) return rc;
+    return reduce_to_host(ctx, launch_dot(n, a, b, red, ctx->stream), red, out, ctx->stream);
+}
+
+extern "C" int sa_grad_normalization(sa_ctx* ctx, size_t n, double* g, double* max_out) {
+    if (!ctx || !g) return SA_ERR_ARG;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    double* red = ctx_red(ctx, &rc);
+    if (rc) return rc;
+    double m = 0;
+    if ((rc = reduce_to_host(ctx, launch_absmax(n, g, red, ctx->stream), red, &m, ctx->stream)))
+        return rc;
+    if (max_out) *max_out = m;
+    if (m < 2.220446049250313e-16) return SA_OK;   // REAL_EPS guard, src/inversion.cpp:316
+    SA_CUDA(launch_axpy(n, 3, m, nullptr, g, ctx->stream));
+    SA_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SA_OK;
+}
+
+extern "C" int sa_descent_angle(sa_ctx* ctx, size_t n, const double* dir, const double* grad,
+                                double* deg) {
+    if (!ctx || !dir || !grad || !deg) return SA_ERR_ARG;
+    double d = 0, gg = 0, dd = 0;
+    int rc;
+    if ((rc = sa_dot(ctx, n, grad, dir, &d))) return rc;
+    if ((rc = sa_dot(ctx, n, grad, grad, &gg))) return rc;
+    if ((rc = sa_dot(ctx, n, dir, dir, &dd))) return rc;
+    const double gn = std::sqrt(gg), dn = std::sqrt(dd);   // src/optimize.cpp:46-47
+    if (gn < 2.220446049250313e-16 || dn < 2.220446049250313e-16) {
+        *deg = 90.0;
+        return SA_OK;
+    }
+    double c = d / (gn * dn);
+    c = std::max(-1.0, std::min(1.0, c));
+    *deg = std::acos(c) * (180.0 / PI_D);
+    return SA_OK;
+}
+
+extern "C" int sa_wolfe_condition(double gd, double kd, double alpha, double* alpha_L,
+                                  double* alpha_R, double f0, double f1, int subiter, double c1,
+                                  double c2, int max_sub_niter, double alpha_init,
+                                  double* next_alpha) {
+    if (!alpha_L || !alpha_R || !next_alpha) return -1;
+    const double q = -gd, q1 = -kd;   // src/optimize.cpp:86-89
+    const bool armijo = f1 <= f0 + alpha * c1 * q;
+    const bool curvature = q1 >= c2 * q;
+    int status;
+    if (armijo && curvature) {
+        status = 0;
+        *next_alpha = alpha;
+    } else if (!armijo) {
+        *alpha_R = alpha;
+        *next_alpha = (*alpha_L + *alpha_R) * 0.5;
+        status = 1;
+    } else {
+        *alpha_L = alpha;
+        const double cand = (*alpha_R > 0.0) ? (*alpha_L + *alpha_R) * 0.5 : alpha * 2.0;
+        if (cand > alpha_init) {
+            *next_alpha = alpha_init;
+            status = 0;
+        } else {
+            *next_alpha = cand;
+            status = 1;
+        }
+    }
+    if (status == 1 && subiter == max_sub_niter - 1) {
+        status = 2;
+        *next_alpha = alpha;
+    }
+    return status;
+}
+
+extern "C" int sa_model_update_vs(sa_ctx* ctx, size_t n, const double* vs, const double* dir,
+                                  double alpha, double* vs_out, double* vp_out, double* rho_out,
+                                  void* stream) {
+    if (!ctx || !vs || !dir || !vs_out) return SA_ERR_ARG;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    SA_CUDA(launch_model_update_vs(n, vs, dir, alpha, vs_out, vp_out, rho_out, st));
     return SA_OK;
 }

@@ -86,6 +86,18 @@ cudaError_t launch_sort_events(int ne, const unsigned int* key_in, unsigned int*
                                cudaStream_t st);
 cudaError_t launch_grad_status(int ncol, const int* colst, const int* ev_worst, int* out,
                                cudaStream_t st);
+// optimize.cu (scratch of reduce_scratch_doubles(); the result lands in its last entry)
+size_t reduce_scratch_doubles();
+cudaError_t launch_dot(size_t n, const double* a, const double* b, double* scratch,
+                       cudaStream_t st);
+cudaError_t launch_absmax(size_t n, const double* a, double* scratch, cudaStream_t st);
+cudaError_t launch_lbfgs_pair(size_t n, const double* m0, const double* m1, const double* g0,
+                              const double* g1, double* s, double* y, cudaStream_t st);
+cudaError_t launch_axpy(size_t n, int kind, double c, const double* x, double* y,
+                        cudaStream_t st);
+cudaError_t launch_model_update_vs(size_t n, const double* vs, const double* dir, double alpha,
+                                   double* vs_out, double* vp_out, double* rho_out,
+                                   cudaStream_t st);
 // postproc.cu
 cudaError_t launch_pde_smooth(int nx, int ny, int nz, double B, double D, const double* rowX,
                               const double* rowY, const double* depE, int nstep, double* field,

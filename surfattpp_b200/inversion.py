@@ -120,3 +120,139 @@ def _fn():
 
     _FN = _Misfit
     return _FN
+
+
+class Inversion:
+    """Inversion::run_inversion (reference src/inversion.cpp:106-160) for one
+    data type (Rayleigh phase), vs-only parametrisation, on the device.
+
+    Per iteration: the forward/adjoint gradient (``MisfitGradient``), kernel
+    smoothing (PostProc::pde_smooth, smooth_method 0) giving
+    gradient = smooth(K) * w / chi, then either steepest descent
+    (src/inversion.cpp:375-394) or L-BFGS with the strong-Wolfe line search
+    and restarts (src/inversion.cpp:396-463, src/optimize.cpp), and the
+    multiplicative model update vs *= (1 - alpha*dir) with Brocher vp, rho.
+    The model and gradient history the reference writes to HDF5 stays on the
+    device (optimize.LBFGS).  Kernel-density preconditioning (is_kden) is not
+    applied.
+    """
+
+    BREAK_ITER = 5          # include/config.h:94
+    MAX_DESC_ANGLE = 92.0   # include/config.h:95
+
+    def __init__(self, grad: MisfitGradient, tt_obs, weight, smooth=None, niter=10,
+                 optim="lbfgs", step_length=0.02, max_sub_niter=10, c1=0.1, c2=0.9,
+                 maxshrink=0.8, min_derr=0.0, data_weight=1.0):
+        """smooth = dict(ygrid, zgrid, dx, dy, dz, sigma_h, sigma_v) or None."""
+        self.g = grad
+        self.tt, self.wt = tt_obs, weight
+        self.smooth = smooth
+        self.niter, self.optim = int(niter), optim
+        self.step_length, self.max_sub_niter = step_length, int(max_sub_niter)
+        self.c1, self.c2, self.maxshrink, self.min_derr = c1, c2, maxshrink, min_derr
+        self.w = data_weight
+        self.misfit, self.alphas, self.sub_iters, self.restarts = [], [], [], 0
+        self._out = None
+
+    def run_forward_adjoint(self, vs):
+        """Inversion::run_forward_adjoint(true) (src/inversion.cpp:245-296):
+        returns (misfit, ker_curr, gradient)."""
+        import torch
+        from . import postproc
+        out = self.g.run(vs, self.tt, self.wt, out=self._out)
+        self._out = out
+        torch.cuda.synchronize()
+        if int(out["status"][0]) != 0:
+            raise _capi.SAError(int(out["status"][0]), "forward/adjoint evaluation failed")
+        chi = float(out["chi"][0])
+        ker = out["ker_vs"]
+        ker_curr = ker * self.w
+        sm = ker.clone()
+        if self.smooth is not None:
+            s = self.smooth
+            postproc.pde_smooth(sm, s["ygrid"], s["zgrid"], s["dx"], s["dy"], s["dz"],
+                                s["sigma_h"], s["sigma_v"])
+        grad = sm * self.w / chi
+        return chi * self.w, ker_curr, grad
+
+    def _check_convergence(self, it):
+        """src/inversion.cpp:212-243."""
+        B = self.BREAK_ITER
+        if it <= B:
+            return False
+        prev = sum(self.misfit[it - 1 - i] for i in range(B + 1)) / B
+        curr = sum(self.misfit[it - i] for i in range(B + 1)) / B
+        red = 100 * (prev - curr) / prev
+        return red < 0 or red < self.min_derr
+
+    MAX_RESTARTS = 8   # a guard: the reference restarts without bound
+
+    def run(self, vs0):
+        """Returns the final model (same shape as vs0)."""
+        from . import optimize as O
+        vs = vs0.detach().clone().contiguous()
+        n = vs.numel()
+        lb = O.LBFGS(n) if self.optim == "lbfgs" else None
+        iter_start = 0
+        alpha = self.step_length
+        for it in range(self.niter):
+            model_it = vs.clone()
+            f0, self._ker, self._grad = self.run_forward_adjoint(vs)
+            self.misfit.append(f0)
+            if lb is not None:
+                lb.store(it, model_it.view(-1), self._grad.view(-1))
+            if self.optim == "sd":
+                d = self._grad.clone().view(-1)
+                O.grad_normalization(d)
+                if it > 0 and self.misfit[it] >= self.misfit[it - 1]:
+                    alpha *= self.maxshrink
+                vs, _, _ = O.model_update_vs(vs.view(-1), d, alpha)
+                vs = vs.view_as(vs0)
+                self.alphas.append(alpha)
+            else:
+                nrs = 0
+                while True:
+                    restart, vs_new, a, nsub = self._line_search(lb, it, iter_start, model_it, f0)
+                    if not restart or nrs >= self.MAX_RESTARTS:
+                        break
+                    iter_start = it
+                    nrs += 1
+                    self.restarts += 1
+                vs = vs_new
+                self.alphas.append(a)
+                self.sub_iters.append(nsub)
+            if self._check_convergence(it):
+                break
+        return vs
+
+    def _line_search(self, lb, it, iter_start, model, f0):
+        """Inversion::line_search (src/inversion.cpp:396-463).  As in the
+        reference, each trial replaces the current kernel and gradient
+        (gradient_, ker_curr_), which a restart then starts from."""
+        from . import optimize as O
+        if it == iter_start:
+            d = self._grad.clone().view(-1)
+        else:
+            d = lb.direction(it)
+        O.grad_normalization(d)
+        if it > iter_start:
+            if O.calc_descent_angle(d, self._grad.view(-1)) > self.MAX_DESC_ANGLE:
+                return True, model, 0.0, 0
+        ker_prev = self._ker
+        gd = O.dot(ker_prev.view(-1), d)
+        alpha, aL, aR = self.step_length, 0.0, 0.0
+        trial = model
+        for sub in range(self.max_sub_niter):
+            trial, _, _ = O.model_update_vs(model.view(-1), d, alpha)
+            trial = trial.view_as(model)
+            f1, self._ker, self._grad = self.run_forward_adjoint(trial)
+            kd = O.dot(self._ker.view(-1), d)
+            st, nxt, aL, aR = O.wolfe_condition(gd, kd, alpha, aL, aR, f0, f1, sub, self.c1,
+                                                self.c2, self.max_sub_niter, self.step_length)
+            if st == O.ACCEPT:
+                return False, trial, alpha, sub + 1
+            if st == O.TRY:
+                alpha = nxt
+                continue
+            return True, trial, alpha, sub + 1
+        return True, trial, alpha, self.max_sub_niter

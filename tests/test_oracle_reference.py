@@ -217,3 +217,26 @@ def test_pde_smooth_nstep_library_matches_oracle(orc):
         assert got == ref
     with pytest.raises(ValueError):
         postproc.pde_smooth_nstep(y, 0.05, 0.05, 2.0, -1.0, 4.0)
+
+
+def test_wolfe_condition_library_matches_oracle(orc):
+    """optimize::wolfe_condition (src/optimize.cpp:74-145): the library's host
+    function and the oracle agree on status, next step and bracket over a grid
+    of cases covering accept / shrink / widen / cap / last-sub-iteration fail."""
+    from surfattpp_b200 import optimize
+    rng = np.random.default_rng(4)
+    n = 0
+    for _ in range(400):
+        gd = rng.uniform(0.1, 2.0)
+        kd = gd * rng.uniform(-0.5, 1.5)
+        alpha = rng.choice([0.005, 0.01, 0.02, 0.04])
+        aL = rng.choice([0.0, 0.005])
+        aR = rng.choice([0.0, 0.03])
+        f0 = 10.0
+        f1 = f0 + rng.uniform(-0.05, 0.05)
+        sub = int(rng.integers(0, 10))
+        a = optimize.wolfe_condition(gd, kd, alpha, aL, aR, f0, f1, sub, 0.1, 0.9, 10, 0.02)
+        b = orc.wolfe_condition(gd, kd, alpha, aL, aR, f0, f1, sub, 0.1, 0.9, 10, 0.02)
+        assert a == b
+        n += a[0] == 2
+    assert n > 0
