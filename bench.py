@@ -272,6 +272,28 @@ def pde_smooth_timing(a, w, dev, stream, peak):
                     "field %.0f MB" % (f.numel() * 8 / 1e6)}
 
 
+def topo_media_timing(dev, stream):
+    """SurfGrid::build_media_matrix_with_topo on the 201 x 201 topography
+    level: gridding, then per period the geographic Gaussian smoothing,
+    gradient, dip angle and media (15 periods)."""
+    import torch
+    from surfattpp_b200 import surfgrid
+    from surfattpp_b200 import workloads as W
+    w = W.config4(level=201, nsta=41, src_range=(3, 5), lam=4.0)
+    lon, lat, z = w.meta["topo_raw"]
+    avg = surfgrid.average_phase_velocity(w.zgrid, w.meta["vs1d"], w.periods)
+    sig = surfgrid.sigma_deg(avg, w.periods, w.meta["wavelen_factor"])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    zg = surfgrid.grid_topography(lon, lat, z, w.xx_deg, w.yy_deg)
+    surfgrid.build_media_with_topo(w.xx_deg, w.yy_deg, zg, sig, stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return {"grid": [w.nx, w.ny], "periods": int(w.nper), "sigma_deg_range": [float(sig.min()),
+            float(sig.max())], "ms_total": e0.elapsed_time(e1)}
+
+
 def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx):
     """The same solves with the FP64 parity path (the reference's arithmetic)."""
     from surfattpp_b200 import preproc
@@ -401,6 +423,7 @@ def main():
         extra["misfit_gradient"] = misfit_gradient_timing(a, w, plan, tt, wt, dev, stream)
         extra["fp64_plain"] = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx)
         extra["pde_smooth"] = pde_smooth_timing(a, w, dev, stream, peaks()[0])
+        extra["topo_media"] = topo_media_timing(dev, stream)
 
     if rank == 0:
         peak, peak_kind = peaks()

@@ -192,6 +192,39 @@ int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg, double dy_
                   double dz_km, const double* ygrid, const double* zgrid, double sigma_h,
                   double sigma_v, double* field, double* work, int* nstep_out, void* stream);
 
+/* ---- topography media (config with topography) ----------------------------- */
+
+/* Topography::grid (reference src/topo.cpp:46-95): interp2d of a raw
+ * topography z_raw (column-major nx_raw x ny_raw, km; host) onto the model
+ * grid x[nx], y[ny] (host) -> z_out (device, column-major nx x ny).
+ * SA_ERR_ARG when the model grid extends beyond the topography (the
+ * reference aborts). */
+int sa_grid_topography(sa_ctx* ctx, int nx_raw, int ny_raw, const double* lon_raw,
+                       const double* lat_raw, const double* z_raw, int nx, int ny,
+                       const double* x, const double* y, double* z_out);
+
+/* The per-period loop of SurfGrid::build_media_matrix_with_topo
+ * (src/surf_grid.cpp:80-166): for each period, gaussian_smooth_geo_2 of the
+ * gridded topography with sigma_deg[iper] (include/utils.h:505-571), its
+ * geographic gradient (gradient_2_geo, :593-649), the dip angle
+ * (src/topo.cpp:97-114) and the media m11 = a, m12 = -c, m22 = b
+ * (src/surf_grid.cpp:185-190).  z_gridded (device, column-major nx x ny);
+ * lon[nx], lat[ny], sigma_deg[nper] host; outputs (device) [nper][ny][nx],
+ * angle in degrees.  The caller forms sigma_deg = c_avg * T * wavelen_factor
+ * / (2 pi) / (R_EARTH * DEG2RAD) (:116-119). */
+int sa_topo_media(sa_ctx* ctx, int nx, int ny, const double* lon, const double* lat,
+                  const double* z_gridded, int nper, const double* sigma_deg, double* m11,
+                  double* m12, double* m22, double* angle, void* stream);
+
+/* SurfGrid::correct_depth_with_topo (src/surf_grid.cpp:307-354): each depth
+ * kernel column (ix, iy, iper) resampled at zgrid / cos(dip), clamped to the
+ * depth range (interp1d, include/utils.h:451-485).  sen_* (device, may be
+ * NULL) are (nx, ny, nz, nper) row-major, in place; angle [nper][ny][nx]
+ * (device, degrees); zgrid[nz] host, nz <= 64. */
+int sa_correct_depth_with_topo(sa_ctx* ctx, int nx, int ny, int nz, int nper, const double* zgrid,
+                               const double* angle, double* sen_vs, double* sen_vp,
+                               double* sen_rho, void* stream);
+
 /* ---- optimizer: L-BFGS, strong Wolfe, model update (vs-only) --------------- */
 
 /* History of the last 6 iterates (model vs and gradient, n values each, kept

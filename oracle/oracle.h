@@ -149,6 +149,19 @@ void orc_model_update_vs(size_t n, const double* vs, const double* dir, double a
 double orc_vs2vp(double vs);
 double orc_vp2rho(double vp);
 
+/* Topography (src/surf_grid.cpp:80-166, :307-354; include/utils.h:505-649;
+ * src/topo.cpp:97-114).  2-D fields column-major nx x ny; per-period outputs
+ * [nper][ny][nx]; ker (nx, ny, nz, nper) row-major, corrected in place. */
+void orc_gaussian_smooth_geo_2(int nx, int ny, const double* data, const double* lons,
+                               const double* lats, double sigma, double* out);
+void orc_gradient_2_geo(int nx, int ny, const double* f, const double* lon, const double* lat,
+                        double* tx, double* ty);
+void orc_topo_media(int nx, int ny, const double* lon, const double* lat,
+                    const double* z_gridded, int nper, const double* sigma_deg, double* m11,
+                    double* m12, double* m22, double* angle);
+void orc_correct_depth_with_topo(int nx, int ny, int nz, int nper, const double* zgrid,
+                                 const double* angle, double* ker);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,10 @@ def lib():
                                       C.POINTER(d)]
     L.orc_wolfe_condition.restype = i
     L.orc_model_update_vs.argtypes = [z, _dp, _dp, d, _dp, _dp, _dp]
+    L.orc_gaussian_smooth_geo_2.argtypes = [i, i, _dp, _dp, _dp, d, _dp]
+    L.orc_gradient_2_geo.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp]
+    L.orc_topo_media.argtypes = [i, i, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]
+    L.orc_correct_depth_with_topo.argtypes = [i, i, i, i, _dp, _dp, _dp]
     _lib = L
     return L
 
@@ -272,3 +276,39 @@ def model_update_vs(vs, direction, alpha):
     o1, o2, o3 = np.zeros(n), np.zeros(n), np.zeros(n)
     lib().orc_model_update_vs(n, v, _c(direction).ravel(), alpha, o1, o2, o3)
     return o1, o2, o3
+
+
+def gaussian_smooth_geo_2(data, lons, lats, sigma):
+    """data (ny, nx) planes as elsewhere in this module ([iy][ix])."""
+    d = _c(data)
+    ny, nx = d.shape
+    out = np.zeros((ny, nx))
+    lib().orc_gaussian_smooth_geo_2(nx, ny, d, _c(lons), _c(lats), float(sigma), out)
+    return out
+
+
+def gradient_2_geo(f, lon, lat):
+    d = _c(f)
+    ny, nx = d.shape
+    tx, ty = np.zeros((ny, nx)), np.zeros((ny, nx))
+    lib().orc_gradient_2_geo(nx, ny, d, _c(lon), _c(lat), tx, ty)
+    return tx, ty
+
+
+def topo_media(lon, lat, z_gridded, sigma_deg):
+    """Per-period media (m11, m12, m22, angle), each (nper, ny, nx)."""
+    z = _c(z_gridded)
+    ny, nx = z.shape
+    s = _c(sigma_deg).ravel()
+    shp = (s.size, ny, nx)
+    m11, m12, m22, ang = np.zeros(shp), np.zeros(shp), np.zeros(shp), np.zeros(shp)
+    lib().orc_topo_media(nx, ny, _c(lon), _c(lat), z, s.size, s, m11, m12, m22, ang)
+    return m11, m12, m22, ang
+
+
+def correct_depth_with_topo(zgrid, angle, ker):
+    """ker (nx, ny, nz, nper) corrected copy; angle (nper, ny, nx)."""
+    k = _c(ker).copy()
+    nx, ny, nz, nper = k.shape
+    lib().orc_correct_depth_with_topo(nx, ny, nz, nper, _c(zgrid), _c(angle), k)
+    return k

@@ -31,6 +31,7 @@ EXPORTED = (
     "sa_pde_smooth_nstep", "sa_pde_smooth",
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
     "sa_grad_normalization", "sa_descent_angle", "sa_wolfe_condition", "sa_model_update_vs",
+    "sa_grid_topography", "sa_topo_media", "sa_correct_depth_with_topo",
 )
 
 
@@ -102,6 +103,9 @@ def lib():
     L.sa_wolfe_condition.argtypes = [d, d, d, C.POINTER(d), C.POINTER(d), d, d, i, d, d, i, d,
                                      C.POINTER(d)]
     L.sa_model_update_vs.argtypes = [_vp, z, _vp, _vp, d, _vp, _vp, _vp, _vp]
+    L.sa_grid_topography.argtypes = [_vp, i, i, _dp, _dp, _dp, i, i, _dp, _dp, _vp]
+    L.sa_topo_media.argtypes = [_vp, i, i, _dp, _dp, _vp, i, _dp, _vp, _vp, _vp, _vp, _vp]
+    L.sa_correct_depth_with_topo.argtypes = [_vp, i, i, i, i, _dp, _vp, _vp, _vp, _vp, _vp]
     L.sa_pde_smooth.argtypes = [_vp, i, i, i, d, d, d, _dp, _dp, d, d, _vp, _vp, C.POINTER(i),
                                 _vp]
     _lib = L

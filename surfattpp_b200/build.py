@@ -31,6 +31,7 @@ UNITS = {
     "noalloc.cu": [],
     "postproc.cu": ["-fmad=false"],
     "optimize.cu": ["-fmad=false"],
+    "topo.cu": ["-fmad=false"],
 }
 
 

@@ -1292,3 +1292,76 @@ extern "C" int sa_model_update_vs(sa_ctx* ctx, size_t n, const double* vs, const
     SA_CUDA(launch_model_update_vs(n, vs, dir, alpha, vs_out, vp_out, rho_out, st));
     return SA_OK;
 }
+
+// ---- topography (src/surf_grid.cpp:80-166, :307-354; src/topo.cpp:46-114) -------
+
+extern "C" int sa_grid_topography(sa_ctx* ctx, int nx_raw, int ny_raw, const double* lon_raw,
+                                  const double* lat_raw, const double* z_raw, int nx, int ny,
+                                  const double* x, const double* y, double* z_out) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx_raw < 2 || ny_raw < 2 || nx < 2 || ny < 2 || !lon_raw || !lat_raw || !z_raw || !x ||
+        !y || !z_out)
+        return fail(ctx, SA_ERR_ARG, "sa_grid_topography: bad sizes or null pointers");
+    // Topography::check_bounds (src/topo.cpp:68-95)
+    const double lo0 = *std::min_element(lon_raw, lon_raw + nx_raw);
+    const double lo1 = *std::max_element(lon_raw, lon_raw + nx_raw);
+    const double la0 = *std::min_element(lat_raw, lat_raw + ny_raw);
+    const double la1 = *std::max_element(lat_raw, lat_raw + ny_raw);
+    if (*std::min_element(x, x + nx) < lo0 || *std::max_element(x, x + nx) > lo1 ||
+        *std::min_element(y, y + ny) < la0 || *std::max_element(y, y + ny) > la1)
+        return fail(ctx, SA_ERR_ARG, "Model grid extends beyond topography bounds");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    DArr<double> dxr, dyr, dzr, dx, dy;
+    SA_CUDA(dxr.upload(lon_raw, nx_raw, st));
+    SA_CUDA(dyr.upload(lat_raw, ny_raw, st));
+    SA_CUDA(dzr.upload(z_raw, (size_t)nx_raw * ny_raw, st));
+    SA_CUDA(dx.upload(x, nx, st));
+    SA_CUDA(dy.upload(y, ny, st));
+    SA_CUDA(launch_grid_topo(nx_raw, ny_raw, dxr.p, dyr.p, dzr.p, nx, ny, dx.p, dy.p, z_out, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+
+extern "C" int sa_topo_media(sa_ctx* ctx, int nx, int ny, const double* lon, const double* lat,
+                             const double* z_gridded, int nper, const double* sigma_deg,
+                             double* m11, double* m12, double* m22, double* angle,
+                             void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 3 || ny < 3 || nper < 1 || !lon || !lat || !z_gridded || !sigma_deg || !m11 ||
+        !m12 || !m22 || !angle)
+        return fail(ctx, SA_ERR_ARG, "sa_topo_media: bad sizes or null pointers");
+    for (int ip = 0; ip < nper; ip++)
+        if (!(sigma_deg[ip] > 0.0)) return fail(ctx, SA_ERR_ARG, "sa_topo_media: sigma <= 0");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const size_t n = (size_t)nx * ny;
+    DArr<double> dlon, dlat, zs;
+    SA_CUDA(dlon.upload(lon, nx, st));
+    SA_CUDA(dlat.upload(lat, ny, st));
+    SA_CUDA(zs.alloc(n));
+    for (int ip = 0; ip < nper; ip++) {
+        // each period starts from the unsmoothed gridded topography (:93-96, :113-114)
+        SA_CUDA(launch_gauss_geo(nx, ny, z_gridded, dlon.p, dlat.p, sigma_deg[ip], zs.p, st));
+        SA_CUDA(launch_topo_media(nx, ny, zs.p, dlon.p, dlat.p, m11 + ip * n, m12 + ip * n,
+                                  m22 + ip * n, angle + ip * n, st));
+    }
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}
+
+extern "C" int sa_correct_depth_with_topo(sa_ctx* ctx, int nx, int ny, int nz, int nper,
+                                          const double* zgrid, const double* angle,
+                                          double* sen_vs, double* sen_vp, double* sen_rho,
+                                          void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 1 || ny < 1 || nz < 2 || nz > 64 || nper < 1 || !zgrid || !angle)
+        return fail(ctx, SA_ERR_ARG, "sa_correct_depth_with_topo: bad sizes (2 <= nz <= 64)");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    DArr<double> dz;
+    SA_CUDA(dz.upload(zgrid, nz, st));
+    SA_CUDA(launch_depth_topo(nx, ny, nz, nper, dz.p, angle, sen_vs, sen_vp, sen_rho, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    return SA_OK;
+}

@@ -98,6 +98,18 @@ cudaError_t launch_axpy(size_t n, int kind, double c, const double* x, double* y
 cudaError_t launch_model_update_vs(size_t n, const double* vs, const double* dir, double alpha,
                                    double* vs_out, double* vp_out, double* rho_out,
                                    cudaStream_t st);
+// topo.cu
+cudaError_t launch_gauss_geo(int nx, int ny, const double* data, const double* lons,
+                             const double* lats, double sigma, double* out, cudaStream_t st);
+cudaError_t launch_topo_media(int nx, int ny, const double* z, const double* lon,
+                              const double* lat, double* m11, double* m12, double* m22,
+                              double* angle, cudaStream_t st);
+cudaError_t launch_depth_topo(int nx, int ny, int nz, int nper, const double* zg,
+                              const double* angle, double* k0, double* k1, double* k2,
+                              cudaStream_t st);
+cudaError_t launch_grid_topo(int nxr, int nyr, const double* xr, const double* yr,
+                             const double* zr, int nx, int ny, const double* x, const double* y,
+                             double* out, cudaStream_t st);
 // postproc.cu
 cudaError_t launch_pde_smooth(int nx, int ny, int nz, double B, double D, const double* rowX,
                               const double* rowY, const double* depE, int nstep, double* field,

@@ -193,6 +193,65 @@ def config3(seed=1003, nsta=400, nper=20, n=301):
                     iper, ptr, idx, tt, np.ones(idx.size), meta=dict(vs_start=vs0))
 
 
+def fractal_topography(rng, lon, lat, relief_km=4.0, slope=-2.0):
+    """Seeded fractal surface on a lon/lat grid: power spectrum ~ k^slope
+    (FFT-filtered white noise), scaled to [0, relief_km].  Returns (nlat, nlon)."""
+    nlat, nlon = lat.size, lon.size
+    noise = rng.standard_normal((nlat, nlon))
+    ky = np.fft.fftfreq(nlat)[:, None]
+    kx = np.fft.fftfreq(nlon)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    k[0, 0] = 1.0
+    amp = k ** (slope / 2.0)
+    amp[0, 0] = 0.0
+    z = np.real(np.fft.ifft2(np.fft.fft2(noise) * amp))
+    z = (z - z.min()) / (z.max() - z.min())
+    return relief_km * z
+
+
+def config4(level=101, seed=1004, nsta=601, nper=15, lam=40.0, src_range=(50, 600),
+            span_deg=2.0, wavelen_factor=2.5):
+    """Topography case: level x level grid over a fixed span (101, 201 or 401
+    nodes), fractal topography with 0-4 km relief and spectral slope -2, 15
+    periods 4-40 s; per period a U{50..600} set of sources, each with a
+    Poisson(lam) set of receivers (capped at nsta - 1).  The raw topography
+    (0.005 deg, a margin beyond the model) is in meta["topo_raw"]."""
+    rng = np.random.default_rng(seed)
+    d = span_deg / (level - 1)
+    xx, yy = _grid(102.0, 24.0, (level, level), d)
+    z = np.arange(0.0, 58.0 + 1e-9, 2.0)
+    vs = add_checker(gradient_model(level, level, z), 0.05, 2, 2, 2)
+    periods = np.geomspace(4.0, 40.0, nper)
+    stlo, stla = _stations(rng, xx, yy, nsta)
+    evlo, evla, iper, ptr, idx = [], [], [], [0], []
+    for ip in range(nper):
+        ns = int(rng.integers(src_range[0], min(src_range[1], nsta) + 1))
+        for s in rng.choice(nsta, size=ns, replace=False):
+            nr = int(min(max(rng.poisson(lam), 1), nsta - 1))
+            others = np.delete(np.arange(nsta), s)
+            rec = np.sort(rng.choice(others, size=nr, replace=False))
+            evlo.append(stlo[s])
+            evla.append(stla[s])
+            iper.append(ip)
+            idx.extend(rec.tolist())
+            ptr.append(len(idx))
+    evlo, evla = np.array(evlo), np.array(evla)
+    iper = np.array(iper, np.int32)
+    ptr, idx = np.array(ptr, np.int32), np.array(idx, np.int32)
+    cref = 2.9 + 0.9 * (np.log(periods) - np.log(4.0)) / (np.log(40.0) - np.log(4.0))
+    ev_of = np.repeat(np.arange(evlo.size), np.diff(ptr))
+    dist = _gc_km(evlo[ev_of], evla[ev_of], stlo[idx], stla[idx])
+    tt = dist / cref[iper[ev_of]] * (1.0 + 0.02 * rng.standard_normal(idx.size))
+    lon_raw = np.arange(101.8, 102.0 + span_deg + 0.2 + 1e-9, 0.005)
+    lat_raw = np.arange(23.8, 24.0 + span_deg + 0.2 + 1e-9, 0.005)
+    topo = fractal_topography(rng, lon_raw, lat_raw)
+    return Workload(f"C4 topography {level}x{level}x{z.size}, {nper} periods, "
+                    f"{evlo.size} solves", xx, yy, z, vs, periods, stlo, stla, evlo, evla, iper,
+                    ptr, idx, tt, np.ones(idx.size),
+                    meta=dict(topo_raw=(lon_raw, lat_raw, topo), wavelen_factor=wavelen_factor,
+                              vs1d=vs.mean(axis=(0, 1))))
+
+
 def _gc_km(lo1, la1, lo2, la2):
     r = np.pi / 180.0
     c = (np.sin(la1 * r) * np.sin(la2 * r)
