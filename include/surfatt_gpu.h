@@ -192,6 +192,34 @@ int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg, double dy_
                   double dz_km, const double* ygrid, const double* zgrid, double sigma_h,
                   double sigma_v, double* field, double* work, int* nstep_out, void* stream);
 
+/* ---- observation table and event builder (host only) ----------------------- */
+
+/* SrcRec::load with get_periods and get_events (reference src/src_rec.cpp:20-228,
+ * :232-264): reads the CSV (columns tt, staname, stla, stlo, evtname, evla,
+ * evlo, period, optional weight / dist / vel, which default to 1, the
+ * great-circle distance (include/utils.h:287-299) and dist / tt), builds the
+ * sorted unique periods with their mean velocities and one event per
+ * (evtname, period) holding its observation rows, ordered as the reference's
+ * events map ("{evtname}_{iper}" keys).  The event arrays feed
+ * sa_plan_create with the per-observation station coordinates as stations
+ * (rec_idx = observation rows).  SA_ERR_ARG for a missing file or column. */
+typedef struct sa_srcrec sa_srcrec;
+int sa_srcrec_load(const char* csv_path, sa_srcrec** out);
+void sa_srcrec_destroy(sa_srcrec* sr);
+int sa_srcrec_sizes(const sa_srcrec* sr, int* n_obs, int* nperiod, int* n_events);
+int sa_srcrec_periods(const sa_srcrec* sr, double* periods, double* meanvel,
+                      int* n_obs_per_period);
+int sa_srcrec_observations(const sa_srcrec* sr, double* stlo, double* stla, double* tt,
+                           double* weight, double* dist, double* vel, double* period);
+/* evlo, evla, iper [n_events]; rec_ptr [n_events + 1]; rec_idx [rec_ptr[n_events]]. */
+int sa_srcrec_events(const sa_srcrec* sr, double* evlo, double* evla, int* iper, int* rec_ptr,
+                     int* rec_idx);
+const char* sa_srcrec_event_name(const sa_srcrec* sr, int event);
+/* SrcRec::write (src/src_rec.cpp:407-457): the observed table, or with
+ * tt_fwd[n_obs] the forward times and dist / tt_fwd velocities
+ * (gather_syn_tt, :326-371). */
+int sa_srcrec_write(const sa_srcrec* sr, const char* csv_path, const double* tt_fwd);
+
 /* ---- topography media (config with topography) ----------------------------- */
 
 /* Topography::grid (reference src/topo.cpp:46-95): interp2d of a raw

@@ -32,6 +32,8 @@ EXPORTED = (
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
     "sa_grad_normalization", "sa_descent_angle", "sa_wolfe_condition", "sa_model_update_vs",
     "sa_grid_topography", "sa_topo_media", "sa_correct_depth_with_topo",
+    "sa_srcrec_load", "sa_srcrec_destroy", "sa_srcrec_sizes", "sa_srcrec_periods",
+    "sa_srcrec_observations", "sa_srcrec_events", "sa_srcrec_event_name", "sa_srcrec_write",
 )
 
 
@@ -103,6 +105,15 @@ def lib():
     L.sa_wolfe_condition.argtypes = [d, d, d, C.POINTER(d), C.POINTER(d), d, d, i, d, d, i, d,
                                      C.POINTER(d)]
     L.sa_model_update_vs.argtypes = [_vp, z, _vp, _vp, d, _vp, _vp, _vp, _vp]
+    L.sa_srcrec_load.argtypes = [C.c_char_p, C.POINTER(_vp)]
+    L.sa_srcrec_destroy.argtypes = [_vp]
+    L.sa_srcrec_sizes.argtypes = [_vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.sa_srcrec_periods.argtypes = [_vp, _vp, _vp, _vp]
+    L.sa_srcrec_observations.argtypes = [_vp] + [_vp] * 7
+    L.sa_srcrec_events.argtypes = [_vp] + [_vp] * 5
+    L.sa_srcrec_event_name.argtypes = [_vp, i]
+    L.sa_srcrec_event_name.restype = C.c_char_p
+    L.sa_srcrec_write.argtypes = [_vp, C.c_char_p, _vp]
     L.sa_grid_topography.argtypes = [_vp, i, i, _dp, _dp, _dp, i, i, _dp, _dp, _vp]
     L.sa_topo_media.argtypes = [_vp, i, i, _dp, _dp, _vp, i, _dp, _vp, _vp, _vp, _vp, _vp]
     L.sa_correct_depth_with_topo.argtypes = [_vp, i, i, i, i, _dp, _vp, _vp, _vp, _vp, _vp]

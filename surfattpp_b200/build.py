@@ -32,6 +32,7 @@ UNITS = {
     "postproc.cu": ["-fmad=false"],
     "optimize.cu": ["-fmad=false"],
     "topo.cu": ["-fmad=false"],
+    "srcrec.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }
 
 
@@ -64,7 +65,7 @@ def build(verbose: bool = False, force: bool = False, defines: list[str] | None 
         src = os.path.join(CSRC, unit)
         if not os.path.exists(src):
             continue
-        obj = os.path.join(bdir, unit.replace(".cu", ".o"))
+        obj = os.path.join(bdir, unit.rsplit(".", 1)[0] + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
             cmd = [nvcc()] + ARCH + COMMON + dflags + flags + ["-c", src, "-o", obj]
