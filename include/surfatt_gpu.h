@@ -160,6 +160,19 @@ int sa_depthkernel_columns(sa_ctx* ctx, int nx, int ny, int nz, const double* zg
                            const double* cp, double* sen_vs, double* sen_vp, double* sen_rho,
                            void* stream);
 
+/* Replaces the column loop of SurfGrid::compute_dispersion_kernel for group
+ * velocity (src/surf_grid.cpp:247-305, itype 1) through
+ * surfker::depthkernel_rayleigh_group (src/surfdisp.cpp:203-285) and sregnpu
+ * (src/surfker/sregn96.f90:1851-1992): phase velocities at t and t(1 +- 0.005)
+ * (three surfdisp96 runs per column), then per (column, period) the group
+ * kernels dU/dvs, dU/dvp, dU/drho.  sen_* (device) (nx, ny, nz, nper);
+ * status (HOST, ny*nx ints, may be NULL): nonzero where a root search failed;
+ * the call then returns SA_ERR_NOROOT.  Synchronous on `stream`. */
+int sa_depthkernel_columns_group(sa_ctx* ctx, int nx, int ny, int nz, const double* zgrid,
+                                 const double* vs3d, int nper, const double* periods,
+                                 double* sen_vs, double* sen_vp, double* sen_rho, int* status,
+                                 void* stream);
+
 /* Replaces preproc::combine_kernels, vs-only parametrisation
  * (src/preproc.cpp:276-304): ker_vs(ix,iy,k) = -sum_iper adj_s(iper,ix,iy) *
  * (sen_vs + sen_vp*dVp/dVs + sen_rho*drho/dVp*dVp/dVs), periods in order.

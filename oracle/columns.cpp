@@ -106,3 +106,47 @@ extern "C" int orc_depthkernel_hti(int nx, int ny, int nz, const double* zgrid,
     });
     return 0;
 }
+
+// surfker::depthkernel_rayleigh_group (src/surfdisp.cpp:203-285) per column:
+// phase velocities at t, t(1 + 0.005) and t(1 - 0.005), then sregnpu.
+extern "C" int orc_depthkernel_group(int nx, int ny, int nz, const double* zgrid,
+                                     const double* vs3d, int nper, const double* periods,
+                                     double* sen_vs, double* sen_vp, double* sen_rho,
+                                     int* status, int nthreads) {
+    const int ncol = nx * ny;
+    const int mmax = nz + 1;
+    const double dt = 0.01;
+    std::vector<double> t1(nper), t2(nper);
+    for (int i = 0; i < nper; ++i) {
+        t1[i] = periods[i] * (1.0 + 0.5 * dt);
+        t2[i] = periods[i] * (1.0 - 0.5 * dt);
+    }
+    for_columns(ncol, nthreads, [&](int col) {
+        const int ix = col / ny, iy = col % ny;
+        std::vector<float> thk, vp, vs, rho;
+        build_layers(nz, zgrid, vs3d + static_cast<size_t>(col) * nz, thk, vp, vs, rho);
+        std::vector<double> cp(nper, 0.0), cp1(nper, 0.0), cp2(nper, 0.0);
+        int st = orc_surfdisp96(thk.data(), vp.data(), vs.data(), rho.data(), mmax, 1, 2, 1, 0,
+                                nper, periods, cp.data());
+        st |= orc_surfdisp96(thk.data(), vp.data(), vs.data(), rho.data(), mmax, 1, 2, 1, 0,
+                             nper, t1.data(), cp1.data());
+        st |= orc_surfdisp96(thk.data(), vp.data(), vs.data(), rho.data(), mmax, 1, 2, 1, 0,
+                             nper, t2.data(), cp2.data());
+        if (status) status[ix + nx * iy] = st;
+        std::vector<double> ua(mmax), ub(mmax), uh(mmax), ur(mmax), ca(mmax), cb(mmax),
+            ch(mmax), cr(mmax);
+        for (int ip = 0; ip < nper; ip++) {
+            double cg = 0.0;
+            orc_sregnpu(thk.data(), vp.data(), vs.data(), rho.data(), mmax, periods[ip], cp[ip],
+                        t1[ip], cp1[ip], t2[ip], cp2[ip], &cg, ua.data(), ub.data(), uh.data(),
+                        ur.data(), ca.data(), cb.data(), ch.data(), cr.data(), 1);
+            for (int k = 0; k < nz; k++) {
+                const size_t i4 = ((static_cast<size_t>(col)) * nz + k) * nper + ip;
+                sen_vs[i4] = ub[k];
+                sen_vp[i4] = ua[k];
+                sen_rho[i4] = ur[k];
+            }
+        }
+    });
+    return 0;
+}

@@ -162,6 +162,17 @@ void orc_topo_media(int nx, int ny, const double* lon, const double* lat,
 void orc_correct_depth_with_topo(int nx, int ny, int nz, int nper, const double* zgrid,
                                  const double* angle, double* ker);
 
+/* sregnpu (src/surfker/sregn96.f90:1851-1992) and the per-column Rayleigh
+ * group-velocity depth kernels (surfker::depthkernel_rayleigh_group,
+ * src/surfdisp.cpp:203-285); outputs as orc_depthkernel_hti. */
+void orc_sregnpu(const float* thk, const float* vp, const float* vs, const float* rhom,
+                 int nlayer, double t, double cp, double t1, double cp1, double t2, double cp2,
+                 double* cg, double* du2da, double* du2db, double* du2dh, double* du2dr,
+                 double* dc2da, double* dc2db, double* dc2dh, double* dc2dr, int iflsph);
+int orc_depthkernel_group(int nx, int ny, int nz, const double* zgrid, const double* vs3d,
+                          int nper, const double* periods, double* sen_vs, double* sen_vp,
+                          double* sen_rho, int* status, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,8 @@ def lib():
                                       C.POINTER(d)]
     L.orc_wolfe_condition.restype = i
     L.orc_model_update_vs.argtypes = [z, _dp, _dp, d, _dp, _dp, _dp]
+    L.orc_depthkernel_group.argtypes = [i, i, i, _dp, _dp, i, _dp, _dp, _dp, _dp, _ip, i]
+    L.orc_sregnpu.argtypes = [_fp, _fp, _fp, _fp, i, d, d, d, d, d, d, C.POINTER(d)] + [_dp] * 8 + [i]
     L.orc_gaussian_smooth_geo_2.argtypes = [i, i, _dp, _dp, _dp, d, _dp]
     L.orc_gradient_2_geo.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp]
     L.orc_topo_media.argtypes = [i, i, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]
@@ -312,3 +314,15 @@ def correct_depth_with_topo(zgrid, angle, ker):
     nx, ny, nz, nper = k.shape
     lib().orc_correct_depth_with_topo(nx, ny, nz, nper, _c(zgrid), _c(angle), k)
     return k
+
+
+def depthkernel_group(zgrid, vs3d, periods, nthreads=1):
+    """Rayleigh group-velocity depth kernels: sen_vs, sen_vp, sen_rho (nx,ny,nz,nper), status."""
+    nx, ny, nz = vs3d.shape
+    p = _c(periods)
+    shp = (nx, ny, nz, p.size)
+    sv, sp, sr = np.zeros(shp), np.zeros(shp), np.zeros(shp)
+    st = np.zeros((ny, nx), np.int32)
+    lib().orc_depthkernel_group(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
+                                int(nthreads))
+    return sv, sp, sr, st

@@ -869,6 +869,128 @@ void run_sregn(const float* thk, const float* vp, const float* vs, const float* 
     *cg = usph;
 }
 
+
+// sregnpu (sregn96.f90:1851-1992): Rayleigh group-velocity kernels from the
+// phase kernels at t, t1 and t2 (finite difference in period).
+void run_sregnpu(const float* thk, const float* vp, const float* vs, const float* rhom,
+                 int nlayer, double t, double cp, double t1, double cp1, double t2, double cp2,
+                 double* cg_out, double* du2da, double* du2db, double* du2dh, double* du2dr,
+                 double* dc2da, double* dc2db, double* dc2dh, double* dc2dr, int iflsph) {
+    RW W;
+    const int mmax = nlayer;
+    W.mmax = mmax;
+    for (auto* v : {&W.zd, &W.zrho, &W.za, &W.zb, &W.xmu, &W.xlam}) v->assign(mmax, 0.0);
+    for (auto* v : {&W.ur, &W.uz, &W.tz, &W.tr, &W.dcda, &W.dcdb, &W.dcdr, &W.dcdh, &W.dcdgc,
+                    &W.dcdgs, &W.exe, &W.exa})
+        v->assign(mmax, 0.0);
+    W.iwat.assign(mmax, 0);
+    W.cd.assign(static_cast<size_t>(mmax) * 5, 0.0);
+    W.vv.assign(static_cast<size_t>(mmax) * 4, 0.0);
+    for (int i = 0; i < mmax; i++) {
+        W.zb[i] = vs[i];
+        W.za[i] = vp[i];
+        W.zrho[i] = rhom[i];
+        W.zd[i] = thk[i];
+    }
+    W.allfluid = true;
+    for (int i = 0; i < mmax; i++) {
+        if (W.zb[i] > 0.0) {
+            W.allfluid = false;
+            W.iwat[i] = 0;
+        } else {
+            W.iwat[i] = 1;
+        }
+    }
+    const int nsph = iflsph;
+    if (nsph > 0) {
+        W.vtp.assign(mmax, 0.0);
+        W.dtp.assign(mmax, 0.0);
+        W.rtp.assign(mmax, 0.0);
+        bldsph(W);
+    }
+    for (int i = 0; i < mmax; i++) {
+        W.xmu[i] = W.zrho[i] * (W.zb[i] * W.zb[i]);
+        W.xlam[i] = W.zrho[i] * (W.za[i] * W.za[i]) - 2.0 * W.xmu[i];
+    }
+    const double pi = 3.1415926535897932384626433832795;
+    const double twopi = 2.0 * pi;
+    std::vector<double> da1(mmax), db1(mmax), dr1(mmax), dh1(mmax), da2(mmax), db2(mmax),
+        dr2(mmax), dh2(mmax);
+    // period t (:1908-1918)
+    double omega = twopi / t;
+    double wvno = omega / cp;
+    svfunc(W, omega, wvno);
+    energy(W, omega, wvno);
+    double cg = W.ugr;
+    for (int i = 0; i < mmax; i++) {
+        dc2da[i] = W.dcda[i];
+        dc2db[i] = W.dcdb[i];
+        dc2dr[i] = W.dcdr[i];
+        dc2dh[i] = W.dcdh[i];
+    }
+    // period t1 (:1921-1930)
+    omega = twopi / t1;
+    wvno = omega / cp1;
+    svfunc(W, omega, wvno);
+    energy(W, omega, wvno);
+    for (int i = 0; i < mmax; i++) {
+        da1[i] = W.dcda[i];
+        db1[i] = W.dcdb[i];
+        dr1[i] = W.dcdr[i];
+        dh1[i] = W.dcdh[i];
+    }
+    // period t2 (:1933-1942)
+    omega = twopi / t2;
+    wvno = omega / cp2;
+    svfunc(W, omega, wvno);
+    energy(W, omega, wvno);
+    for (int i = 0; i < mmax; i++) {
+        da2[i] = W.dcda[i];
+        db2[i] = W.dcdb[i];
+        dr2[i] = W.dcdr[i];
+        dh2[i] = W.dcdh[i];
+    }
+    // :1945-1949.  The first term reads the module arrays dcda.. , which hold
+    // the t2 evaluation at this point.
+    const double uc1 = cg / cp;
+    for (int i = 0; i < mmax; i++) {
+        du2da[i] = uc1 * (2.0 - uc1) * W.dcda[i] - uc1 * uc1 * t * (da2[i] - da1[i]) / (t2 - t1);
+        du2db[i] = uc1 * (2.0 - uc1) * W.dcdb[i] - uc1 * uc1 * t * (db2[i] - db1[i]) / (t2 - t1);
+        du2dr[i] = uc1 * (2.0 - uc1) * W.dcdr[i] - uc1 * uc1 * t * (dr2[i] - dr1[i]) / (t2 - t1);
+        du2dh[i] = uc1 * (2.0 - uc1) * W.dcdh[i] - uc1 * uc1 * t * (dh2[i] - dh1[i]) / (t2 - t1);
+    }
+    if (nsph > 0) {   // :1952-1971
+        const double ar = 6371.0;
+        omega = twopi / t;
+        const double r = cp / (2.0 * ar * omega);
+        const double tm = std::sqrt(1.0 + r * r);
+        const double q = 0.5 / (ar * omega);
+        const double tm1 = (q * q) / tm;
+        const double tm3 = (tm * tm) * tm;
+        for (int i = 0; i < mmax; i++) {
+            du2da[i] = (tm * du2da[i] + cg * cp * dc2da[i] * tm1) * W.vtp[i];
+            du2db[i] = (tm * du2db[i] + cg * cp * dc2db[i] * tm1) * W.vtp[i];
+            du2dr[i] = (tm * du2dr[i] + cg * cp * dc2dr[i] * tm1) * W.rtp[i];
+            du2dh[i] = (tm * du2dh[i] + cg * cp * dc2dh[i] * tm1) * W.dtp[i];
+            dc2da[i] = dc2da[i] / tm3 * W.vtp[i];
+            dc2db[i] = dc2db[i] / tm3 * W.vtp[i];
+            dc2dr[i] = dc2dr[i] / tm3 * W.rtp[i];
+            dc2dh[i] = dc2dh[i] / tm3 * W.dtp[i];
+        }
+        cg = cg * tm;
+    }
+    for (int i = 0; i < mmax - 1; i++) {   // :1974-1981
+        double sums = 0.0;
+        for (int k = i + 1; k < mmax; k++) sums = sums + dc2dh[k];
+        dc2dh[i] = sums;
+        sums = 0.0;
+        for (int k = i + 1; k < mmax; k++) sums = sums + du2dh[k];
+        du2dh[i] = sums;
+    }
+    dc2dh[mmax - 1] = 0.0;
+    du2dh[mmax - 1] = 0.0;
+    *cg_out = cg;
+}
 }  // namespace
 
 extern "C" void orc_sregn96_hti(const float* thk, const float* vp, const float* vs,
@@ -887,4 +1009,13 @@ extern "C" void orc_sregn96(const float* thk, const float* vp, const float* vs,
                             int iflsph) {
     run_sregn(thk, vp, vs, rhom, nlayer, t, cp, cg, dispu, dispw, stressu, stressw, dc2da,
               dc2db, dc2dh, dc2dr, nullptr, nullptr, iflsph);
+}
+
+extern "C" void orc_sregnpu(const float* thk, const float* vp, const float* vs, const float* rhom,
+                            int nlayer, double t, double cp, double t1, double cp1, double t2,
+                            double cp2, double* cg, double* du2da, double* du2db, double* du2dh,
+                            double* du2dr, double* dc2da, double* dc2db, double* dc2dh,
+                            double* dc2dr, int iflsph) {
+    run_sregnpu(thk, vp, vs, rhom, nlayer, t, cp, t1, cp1, t2, cp2, cg, du2da, du2db, du2dh,
+                du2dr, dc2da, dc2db, dc2dh, dc2dr, iflsph);
 }

@@ -26,6 +26,7 @@ EXPORTED = (
     "sa_plan_create", "sa_plan_destroy", "sa_plan_set_graph", "sa_plan_forward_adjoint",
     "sa_forward_for_events", "sa_plan_debug_fields", "sa_plan_kernel_timing", "sa_plan_kernel_ms",
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
+    "sa_depthkernel_columns_group",
     "sa_eik_fwd_field_noalloc",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
@@ -86,6 +87,8 @@ def lib():
                                         C.POINTER(d), _ip, _ip]
     L.sa_surfdisp_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, i, i, _vp, _vp, _vp]
     L.sa_depthkernel_columns.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, _vp, _vp, _vp, _vp, _vp]
+    L.sa_depthkernel_columns_group.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, _vp, _vp, _vp,
+                                               _vp, _vp]
     L.sa_combine_kernels_vs.argtypes = [_vp, i, i, i, i] + [_vp] * 7 + [_vp]
     L.sa_eik_fwd_field_noalloc.argtypes = [i, i] + [_vp] * 6 + [d, d] + [_vp] * 4
     L.sa_grad_create.argtypes = [_vp, i, _dp, _dp, C.POINTER(_vp)]

@@ -866,6 +866,53 @@ extern "C" int sa_depthkernel_columns(sa_ctx* ctx, int nx, int ny, int nz, const
     return SA_OK;
 }
 
+extern "C" int sa_depthkernel_columns_group(sa_ctx* ctx, int nx, int ny, int nz,
+                                            const double* zgrid, const double* vs3d, int nper,
+                                            const double* periods, double* sen_vs,
+                                            double* sen_vp, double* sen_rho, int* status,
+                                            void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 1 || ny < 1 || nz < 2 || nper < 1 || nper > 64 || !zgrid || !periods || !vs3d ||
+        !sen_vs || !sen_vp || !sen_rho)
+        return fail(ctx, SA_ERR_ARG, "sa_depthkernel_columns_group: bad sizes or null pointers");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    const void* L = layer_const_dev(ctx, nz, zgrid, &rc);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    // periods t(1 +- 0.5*0.01) (src/surfdisp.cpp:223-228)
+    const double dt = 0.01;
+    std::vector<double> t3(3 * (size_t)nper);
+    for (int i = 0; i < nper; ++i) {
+        t3[i] = periods[i];
+        t3[nper + i] = periods[i] * (1.0 + 0.5 * dt);
+        t3[2 * nper + i] = periods[i] * (1.0 - 0.5 * dt);
+    }
+    const size_t plane = (size_t)nx * ny * nper;
+    DArr<double> dper, cps;
+    DArr<int> st3;
+    SA_CUDA(dper.upload(t3.data(), t3.size(), st));
+    SA_CUDA(cps.alloc(3 * plane));
+    SA_CUDA(st3.alloc(3 * (size_t)nx * ny));
+    for (int k = 0; k < 3; k++)
+        SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, dper.p + k * nper, 1, 2, 0, L,
+                                        cps.p + k * plane, st3.p + k * (size_t)nx * ny, st));
+    SA_CUDA(launch_depthkernel_group(nx, ny, nz, vs3d, nper, dper.p, dper.p + nper,
+                                     dper.p + 2 * nper, cps.p, cps.p + plane, cps.p + 2 * plane, L,
+                                     sen_vs, sen_vp, sen_rho, st));
+    std::vector<int> hs(3 * (size_t)nx * ny);
+    SA_CUDA(cudaMemcpyAsync(hs.data(), st3.p, hs.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    int bad = 0;
+    for (size_t c = 0; c < (size_t)nx * ny; c++) {
+        const int v = hs[c] | hs[(size_t)nx * ny + c] | hs[2 * (size_t)nx * ny + c];
+        if (status) status[c] = v;
+        bad |= v;
+    }
+    if (bad) return fail(ctx, SA_ERR_NOROOT, "Dispersion calculation failed");
+    return SA_OK;
+}
+
 extern "C" int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper,
                                      const double* adj_s, const double* vs3d, const double* vp3d,
                                      const double* sen_vs, const double* sen_vp,

@@ -66,3 +66,24 @@ def combine_kernels_vs(adj_s, vs3d, vp3d, sen_vs, sen_vp, sen_rho, ctx=None, str
                                            ptr(ker), stream)
     _capi.check(ctx.h, rc)
     return ker
+
+
+def depthkernel_group(zgrid, vs3d, periods, ctx=None, stream=None):
+    """Rayleigh group-velocity depth kernels (surfker::depthkernel_rayleigh_group):
+    (sen_vs, sen_vp, sen_rho) each (nx, ny, nz, nper); raises DispersionError
+    where a root search fails."""
+    import torch
+    ctx = ctx or default_context()
+    nx, ny, nz = vs3d.shape
+    p = np.ascontiguousarray(periods, dtype=np.float64)
+    z = np.ascontiguousarray(zgrid, dtype=np.float64)
+    out = [torch.empty((nx, ny, nz, p.size), dtype=torch.float64, device=vs3d.device)
+           for _ in range(3)]
+    status = np.zeros(nx * ny, np.int32)
+    rc = _capi.lib().sa_depthkernel_columns_group(ctx.h, nx, ny, nz, z, ptr(vs3d), p.size, p,
+                                                  ptr(out[0]), ptr(out[1]), ptr(out[2]),
+                                                  status.ctypes.data, stream)
+    if rc == _capi.SA_ERR_NOROOT:
+        raise DispersionError(f"Dispersion calculation failed in {int((status != 0).sum())} columns")
+    _capi.check(ctx.h, rc)
+    return tuple(out)

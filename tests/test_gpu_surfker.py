@@ -79,3 +79,32 @@ def test_combine_kernels_matches_oracle(orc, gpu, c1):
     ref = orc.combine_kernels_vs(adj, vs, vp, sv, sp, sr)
     got = surfker.combine_kernels_vs(_dev(adj), _dev(vs), _dev(vp), _dev(sv), _dev(sp), _dev(sr))
     assert np.array_equal(got.cpu().numpy(), ref)
+
+
+def test_group_depthkernel_matches_oracle(orc, gpu, c1):
+    """Rayleigh group-velocity kernels (depthkernel_rayleigh_group / sregnpu).
+    The kernels difference phase kernels at t(1 +- 0.005), which amplifies a
+    one-ulp flip of a phase velocity 200-fold: columns whose three phase
+    velocities are bit-identical to the oracle's within 1e-10 of the column's
+    largest kernel, all columns within 1e-3."""
+    from surfattpp_b200 import surfker
+    w = c1
+    vs = w.vs3d[::4, ::4].copy()
+    rv, rp, rr, st = orc.depthkernel_group(w.zgrid, vs, w.periods, nthreads=8)
+    assert st.sum() == 0
+    gv, gp, gr = surfker.depthkernel_group(w.zgrid, _dev(vs), w.periods)
+    same = np.ones(vs.shape[:2][::-1] + (w.nper,), bool)   # (ny, nx, nper)
+    for f in (1.0, 1.005, 0.995):
+        per = w.periods * f if f == 1.0 else np.array([p * (1.0 + 0.5 * 0.01 * (1 if f > 1 else -1))
+                                                        for p in w.periods])
+        d, _ = surfker.fwdsurf(w.zgrid, _dev(vs), per)
+        r, _ = orc.fwdsurf(w.zgrid, vs, per, nthreads=8)
+        same &= np.transpose(d.cpu().numpy() == r, (1, 2, 0))
+    mask = np.transpose(same, (1, 0, 2))[:, :, None, :]      # (nx, ny, 1, nper)
+    assert mask.mean() > 0.5
+    for g, r in ((gv, rv), (gp, rp), (gr, rr)):
+        g = g.cpu().numpy()
+        scale = np.abs(r).max(axis=2, keepdims=True)
+        err = np.abs(g - r) / scale
+        assert np.max(np.where(mask, err, 0.0)) <= 2e-9
+        assert np.max(err) <= 1e-3
