@@ -318,7 +318,7 @@ def main():
     if a.impl == "reference":
         return run_reference(a)
     import torch
-    from surfattpp_b200 import preproc
+    from surfattpp_b200 import distributed, preproc
     from surfattpp_b200._capi import Context
 
     rank = int(os.environ.get("RANK", "0"))
@@ -347,8 +347,7 @@ def main():
     def step():
         plan.run(sv, tt, wt, out=out, stream=cs)
         if dist is not None:
-            dist.all_reduce(out["adj_s"])
-            dist.all_reduce(out["chi"])
+            distributed.reduce_gradient(out["adj_s"], out["chi"])
 
     for _ in range(max(a.warmup, 3)):
         step()

@@ -334,6 +334,15 @@ int sa_grad_run(sa_grad* grad, const double* vs3d, const double* vp3d, const dou
  * sen_rho ((nx, ny, nz, nper) row-major; any may be NULL), on `stream`. */
 int sa_grad_sen(sa_grad* grad, double* sen_vs, double* sen_vp, double* sen_rho, void* stream);
 
+/* Multi-rank gradient: preproc::combine_kernels after the rank sum of adj_s
+ * (src/preproc.cpp:225-304, mpi.sum_all_all of adj_s_local per period, then
+ * the combination).  Combines the depth kernels of this handle's last
+ * sa_grad_run with a caller-supplied adj_s (nper, ny, nx) -- the sum over
+ * ranks of every rank's adj_s_out -- into ker_vs (nx, ny, nz).  vp3d NULL =
+ * vs2vp(vs3d); vs3d must be the model of the last run.  Device pointers. */
+int sa_grad_combine(sa_grad* grad, const double* vs3d, const double* vp3d, const double* adj_s,
+                    double* ker_vs, void* stream);
+
 /* ---- allocation-free entry point ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -28,7 +28,7 @@ EXPORTED = (
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
     "sa_depthkernel_columns_group",
     "sa_eik_fwd_field_noalloc",
-    "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen",
+    "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen", "sa_grad_combine",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
     "sa_grad_normalization", "sa_descent_angle", "sa_wolfe_condition", "sa_model_update_vs",
@@ -95,6 +95,7 @@ def lib():
     L.sa_grad_destroy.argtypes = [_vp]
     L.sa_grad_run.argtypes = [_vp] + [_vp] * 9 + [_vp]
     L.sa_grad_sen.argtypes = [_vp] * 5
+    L.sa_grad_combine.argtypes = [_vp] * 6
     L.sa_pde_smooth_nstep.argtypes = [i, d, d, d, _dp, d, d, C.POINTER(i), C.POINTER(d),
                                       C.POINTER(d)]
     z = C.c_size_t

@@ -1037,6 +1037,21 @@ extern "C" int sa_grad_sen(sa_grad* g, double* sen_vs, double* sen_vp, double* s
     return SA_OK;
 }
 
+extern "C" int sa_grad_combine(sa_grad* g, const double* vs3d, const double* vp3d,
+                               const double* adj_s, double* ker_vs, void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (!vs3d || !adj_s || !ker_vs) return fail(ctx, SA_ERR_ARG, "vs3d, adj_s and ker_vs are required");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    // the depth kernels of the last run were written on the side stream
+    SA_CUDA(cudaStreamWaitEvent(st, g->e_sen, 0));
+    SA_CUDA(launch_combine_vs(P->nx, P->ny, g->nz, P->nper, adj_s, vs3d, vp3d, g->sen_vs.p,
+                              g->sen_vp.p, g->sen_rho.p, ker_vs, st));
+    return SA_OK;
+}
+
 // ---- PostProc::pde_smooth ------------------------------------------------------
 
 namespace {

@@ -53,12 +53,22 @@ class MisfitGradient:
         except Exception:
             pass
 
-    def run(self, vs3d, tt_obs, weight, vp3d=None, out=None, stream=None):
+    def run(self, vs3d, tt_obs, weight, vp3d=None, out=None, stream=None, group=None):
         """Enqueue one evaluation on device tensors (float64, contiguous).
 
         vs3d (nx, ny, nz); vp3d (nx, ny, nz) or None for vs2vp(vs3d).
         Returns dict(ker_vs (nx, ny, nz), chi (1,), svel, adj_s
-        (nper, ny, nx), status (1,)); synchronise before reading."""
+        (nper, ny, nx), status (1,)); synchronise before reading.
+
+        Under torch.distributed with more than one rank, the plan holds this
+        rank's events (``distributed.shard_events``): adj_s and chi are summed
+        over ``group`` and ker_vs is combined from the sums, as
+        src/preproc.cpp:146, :225-304 do after the local events.  The work
+        then runs on torch's current stream (``stream`` must be None)."""
+        from . import distributed
+        multi = distributed._world(group)[1] > 1
+        if multi and stream is not None:
+            raise ValueError("a multi-rank run uses torch's current stream")
         import torch
         dev = vs3d.device
         p = self.plan
@@ -69,11 +79,29 @@ class MisfitGradient:
         out.setdefault("svel", torch.empty((p.nper, p.ny, p.nx), **f64))
         out.setdefault("adj_s", torch.empty((p.nper, p.ny, p.nx), **f64))
         out.setdefault("status", torch.zeros(1, dtype=torch.int32, device=dev))
+        if multi:
+            stream = torch.cuda.current_stream(dev).cuda_stream
         rc = _capi.lib().sa_grad_run(self.h, ptr(vs3d), ptr(vp3d), ptr(tt_obs), ptr(weight),
                                      ptr(out["ker_vs"]), ptr(out["chi"]), ptr(out["svel"]),
                                      ptr(out["adj_s"]), ptr(out["status"]), stream)
         _capi.check(p.ctx.h, rc)
+        if multi:
+            distributed.reduce_gradient(out["adj_s"], out["chi"], out["status"], group)
+            self.combine(vs3d, out["adj_s"], vp3d, out["ker_vs"], stream)
         return out
+
+    def combine(self, vs3d, adj_s, vp3d=None, ker_vs=None, stream=None):
+        """combine_kernels of the last run's depth kernels with ``adj_s``
+        (nper, ny, nx) -- e.g. the rank sum -- into ker_vs (nx, ny, nz)
+        (sa_grad_combine)."""
+        import torch
+        p = self.plan
+        if ker_vs is None:
+            ker_vs = torch.empty((p.nx, p.ny, self.nz), dtype=torch.float64, device=vs3d.device)
+        rc = _capi.lib().sa_grad_combine(self.h, ptr(vs3d), ptr(vp3d), ptr(adj_s), ptr(ker_vs),
+                                         stream)
+        _capi.check(p.ctx.h, rc)
+        return ker_vs
 
     def sen(self, stream=None):
         """(sen_vs, sen_vp, sen_rho) of the last run as device tensors

@@ -107,6 +107,13 @@ def test_gradient_chain_equals_parts(c2, gpu, orc):
     K2 = surfker.combine_kernels_vs(out["adj_s"], vs, vp, kv, kp, kr)
     torch.cuda.synchronize()
     assert torch.equal(K2, out["ker_vs"])
+    # sa_grad_combine: the last run's depth kernels with a given adj_s (the
+    # multi-rank path passes the rank sum); linear in adj_s
+    K3 = g.combine(vs, out["adj_s"])
+    K4 = g.combine(vs, 2.0 * out["adj_s"], vp)
+    torch.cuda.synchronize()
+    assert torch.equal(K3, out["ker_vs"])
+    assert torch.equal(K4, 2.0 * out["ker_vs"])
 
 
 def test_gradient_repeat_and_autograd(c2, gpu):
