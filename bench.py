@@ -147,17 +147,20 @@ def algorithmic_bytes(nx, ny, fwd_iters, adj_iters, bpu_fwd, bpu_adj):
     return fwd * bpu_fwd + adj * bpu_adj, fwd, adj
 
 
-def cpu_baseline(a, w, svel, nev=16):
+def cpu_baseline(a, w, svel, nev=None):
     """The oracle (port of the reference) on a bounded sample of events with
-    every host thread."""
+    every host thread: 24 events per thread by default (about 10 s on the
+    301x301 grid, where one FP64 forward + adjoint solve takes ~0.4 s on one
+    core)."""
     from oracle import oracle as O
     from surfattpp_b200 import workloads as W
     O.build()
     rng = np.random.default_rng(7)
+    nth = os.cpu_count() or 1
+    nev = 24 * nth if nev is None else nev
     keep = np.sort(rng.choice(w.n_events, size=min(nev, w.n_events), replace=False))
     sub = W.subset_events(w, keep)
     m11, m12, m22 = sub.media()
-    nth = os.cpu_count() or 1
     t0 = time.perf_counter()
     O.forward_for_events(sub.xx_deg, sub.yy_deg, svel, m11, m12, m22, sub.events(),
                          calc_adj=True, nthreads=nth)
@@ -173,15 +176,16 @@ def run_reference(a):
     if rank != 0:
         return 0
     w, svel = make_inputs(a, 0)
-    base = cpu_baseline(a, w, svel, nev=8)
-    vals = []
-    for _ in range(max(a.warmup, 0)):
-        pass   # the CPU sample has no warm-up state
-    for _ in range(a.steps):
-        vals.append(cpu_baseline(a, w, svel, nev=8)["value"])
+    # each step: 8 events per host thread (~3 s), so --steps 5 ends in well
+    # under a minute; the sample has no warm-up state
+    nev = 8 * (os.cpu_count() or 1)
+    base = cpu_baseline(a, w, svel, nev=nev)
+    vals = [base["value"]]
+    for _ in range(max(a.steps - 1, 0)):
+        vals.append(cpu_baseline(a, w, svel, nev=nev)["value"])
     v = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 8.0 / v * 1e3,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": nev / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": workload_config(a, world),
             "cpu_baseline": {**base, "value": v},
