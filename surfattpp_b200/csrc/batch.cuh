@@ -54,7 +54,7 @@ struct BatchArgs {
 // forward operands (PK) and the packed adjoint coefficients share one region:
 // the forward planes are dead once T is formed.
 struct SlotLayout {
-    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, flags, total;
+    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, flags, rng, total;
 };
 template <class S>
 __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
@@ -85,6 +85,7 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     L.sadj = take(r * sizeof(double));
     L.syn = take(r * sizeof(double));
     L.flags = take(n);   // sweep flags (systolic.cuh), forward then adjoint
+    L.rng = take((size_t)ny * sizeof(int2));   // per-row flag ranges (systolic.cuh)
     L.total = o;
     return L;
 }
@@ -92,8 +93,8 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
 template <class S, bool ISO>
 __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo& si, int ip,
                                             int src, S* tau, S* tst, Q4<S>* pk,
-                                            unsigned char* flags, double* T, int& iters,
-                                            int& status) {
+                                            unsigned char* flags, int2* rng, double* T,
+                                            int& iters, int& status) {
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
     const size_t n = (size_t)nx * ny;
@@ -129,22 +130,34 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     P.tau = tau;
     P.tau_start = tst;
     P.flags = flags;
+    P.rng = rng;
     P.fix_x0 = si.fix_x0;
     P.fix_x1 = si.fix_x1;
-    P.yy = g.yy;
-    P.y0 = si.y0;
-    P.dy64 = g.dy;
+    // rows with |(yy - y0)/dy| <= 1 (src/eikonal_solver.cpp:118-129, :162):
+    // one contiguous range, yy being monotone
+    int fy0 = ny, fy1 = -1;
+    for (int iy = lane; iy < ny; iy += 32)
+        if (fabs((g.yy[iy] - si.y0) / g.dy) <= 1.0) {
+            fy0 = min(fy0, iy);
+            fy1 = max(fy1, iy);
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        fy0 = min(fy0, __shfl_xor_sync(FULL_MASK, fy0, o));
+        fy1 = max(fy1, __shfl_xor_sync(FULL_MASK, fy1, o));
+    }
+    P.fy0 = fy0;
+    P.fy1 = fy1;
     // initial tau (src/eikonal_solver.cpp:118-129); FP32 stores u = tau - 1
     const S off = (sizeof(S) == sizeof(double)) ? S(0) : S(1);
     for (size_t k = lane; k < n; k += 32) {
         const int iy = (int)(k / nx), ix = (int)(k % nx);
-        const bool fixed =
-            fabs((g.yy[iy] - si.y0) / g.dy) <= 1.0 && ix >= si.fix_x0 && ix <= si.fix_x1;
+        const bool fixed = iy >= fy0 && iy <= fy1 && ix >= si.fix_x0 && ix <= si.fix_x1;
         const S v = (fixed ? S(1) : S(10)) - off;
         tau[k] = v;
         tst[k] = v;
         flags[k] = 1;
     }
+    for (int iy = lane; iy < ny; iy += 32) rng[iy] = make_int2(0, nx - 1);
     __syncwarp();
     iters = 0;
     for (int iter = 0; iter < 2000; iter++) {
@@ -190,6 +203,7 @@ batch_kernel(BatchArgs<S> B) {
     double* P_syn = reinterpret_cast<double*>(base + L.syn);
     Q4<S>* P_pk = reinterpret_cast<Q4<S>*>(base + L.PK);
     unsigned char* P_fl = base + L.flags;
+    int2* P_rng = reinterpret_cast<int2*>(base + L.rng);
 
     for (;;) {
         const unsigned int qi = warp_next_event(B.sc.queue);
@@ -204,8 +218,8 @@ batch_kernel(BatchArgs<S> B) {
 
         if (B.mode != MODE_ADJ_ONLY) {
             int iters = 0;
-            fwd_solve<S, ISO>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_fl, P_T, iters,
-                              status);
+            fwd_solve<S, ISO>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_fl, P_rng, P_T,
+                              iters, status);
             if (lane == 0 && B.out.fwd_iters) B.out.fwd_iters[e] = iters;
             if (B.out.T_out)
                 for (size_t k = lane; k < n; k += 32) B.out.T_out[(size_t)e * n + k] = P_T[k];
@@ -281,6 +295,7 @@ batch_kernel(BatchArgs<S> B) {
                     P_Tst[k] = v0;
                     P_fl[k] = 1;
                 }
+                for (int iy = lane; iy < ny; iy += 32) P_rng[iy] = make_int2(1, nx - 2);
                 __syncwarp();
                 AdjPolicyExact Q;
                 Q.nx = nx;
@@ -292,6 +307,7 @@ batch_kernel(BatchArgs<S> B) {
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_Tst;
                 Q.flags = P_fl;
+                Q.rng = P_rng;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
@@ -352,6 +368,7 @@ batch_kernel(BatchArgs<S> B) {
                     P_tst[k] = v0;
                     P_fl[k] = 1;
                 }
+                for (int iy = lane; iy < ny; iy += 32) P_rng[iy] = make_int2(1, nx - 2);
                 __syncwarp();
                 AdjPolicyW32 Q;
                 Q.nx = nx;
@@ -362,6 +379,7 @@ batch_kernel(BatchArgs<S> B) {
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_tst;
                 Q.flags = P_fl;
+                Q.rng = P_rng;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;

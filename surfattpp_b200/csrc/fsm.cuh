@@ -144,11 +144,18 @@ struct MetricCell {
 template <class S>
 struct MetricCell<S, true> {};
 
+#ifndef SA_FWD_LEAD
+#define SA_FWD_LEAD 1
+#endif
+#ifndef SA_FWD_ROLLED
+#define SA_FWD_ROLLED 1
+#endif
 template <class S, bool ISO>
 struct FwdBase {
     using V = S;
     using X = S;
-    static constexpr int kLead = 1;
+    static constexpr int kLead = SA_FWD_LEAD;
+    static constexpr bool kRolled = SA_FWD_ROLLED;
     struct Cell {
         S v;    // field before this update
         S x;    // T0 of the cell
@@ -158,6 +165,7 @@ struct FwdBase {
     };
     int nx, ny;
     unsigned char* flags;  // per event
+    int2* rng;           // per row: x range of flag bit 0 (systolic.cuh)
     const Q4<S>* pk;     // per event
     const Q4<S>* mt;     // per period (general metric) or null
     const S* a_row;      // iso: [ny]
@@ -165,22 +173,22 @@ struct FwdBase {
     S* tau;
     S* tau_start;
     int fix_x0, fix_x1;  // fixed source columns [fix_x0, fix_x1]
-    const double* yy;
-    double y0, dy64;
+    int fy0, fy1;        // fixed source rows [fy0, fy1]
     bool row_fixed;
     S row_a;
 
     __device__ int nrows() const { return ny; }
     __device__ int ncols() const { return nx; }
+    __device__ int stride() const { return nx; }
     __device__ int row(int rp, int yd) const { return yd > 0 ? rp : ny - 1 - rp; }
     __device__ int col(int cp, int xd) const { return xd > 0 ? cp : nx - 1 - cp; }
+    __device__ int cp_of(int ix, int xd) const { return xd > 0 ? ix : nx - 1 - ix; }
     __device__ void begin_row(int iy, bool act) {
         if (!act) return;
-        row_fixed = fabs((yy[iy] - y0) / dy64) <= 1.0;
+        row_fixed = iy >= fy0 && iy <= fy1;
         if (ISO) row_a = a_row[iy];
     }
-    __device__ Cell load(int iy, int ix, bool last) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ Cell load(int k, bool last) const {
         Cell c;
         c.v = tau[k];
         const Q4<S> q = ld4(pk + k);
@@ -207,22 +215,18 @@ struct FwdBase {
     __device__ S cc(const Cell& c) const {
         if constexpr (ISO) return S(0); else return c.m.c;
     }
-    __device__ Cell load_nb(int iy, int ix) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ Cell load_nb(int k) const {
         Cell c{};
         c.v = tau[k];
         c.x = pk[k].x;
         c.fl = flags[k];
         return c;
     }
-    __device__ void store(int iy, int ix, S v, bool write_v, bool write_start) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ void store(int k, S v, bool write_v, bool write_start) const {
         if (write_v) tau[k] = v;
         if (write_start) tau_start[k] = v;
     }
-    __device__ void store_flag(int iy, int ix, unsigned f) const {
-        flags[(size_t)iy * nx + ix] = (unsigned char)f;
-    }
+    __device__ void store_flag(int k, unsigned f) const { flags[k] = (unsigned char)f; }
 };
 
 // FP64 forward: field tau, exact reference update.
@@ -234,13 +238,19 @@ struct FwdPolicy64 : FwdBase<double, ISO> {
     using Base::fix_x0;
     using Base::fix_x1;
     double dx, dy;
-    __device__ double update(const Cell& cur, int iy, int ix, const Nb<double, double>& xm,
+    // Neighbours come in sweep order (xm / ym upwind).  The update is
+    // evaluated in the sweep's reflected frame x' = xd*x, y' = yd*y: T0x,
+    // T0y and the cross term c change sign, every intermediate is the
+    // reference's own value times +-1 (exact), and the set of candidates is
+    // the same, so the result is bit-identical to the unreflected update.
+    __device__ double update(const Cell& cur, int ix, const Nb<double, double>& xm,
                              const Nb<double, double>& xp, const Nb<double, double>& ym,
-                             const Nb<double, double>& yp) const {
+                             const Nb<double, double>& yp, int xd, int yd) const {
         if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;   // ischange == 0
-        return fsm_update<double, ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur),
-                                       this->cb(cur), this->cc(cur), cur.f, dx, dy, xm, xp, ym,
-                                       yp);
+        return fsm_update<double, ISO>(cur.v, cur.x, (double)xd * cur.gx, (double)yd * cur.gy,
+                                       this->ca(cur), this->cb(cur),
+                                       (double)(xd * yd) * this->cc(cur), cur.f, dx, dy, xm, xp,
+                                       ym, yp);
     }
     // convergence sums of src/eikonal_solver.cpp:292-302, last sweep only
     __device__ void account(const Cell& cur, double nv, double& l1, double& linf) const {
@@ -349,12 +359,16 @@ struct FwdPolicyDelta32 : FwdBase<float, ISO> {
     using Base::fix_x0;
     using Base::fix_x1;
     float idx, idy;
-    __device__ float update(const Cell& cur, int iy, int ix, const Nb<float, float>& xm,
+    // neighbours in sweep order, evaluated in the reflected frame (see
+    // FwdPolicy64::update)
+    __device__ float update(const Cell& cur, int ix, const Nb<float, float>& xm,
                             const Nb<float, float>& xp, const Nb<float, float>& ym,
-                            const Nb<float, float>& yp) const {
+                            const Nb<float, float>& yp, int xd, int yd) const {
         if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;
-        return fsm_update_delta<ISO>(cur.v, cur.x, cur.gx, cur.gy, this->ca(cur), this->cb(cur),
-                                     this->cc(cur), cur.f, idx, idy, xm, xp, ym, yp);
+        return fsm_update_delta<ISO>(cur.v, cur.x, (float)xd * cur.gx, (float)yd * cur.gy,
+                                     this->ca(cur), this->cb(cur),
+                                     (float)(xd * yd) * this->cc(cur), cur.f, idx, idy, xm, xp,
+                                     ym, yp);
     }
     __device__ void account(const Cell& cur, float nv, double& l1, double& linf) const {
         const double d = fabs((double)nv - (double)cur.vs) * (double)cur.x;
@@ -371,6 +385,7 @@ struct AdjPolicyExact {
     using V = double;
     using X = float;      // no auxiliary neighbour data
     static constexpr int kLead = 2;
+    static constexpr bool kRolled = false;
     struct Cell {
         double v;
         float x;
@@ -382,6 +397,7 @@ struct AdjPolicyExact {
     int nx, ny;
     double dx, dy;
     unsigned char* flags;
+    int2* rng;
     const Q4<double>* aq;
     const double2* dd;
     double* Ta;
@@ -389,11 +405,12 @@ struct AdjPolicyExact {
 
     __device__ int nrows() const { return ny - 2; }
     __device__ int ncols() const { return nx - 2; }
+    __device__ int stride() const { return nx; }
     __device__ int row(int rp, int yd) const { return yd > 0 ? 1 + rp : ny - 2 - rp; }
     __device__ int col(int cp, int xd) const { return xd > 0 ? 1 + cp : nx - 2 - cp; }
+    __device__ int cp_of(int ix, int xd) const { return xd > 0 ? ix - 1 : nx - 2 - ix; }
     __device__ void begin_row(int, bool) {}
-    __device__ Cell load(int iy, int ix, bool last) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ Cell load(int k, bool last) const {
         Cell c;
         c.v = Ta[k];
         c.x = 0.f;
@@ -403,16 +420,21 @@ struct AdjPolicyExact {
         c.fl = flags[k];
         return c;
     }
-    __device__ Cell load_nb(int iy, int ix) const {
+    __device__ Cell load_nb(int k) const {
         Cell c{};
-        const size_t k = (size_t)iy * nx + ix;
         c.v = Ta[k];
         c.fl = flags[k];
         return c;
     }
-    __device__ double update(const Cell& cur, int iy, int ix, const Nb<double, float>& xm,
-                             const Nb<double, float>& xp, const Nb<double, float>& ym,
-                             const Nb<double, float>& yp) const {
+    // um / dm: upwind / downwind x neighbour in sweep order (likewise uy /
+    // dy_), mapped back to the grid's left/right and bottom/top
+    __device__ double update(const Cell& cur, int, const Nb<double, float>& um,
+                             const Nb<double, float>& dm, const Nb<double, float>& uy,
+                             const Nb<double, float>& dy_, int xd, int yd) const {
+        const Nb<double, float>& xm = xd > 0 ? um : dm;
+        const Nb<double, float>& xp = xd > 0 ? dm : um;
+        const Nb<double, float>& ym = yd > 0 ? uy : dy_;
+        const Nb<double, float>& yp = yd > 0 ? dy_ : uy;
         const double2 de = cur.de;
         double nv;
         if (fabs(de.y) < 1e-14) {
@@ -434,23 +456,24 @@ struct AdjPolicyExact {
         l1 += dv;
         linf = fmax(linf, dv);
     }
-    __device__ void store(int iy, int ix, double v, bool write_v, bool write_start) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ void store(int k, double v, bool write_v, bool write_start) const {
         if (write_v) Ta[k] = v;
         if (write_start) Ta_start[k] = v;
     }
-    __device__ void store_flag(int iy, int ix, unsigned f) const {
-        flags[(size_t)iy * nx + ix] = (unsigned char)f;
-    }
+    __device__ void store_flag(int k, unsigned f) const { flags[k] = (unsigned char)f; }
 };
 
 // Adjoint sweep policy, FP32 weight form: the same Gauss-Seidel update
 // rewritten as Ta = c0 + wxm*Ta(ix-1) + wxp*Ta(ix+1) + wym*Ta(iy-1) + wyp*Ta(iy+1)
 // with FP32 weights computed in FP64 (w = {wxm, wxp, wym, wyp}, c0 separate).
+#ifndef SA_ADJ32_LEAD
+#define SA_ADJ32_LEAD 3
+#endif
 struct AdjPolicyW32 {
     using V = float;
     using X = float;
-    static constexpr int kLead = 4;
+    static constexpr int kLead = SA_ADJ32_LEAD;
+    static constexpr bool kRolled = false;
     struct Cell {
         float v;
         float x;
@@ -461,6 +484,7 @@ struct AdjPolicyW32 {
     };
     int nx, ny;
     unsigned char* flags;
+    int2* rng;
     const Q4<float>* W;
     const float* C0;
     float* Ta;
@@ -469,11 +493,12 @@ struct AdjPolicyW32 {
 
     __device__ int nrows() const { return ny - 2; }
     __device__ int ncols() const { return nx - 2; }
+    __device__ int stride() const { return nx; }
     __device__ int row(int rp, int yd) const { return yd > 0 ? 1 + rp : ny - 2 - rp; }
     __device__ int col(int cp, int xd) const { return xd > 0 ? 1 + cp : nx - 2 - cp; }
+    __device__ int cp_of(int ix, int xd) const { return xd > 0 ? ix - 1 : nx - 2 - ix; }
     __device__ void begin_row(int, bool) {}
-    __device__ Cell load(int iy, int ix, bool last) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ Cell load(int k, bool last) const {
         Cell c;
         c.v = Ta[k];
         c.x = 0.f;
@@ -483,16 +508,20 @@ struct AdjPolicyW32 {
         c.fl = flags[k];
         return c;
     }
-    __device__ Cell load_nb(int iy, int ix) const {
+    __device__ Cell load_nb(int k) const {
         Cell c{};
-        const size_t k = (size_t)iy * nx + ix;
         c.v = Ta[k];
         c.fl = flags[k];
         return c;
     }
-    __device__ float update(const Cell& cur, int, int, const Nb<float, float>& xm,
-                            const Nb<float, float>& xp, const Nb<float, float>& ym,
-                            const Nb<float, float>& yp) const {
+    // neighbours in sweep order, mapped back as in AdjPolicyExact::update
+    __device__ float update(const Cell& cur, int, const Nb<float, float>& um,
+                            const Nb<float, float>& dm, const Nb<float, float>& uy,
+                            const Nb<float, float>& dy_, int xd, int yd) const {
+        const Nb<float, float>& xm = xd > 0 ? um : dm;
+        const Nb<float, float>& xp = xd > 0 ? dm : um;
+        const Nb<float, float>& ym = yd > 0 ? uy : dy_;
+        const Nb<float, float>& yp = yd > 0 ? dy_ : uy;
         const float txm = xm.has ? xm.v : 0.f;
         const float txp = xp.has ? xp.v : 0.f;
         const float tym = ym.has ? ym.v : 0.f;
@@ -505,14 +534,11 @@ struct AdjPolicyW32 {
         linf = fmax(linf, dv);
         vmax = fmax(vmax, fabs((double)nv));
     }
-    __device__ void store(int iy, int ix, float v, bool write_v, bool write_start) const {
-        const size_t k = (size_t)iy * nx + ix;
+    __device__ void store(int k, float v, bool write_v, bool write_start) const {
         if (write_v) Ta[k] = v;
         if (write_start) Ta_start[k] = v;
     }
-    __device__ void store_flag(int iy, int ix, unsigned f) const {
-        flags[(size_t)iy * nx + ix] = (unsigned char)f;
-    }
+    __device__ void store_flag(int k, unsigned f) const { flags[k] = (unsigned char)f; }
 };
 
 }  // namespace sa

@@ -51,11 +51,14 @@ struct Nb {
 // All flags start at 1 (every cell is updated at its first visit).
 //
 // P must provide: types V (field value), X (neighbour aux), Cell {V v; X x;
-//   unsigned fl;}, nrows(), ncols(), row(rp, yd), col(cp, xd),
-//   begin_row(iy, active), load(iy, ix, last) -> Cell, load_nb(iy, ix) -> Cell,
-//   update(cur, iy, ix, xm, xp, ym, yp) -> V, account(cur, v, l1, linf)
-//   (last sweep of an iteration), store(iy, ix, v, write_v, write_start),
-//   store_flag(iy, ix, f).
+//   unsigned fl;}, kLead, nrows(), ncols(), stride() (row pitch), row(rp, yd),
+//   col(cp, xd) (sweep-ordered -> grid index), begin_row(iy, active),
+//   load(k, last) -> Cell and load_nb(k) -> Cell (v, x, fl) at grid offset k,
+//   update(cur, ix, xm, xp, ym, yp, xd, yd) -> V with xm / ym the upwind and
+//   xp / yp the downwind neighbours in sweep order, account(cur, v, l1, linf)
+//   (last sweep of an iteration), store(k, v, write_v, write_start),
+//   store_flag(k, f), cp_of(ix, xd) (grid x -> sweep-ordered column, the
+//   inverse of col) and rng (per-row x range of flag bit 0, see below).
 template <class V>
 __device__ __forceinline__ bool same_bits(V a, V b);
 template <>
@@ -67,88 +70,122 @@ __device__ __forceinline__ bool same_bits<double>(double a, double b) {
     return __double_as_longlong(a) == __double_as_longlong(b);
 }
 
+// Per-lane state of one strip's march.
+template <class V, class X>
+struct March {
+    int lane, NC, ioff, eoff, nr_strip, xd, yd;
+    bool act, has_up, has_dn, eup, edn, last;
+    V prev_v;           // this lane's previous result (upwind-x of its next cell)
+    X prev_x;
+    unsigned bal;       // ballot of "changed" of the previous step
+    unsigned pfl;       // flags of this lane's previous cell
+    int rmin, rmax;     // grid x range of this row's cells left with bit 0 set
+    int umin, umax;     // lane 0: grid x where its row changed (bit 0 set above)
+    int uf, ul;         // sweep columns where the row above changed in this sweep
+    int lf, ll;         // sweep columns where the strip's last row changed
+};
+
 // One step of the march.  cur = column c, nx1 = column c+1, ld = target of the
 // load of column c+1+LEAD.  Loads are issued LEAD steps before their first
-// use (as downwind-x / downwind-y neighbour) and buffer roles rotate
-// statically (the caller unrolls by LEAD+2), so no register copy ever waits
-// on a load in flight.  bal = ballot of "changed" of the previous step,
-// pfl = flags of this lane's previous cell.
+// use (as downwind-x / downwind-y neighbour); the caller either unrolls by
+// LEAD+2 and rotates the buffer roles statically, so no register copy ever
+// waits on a load in flight, or (LEAD 1, long updates) runs one copy of the
+// step and moves the buffers down after it.  Cells are addressed by their
+// grid offset: ioff = this lane's row, eoff = the seam row streamed by the
+// strip's first lane (eup, the row above) or last lane (edn, the row below);
+// no lane does both, since a strip with one row is the grid's last.
 template <int LEAD, class P, class Cell, class V, class X>
-__device__ __forceinline__ void systolic_step(P& p, const int t, const int lane, const int NR,
-                                              const int NC, const int rp, const bool act,
-                                              const int iy, const bool edge_up,
-                                              const bool edge_dn, const int iy_up,
-                                              const int iy_dn, const int nr_strip, const int xd,
-                                              const int yd, const bool last, Cell& cur,
-                                              Cell& nx1, Cell& ld, Cell& ucur, Cell& uld,
-                                              Cell& dcur, Cell& dld, V& prev_v, X& prev_x,
-                                              unsigned& bal, unsigned& pfl, double& l1,
-                                              double& linf) {
+__device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t, Cell& cur,
+                                              Cell& nx1, Cell& ld, Cell& ecur, Cell& eld,
+                                              double& l1, double& linf) {
+    const int lane = L.lane, NC = L.NC, xd = L.xd;
     const int c = t - lane;
-    const bool valid = act && c >= 0 && c < NC;
+    const bool valid = L.act && (unsigned)c < (unsigned)NC;
     const int c2 = c + 1 + LEAD;
-    if (act && c2 >= 0 && c2 < NC) {
+    if (L.act && (unsigned)c2 < (unsigned)NC) {
         const int ix2 = p.col(c2, xd);
-        ld = p.load(iy, ix2, last);
-        if (edge_up) uld = p.load_nb(iy_up, ix2);
-        if (edge_dn) dld = p.load_nb(iy_dn, ix2);
+        ld = p.load(L.ioff + ix2, L.last);
+        if (L.eup || L.edn) eld = p.load_nb(L.eoff + ix2);
     }
-    V up_v = __shfl_up_sync(FULL_MASK, prev_v, 1);
-    X up_x = __shfl_up_sync(FULL_MASK, prev_x, 1);
+    V up_v = __shfl_up_sync(FULL_MASK, L.prev_v, 1);
+    X up_x = __shfl_up_sync(FULL_MASK, L.prev_x, 1);
     V dn_v = __shfl_down_sync(FULL_MASK, nx1.v, 1);
     X dn_x = __shfl_down_sync(FULL_MASK, nx1.x, 1);
     // left neighbour changed: own bit of the last ballot; upper: lane-1's bit
-    // (the strip's first lane reads the row above)
-    unsigned up_chg = lane > 0 ? (bal >> (lane - 1)) & 1u : 0u;
-    if (edge_up) up_chg = (ucur.fl >> 1) & 1u;
-    const bool dirty = valid && (((cur.fl | (bal >> lane) | up_chg) & 1u) != 0u);
+    // (the strip's first lane reads bit 1 of the row above, current only
+    // where that row changed in this sweep)
+    unsigned up_chg = lane > 0 ? (L.bal >> (lane - 1)) & 1u : 0u;
+    if (L.eup) {
+        up_v = ecur.v;
+        up_x = ecur.x;
+        up_chg = (c >= L.uf && c <= L.ul) ? (ecur.fl >> 1) & 1u : 0u;
+    }
+    if (L.edn) {
+        dn_v = ecur.v;
+        dn_x = ecur.x;
+    }
+    const bool dirty = valid && (((cur.fl | (L.bal >> lane) | up_chg) & 1u) != 0u);
     const bool work = __any_sync(FULL_MASK, dirty);
     bool chg = false;
     int ix = 0;
     if (valid) {
         ix = p.col(c, xd);
-        const bool has_up = rp > 0;
-        const bool has_dn = rp + 1 < NR;
-        if (edge_up) {
-            up_v = ucur.v;
-            up_x = ucur.x;
-        }
-        if (edge_dn) {
-            dn_v = dcur.v;
-            dn_x = dcur.x;
-        }
         V nv = cur.v;
-        if (work) {
-            const Nb<V, X> upw_x{c > 0, prev_v, prev_x};
-            const Nb<V, X> dnw_x{c + 1 < NC, nx1.v, nx1.x};
-            const Nb<V, X> upw_y{has_up, up_v, up_x};
-            const Nb<V, X> dnw_y{has_dn, dn_v, dn_x};
-            nv = p.update(cur, iy, ix, xd > 0 ? upw_x : dnw_x, xd > 0 ? dnw_x : upw_x,
-                          yd > 0 ? upw_y : dnw_y, yd > 0 ? dnw_y : upw_y);
-        }
+        if (work)
+            nv = p.update(cur, ix, Nb<V, X>{c > 0, L.prev_v, L.prev_x},
+                          Nb<V, X>{c + 1 < NC, nx1.v, nx1.x}, Nb<V, X>{L.has_up, up_v, up_x},
+                          Nb<V, X>{L.has_dn, dn_v, dn_x}, xd, L.yd);
         chg = !same_bits(nv, cur.v);
         bool wst = false;
-        if (last) {
+        if (L.last) {
             p.account(cur, nv, l1, linf);
             wst = !same_bits(nv, cur.vs);
         }
-        if (chg || wst) p.store(iy, ix, nv, chg, wst);
-        prev_v = nv;
-        prev_x = cur.x;
+        if (chg || wst) p.store(L.ioff + ix, nv, chg, wst);
+        L.prev_v = nv;
+        L.prev_x = cur.x;
     }
     const unsigned nbal = __ballot_sync(FULL_MASK, chg);
     // flags of the previous cell (r', c-1): changed at its visit; a later
     // neighbour (right = this cell, lower = lane+1's cell of this step) changed
-    if (act && c >= 1 && c <= NC) {
-        const unsigned lower = (lane + 1 < nr_strip) ? (nbal >> (lane + 1)) & 1u : 0u;
-        const unsigned f = (((bal >> lane) & 1u) << 1) | ((nbal >> lane) & 1u) | lower;
-        if (f != pfl) p.store_flag(iy, p.col(c - 1, xd), f);
+    if (L.act && c >= 1 && c <= NC) {
+        const int ixp = p.col(c - 1, xd);
+        const unsigned lower = (lane + 1 < L.nr_strip) ? (nbal >> (lane + 1)) & 1u : 0u;
+        const unsigned f = (((L.bal >> lane) & 1u) << 1) | ((nbal >> lane) & 1u) | lower;
+        if (f != L.pfl) p.store_flag(L.ioff + ixp, f);
+        if (f & 1u) {
+            L.rmin = min(L.rmin, ixp);
+            L.rmax = max(L.rmax, ixp);
+        }
     }
-    if (edge_up && chg) p.store_flag(iy_up, ix, ucur.fl | 1u);
-    if (valid) pfl = cur.fl;
-    bal = nbal;
+    if (L.eup && chg) {
+        p.store_flag(L.eoff + ix, ecur.fl | 1u);
+        L.umin = min(L.umin, ix);
+        L.umax = max(L.umax, ix);
+    }
+    if ((nbal >> (L.nr_strip - 1)) & 1u) {
+        const int cl = t - (L.nr_strip - 1);
+        L.lf = min(L.lf, cl);
+        L.ll = max(L.ll, cl);
+    }
+    if (valid) L.pfl = cur.fl;
+    L.bal = nbal;
 }
 
+// Marching only where something can change.  Per row the policy keeps the
+// grid x range of its cells with flag bit 0 set (p.rng[iy], empty when
+// x > y).  A strip's cells can only change from column `first` on: the
+// first column of its rows' ranges, or where the row above changed in this
+// sweep.  Before it every cell is clean and stays so, so the march starts
+// there: each lane takes its previous cell (value, aux, flags) from memory
+// and the pipeline is filled from that column.  After `lastd` (the last such
+// column) and one step in which no cell changed, nothing can change any
+// more: the march stops.  A strip with nothing to do is not marched.  The
+// last sweep of an iteration marches every cell (its convergence sums and
+// start-of-iteration copy need all of them).  All of this is exact: the
+// cells not visited are exactly those the full march would have left
+// bit-identical.
+//
 // P::kLead = how many steps ahead a lane loads its row (1 for the long
 // forward update, more for the short adjoint update).
 template <class P>
@@ -162,51 +199,126 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
     const int lane = threadIdx.x & 31;
     const int NR = p.nrows();
     const int NC = p.ncols();
+    const int S = p.stride();
+    int uf = NC, ul = -1;   // changes of the row above the current strip
     for (int k0 = 0; k0 < NR; k0 += 32) {
         const int rp = k0 + lane;
         const bool act = rp < NR;
         const int nr_strip = min(32, NR - k0);
         const int iy = act ? p.row(rp, yd) : 0;
+        // columns (sweep order) this strip's march must cover
+        int fc = NC, lc = -1;
+        if (act) {
+            const int2 r = p.rng[iy];
+            if (r.x <= r.y) {
+                const int a = p.cp_of(r.x, xd), b = p.cp_of(r.y, xd);
+                fc = min(a, b);
+                lc = max(a, b);
+            }
+        }
+        int first = min(__reduce_min_sync(FULL_MASK, fc), uf);
+        int lastd = max(__reduce_max_sync(FULL_MASK, lc), ul);
+        if (last) {
+            first = 0;
+            lastd = NC;
+        }
+        if (first >= NC) {   // no cell of the strip can change
+            uf = NC;
+            ul = -1;
+            continue;
+        }
+        March<V, X> L;
+        L.lane = lane;
+        L.NC = NC;
+        L.xd = xd;
+        L.yd = yd;
+        L.last = last;
+        L.act = act;
+        L.nr_strip = nr_strip;
+        L.ioff = iy * S;
+        L.has_up = act && rp > 0;
+        L.has_dn = act && rp + 1 < NR;
         // strip-edge lanes also stream the neighbouring row of the adjacent
         // strip, with the same lead as their own row
-        const bool edge_up = act && lane == 0 && rp > 0;
-        const bool edge_dn = act && lane == nr_strip - 1 && rp + 1 < NR;
-        const int iy_up = edge_up ? p.row(rp - 1, yd) : 0;
-        const int iy_dn = edge_dn ? p.row(rp + 1, yd) : 0;
+        L.eup = lane == 0 && L.has_up;
+        L.edn = lane == nr_strip - 1 && L.has_dn;
+        const int iy_up = L.eup ? p.row(rp - 1, yd) : 0;
+        L.eoff = L.eup ? iy_up * S : (L.edn ? p.row(rp + 1, yd) * S : 0);
+        L.uf = uf;
+        L.ul = ul;
+        L.lf = NC;
+        L.ll = -1;
+        L.rmin = 0x7fffffff;
+        L.rmax = -1;
+        L.umin = 0x7fffffff;
+        L.umax = -1;
+        L.bal = 0u;
+        L.pfl = 0u;
+        L.prev_v = V(0);
+        L.prev_x = X(0);
         p.begin_row(iy, act);
-        Cell buf[NB], ub[NB], db[NB];
-        // columns c .. c+LEAD of step 0 (what earlier steps would have loaded)
+        // this lane's first column and the cell before it
+        const int c0 = first - lane;
+        if (act && c0 >= 1) {
+            const Cell q = p.load_nb(L.ioff + p.col(c0 - 1, xd));
+            L.prev_v = q.v;
+            L.prev_x = q.x;
+            L.pfl = q.fl;
+        }
+        Cell buf[NB], eb[NB];
+        // columns c0 .. c0+LEAD (what earlier steps would have loaded)
 #pragma unroll
         for (int q = 0; q < NB; q++) {
             buf[q] = Cell{};
-            ub[q] = Cell{};
-            db[q] = Cell{};
-            const int cq = q - lane;
+            eb[q] = Cell{};
+            const int cq = c0 + q;
             if (q <= LEAD && act && cq >= 0 && cq < NC) {
                 const int ixq = p.col(cq, xd);
-                buf[q] = p.load(iy, ixq, last);
-                if (edge_up) ub[q] = p.load_nb(iy_up, ixq);
-                if (edge_dn) db[q] = p.load_nb(iy_dn, ixq);
+                buf[q] = p.load(L.ioff + ixq, last);
+                if (L.eup || L.edn) eb[q] = p.load_nb(L.eoff + ixq);
             }
         }
-        V prev_v = V(0);
-        X prev_x = X(0);
-        unsigned bal = 0u, pfl = 0u;
         // one step more than the march: the last cell's flags are written
         // one step after its visit
         const int nsteps = NC + nr_strip;
-        for (int t = 0; t < nsteps; t += NB) {
+        if constexpr (P::kRolled && LEAD == 1) {
+            // one copy of the step (long updates: instruction-cache footprint
+            // over register moves); the load of this step lands in `ld` and
+            // moves down the buffer at the end of the step
+            Cell cur = buf[0], nx1 = buf[1], ecur = eb[0], enx1 = eb[1];
+            for (int t = first; t < nsteps; t++) {
+                Cell ld = cur, eld = ecur;
+                systolic_step<LEAD>(p, L, t, cur, nx1, ld, ecur, eld, l1, linf);
+                cur = nx1;
+                nx1 = ld;
+                ecur = enx1;
+                enx1 = eld;
+                if (t - 31 > lastd && L.bal == 0u) break;
+            }
+        } else {
+            for (int t = first; t < nsteps; t += NB) {
 #pragma unroll
-            for (int i = 0; i < NB; i++) {
-                if (t + i < nsteps)
-                    systolic_step<LEAD>(p, t + i, lane, NR, NC, rp, act, iy, edge_up, edge_dn,
-                                        iy_up, iy_dn, nr_strip, xd, yd, last, buf[i % NB],
-                                        buf[(i + 1) % NB], buf[(i + 1 + LEAD) % NB], ub[i % NB],
-                                        ub[(i + 1 + LEAD) % NB], db[i % NB],
-                                        db[(i + 1 + LEAD) % NB], prev_v, prev_x, bal, pfl, l1,
-                                        linf);
+                for (int i = 0; i < NB; i++) {
+                    if (t + i < nsteps)
+                        systolic_step<LEAD>(p, L, t + i, buf[i % NB], buf[(i + 1) % NB],
+                                            buf[(i + 1 + LEAD) % NB], eb[i % NB],
+                                            eb[(i + 1 + LEAD) % NB], l1, linf);
+                }
+                if (t + NB - 1 - 31 > lastd && L.bal == 0u) break;
             }
         }
+        // every cell of the row that had bit 0 set was visited: the range is
+        // replaced; lane 0 then adds where it set bit 0 in the row above
+        if (act) p.rng[iy] = make_int2(L.rmin, L.rmax);
+        __syncwarp();
+        if (L.eup && L.umin <= L.umax) {
+            int2 r = p.rng[iy_up];
+            r.x = min(r.x, L.umin);
+            r.y = max(r.y, L.umax);
+            p.rng[iy_up] = r;
+        }
+        uf = L.lf;
+        ul = L.ll;
         __syncwarp();
     }
 }
