@@ -85,7 +85,9 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     L.sadj = take(r * sizeof(double));
     L.syn = take(r * sizeof(double));
     L.flags = take(n);   // sweep flags (systolic.cuh), forward then adjoint
-    L.rng = take((size_t)ny * sizeof(int2));   // per-row flag ranges (systolic.cuh)
+    // per-row x ranges (systolic.cuh): [0, ny) flag bit 0, [ny, 2 ny) cells
+    // changed in the current iteration
+    L.rng = take(2 * (size_t)ny * sizeof(int2));
     L.total = o;
     return L;
 }
@@ -131,6 +133,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     P.tau_start = tst;
     P.flags = flags;
     P.rng = rng;
+    P.crng = rng + ny;
     P.fix_x0 = si.fix_x0;
     P.fix_x1 = si.fix_x1;
     // rows with |(yy - y0)/dy| <= 1 (src/eikonal_solver.cpp:118-129, :162):
@@ -157,7 +160,10 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
         tst[k] = v;
         flags[k] = 1;
     }
-    for (int iy = lane; iy < ny; iy += 32) rng[iy] = make_int2(0, nx - 1);
+    for (int iy = lane; iy < ny; iy += 32) {
+        rng[iy] = make_int2(0, nx - 1);
+        rng[ny + iy] = make_int2(0x7fffffff, -1);   // crng: nothing changed yet
+    }
     __syncwarp();
     iters = 0;
     for (int iter = 0; iter < 2000; iter++) {
@@ -295,7 +301,10 @@ batch_kernel(BatchArgs<S> B) {
                     P_Tst[k] = v0;
                     P_fl[k] = 1;
                 }
-                for (int iy = lane; iy < ny; iy += 32) P_rng[iy] = make_int2(1, nx - 2);
+                for (int iy = lane; iy < ny; iy += 32) {
+                    P_rng[iy] = make_int2(1, nx - 2);
+                    P_rng[ny + iy] = make_int2(0x7fffffff, -1);
+                }
                 __syncwarp();
                 AdjPolicyExact Q;
                 Q.nx = nx;
@@ -308,6 +317,7 @@ batch_kernel(BatchArgs<S> B) {
                 Q.Ta_start = P_Tst;
                 Q.flags = P_fl;
                 Q.rng = P_rng;
+                Q.crng = P_rng + ny;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
@@ -368,18 +378,21 @@ batch_kernel(BatchArgs<S> B) {
                     P_tst[k] = v0;
                     P_fl[k] = 1;
                 }
-                for (int iy = lane; iy < ny; iy += 32) P_rng[iy] = make_int2(1, nx - 2);
+                for (int iy = lane; iy < ny; iy += 32) {
+                    P_rng[iy] = make_int2(1, nx - 2);
+                    P_rng[ny + iy] = make_int2(0x7fffffff, -1);
+                }
                 __syncwarp();
                 AdjPolicyW32 Q;
                 Q.nx = nx;
                 Q.ny = ny;
                 Q.W = P_W;
                 Q.C0 = P_C0;
-                Q.vmax = 0.0;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_tst;
                 Q.flags = P_fl;
                 Q.rng = P_rng;
+                Q.crng = P_rng + ny;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
@@ -389,9 +402,18 @@ batch_kernel(BatchArgs<S> B) {
                         const double L1 = warp_sum(l1) / (double)(nx * ny);
                         const double Linf = warp_max(linf);
                         if (L1 < 1e-9 && Linf < 1e-9) break;
-                        // FP32 fixed point: no cell changed by more than a few ulps
-                        const double vmax = warp_max(Q.vmax);
-                        Q.vmax = 0.0;
+                        // FP32 fixed point: no cell changed by more than a few
+                        // ulps of the field's largest magnitude
+                        float vm = 0.f;
+                        const float4* T4 = reinterpret_cast<const float4*>(P_Ta);
+                        for (size_t k = lane; k < n / 4; k += 32) {
+                            const float4 q = T4[k];
+                            vm = fmaxf(vm, fmaxf(fmaxf(fabsf(q.x), fabsf(q.y)),
+                                                 fmaxf(fabsf(q.z), fabsf(q.w))));
+                        }
+                        for (size_t k = (n / 4) * 4 + lane; k < n; k += 32)
+                            vm = fmaxf(vm, fabsf(P_Ta[k]));
+                        const double vmax = warp_max((double)vm);
                         if (Linf <= 4.0 * 5.960464477539063e-08 * vmax) break;
                     }
             }

@@ -166,6 +166,7 @@ struct FwdBase {
     int nx, ny;
     unsigned char* flags;  // per event
     int2* rng;           // per row: x range of flag bit 0 (systolic.cuh)
+    int2* crng;          // per row: x range changed in this iteration
     const Q4<S>* pk;     // per event
     const Q4<S>* mt;     // per period (general metric) or null
     const S* a_row;      // iso: [ny]
@@ -398,6 +399,7 @@ struct AdjPolicyExact {
     double dx, dy;
     unsigned char* flags;
     int2* rng;
+    int2* crng;
     const Q4<double>* aq;
     const double2* dd;
     double* Ta;
@@ -485,11 +487,11 @@ struct AdjPolicyW32 {
     int nx, ny;
     unsigned char* flags;
     int2* rng;
+    int2* crng;
     const Q4<float>* W;
     const float* C0;
     float* Ta;
     float* Ta_start;
-    double vmax;        // max |Ta| seen in the last sweep of an iteration
 
     __device__ int nrows() const { return ny - 2; }
     __device__ int ncols() const { return nx - 2; }
@@ -528,11 +530,10 @@ struct AdjPolicyW32 {
         const float typ = yp.has ? yp.v : 0.f;
         return cur.c0 + cur.w.x * txm + cur.w.y * txp + cur.w.z * tym + cur.w.w * typ;
     }
-    __device__ void account(const Cell& cur, float nv, double& l1, double& linf) {
+    __device__ void account(const Cell& cur, float nv, double& l1, double& linf) const {
         const double dv = fabs((double)nv - (double)cur.vs);
         l1 += dv;
         linf = fmax(linf, dv);
-        vmax = fmax(vmax, fabs((double)nv));
     }
     __device__ void store(int k, float v, bool write_v, bool write_start) const {
         if (write_v) Ta[k] = v;

@@ -58,7 +58,8 @@ struct Nb {
 //   xp / yp the downwind neighbours in sweep order, account(cur, v, l1, linf)
 //   (last sweep of an iteration), store(k, v, write_v, write_start),
 //   store_flag(k, f), cp_of(ix, xd) (grid x -> sweep-ordered column, the
-//   inverse of col) and rng (per-row x range of flag bit 0, see below).
+//   inverse of col), rng and crng (per-row x ranges of flag bit 0 and of
+//   cells changed in the current iteration, see below).
 template <class V>
 __device__ __forceinline__ bool same_bits(V a, V b);
 template <>
@@ -81,6 +82,7 @@ struct March {
     unsigned pfl;       // flags of this lane's previous cell
     int rmin, rmax;     // grid x range of this row's cells left with bit 0 set
     int umin, umax;     // lane 0: grid x where its row changed (bit 0 set above)
+    int cmin, cmax;     // grid x range of this row's cells changed in this march
     int uf, ul;         // sweep columns where the row above changed in this sweep
     int lf, ll;         // sweep columns where the strip's last row changed
 };
@@ -142,6 +144,10 @@ __device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t,
             wst = !same_bits(nv, cur.vs);
         }
         if (chg || wst) p.store(L.ioff + ix, nv, chg, wst);
+        if (chg) {
+            L.cmin = min(L.cmin, ix);
+            L.cmax = max(L.cmax, ix);
+        }
         L.prev_v = nv;
         L.prev_x = cur.x;
     }
@@ -180,11 +186,13 @@ __device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t,
 // there: each lane takes its previous cell (value, aux, flags) from memory
 // and the pipeline is filled from that column.  After `lastd` (the last such
 // column) and one step in which no cell changed, nothing can change any
-// more: the march stops.  A strip with nothing to do is not marched.  The
-// last sweep of an iteration marches every cell (its convergence sums and
-// start-of-iteration copy need all of them).  All of this is exact: the
-// cells not visited are exactly those the full march would have left
-// bit-identical.
+// more: the march stops.  A strip with nothing to do is not marched.
+// The last sweep of an iteration also visits every cell that changed since
+// the iteration began (p.crng[iy], the x range of such cells per row): only
+// those can add to the convergence sums or differ from the
+// start-of-iteration copy; every other cell adds an exact zero.  All of
+// this is exact: the cells not visited are exactly those the full march
+// would have left bit-identical and whose sums terms are zero.
 //
 // P::kLead = how many steps ahead a lane loads its row (1 for the long
 // forward update, more for the short adjoint update).
@@ -209,19 +217,20 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         // columns (sweep order) this strip's march must cover
         int fc = NC, lc = -1;
         if (act) {
-            const int2 r = p.rng[iy];
+            int2 r = p.rng[iy];
+            if (last) {
+                const int2 q = p.crng[iy];
+                r.x = min(r.x, q.x);
+                r.y = max(r.y, q.y);
+            }
             if (r.x <= r.y) {
                 const int a = p.cp_of(r.x, xd), b = p.cp_of(r.y, xd);
                 fc = min(a, b);
                 lc = max(a, b);
             }
         }
-        int first = min(__reduce_min_sync(FULL_MASK, fc), uf);
-        int lastd = max(__reduce_max_sync(FULL_MASK, lc), ul);
-        if (last) {
-            first = 0;
-            lastd = NC;
-        }
+        const int first = min(__reduce_min_sync(FULL_MASK, fc), uf);
+        const int lastd = max(__reduce_max_sync(FULL_MASK, lc), ul);
         if (first >= NC) {   // no cell of the strip can change
             uf = NC;
             ul = -1;
@@ -252,6 +261,8 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         L.rmax = -1;
         L.umin = 0x7fffffff;
         L.umax = -1;
+        L.cmin = 0x7fffffff;
+        L.cmax = -1;
         L.bal = 0u;
         L.pfl = 0u;
         L.prev_v = V(0);
@@ -308,8 +319,20 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
             }
         }
         // every cell of the row that had bit 0 set was visited: the range is
-        // replaced; lane 0 then adds where it set bit 0 in the row above
-        if (act) p.rng[iy] = make_int2(L.rmin, L.rmax);
+        // replaced; lane 0 then adds where it set bit 0 in the row above.
+        // Cells changed since the iteration began: added to, or (after the
+        // last sweep, whose copy makes start == current) cleared.
+        if (act) {
+            p.rng[iy] = make_int2(L.rmin, L.rmax);
+            if (last) {
+                p.crng[iy] = make_int2(0x7fffffff, -1);
+            } else if (L.cmin <= L.cmax) {
+                int2 q = p.crng[iy];
+                q.x = min(q.x, L.cmin);
+                q.y = max(q.y, L.cmax);
+                p.crng[iy] = q;
+            }
+        }
         __syncwarp();
         if (L.eup && L.umin <= L.umax) {
             int2 r = p.rng[iy_up];
