@@ -261,6 +261,13 @@ struct FwdPolicy64 : FwdBase<double, ISO> {
     }
 };
 
+// FP32 division in the FP32 forward update: the hardware approximate
+// reciprocal (2 ulp over the operand range used here: |denominator| in
+// [1e-30, 2^126]).
+#ifndef SA_FDIV
+#define SA_FDIV(a, b) __fdividef((a), (b))
+#endif
+
 // FP32 forward update in increment form.  The stored field is u = tau - 1
 // (tau ~ 1 everywhere, so u keeps ~20x more absolute resolution than tau),
 // and each stencil is solved for the increment D = u - u_neighbour.  This is
@@ -311,15 +318,17 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
         const float sq = sqrtf(disc);
         const float qq = -0.5f * (be + copysignf(sq, be));
         float Dr[2];
-        Dr[0] = qq / al;
-        Dr[1] = (qq != 0.f) ? ga / qq : Dr[0];
+        Dr[0] = SA_FDIV(qq, al);
+        Dr[1] = (qq != 0.f) ? SA_FDIV(ga, qq) : Dr[0];
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const float D = Dr[r];
             const float Tx = fmaf(A1, D, A0);
             const float Ty = fmaf(B1, D, B0);
-            const float char_x = ISO ? aij * Tx : aij * Tx - cij * Ty;
-            const float char_y = ISO ? bij * Ty : bij * Ty - cij * Tx;
+            // isotropic metric: a, b > 0, so the characteristic has the
+            // signs of (Tx, Ty)
+            const float char_x = ISO ? Tx : aij * Tx - cij * Ty;
+            const float char_y = ISO ? Ty : bij * Ty - cij * Tx;
             if (-sx * char_x >= 0.f && -sy * char_y >= 0.f) {
                 const float c = ux + D;
                 if (c < u) u = c;
@@ -327,15 +336,16 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
         }
     }
     if (det > 0.f) {
-        const float disx = sqrtf(f2 * bij / det);
-        const float disy = sqrtf(f2 * aij / det);
+        const float disx = sqrtf(SA_FDIV(f2 * bij, det));
+        const float disy = sqrtf(SA_FDIV(f2 * aij, det));
         auto one_point = [&](const Nb<float, float>& n, float g, float kk, int s, float dis) {
             // (T0 tau)_axis = g*tau - s*kk*(tau - tau_n) = +-dis
             const float g1 = fmaf(g, n.v, g);
             const float den = g - s * kk;
+            const float rden = SA_FDIV(1.f, den);
 #pragma unroll
             for (int sgn = 0; sgn < 2; sgn++) {
-                const float D = ((sgn == 0 ? dis : -dis) - g1) / den;
+                const float D = ((sgn == 0 ? dis : -dis) - g1) * rden;
                 const float c = n.v + D;
                 // (1+c)*t0 >= (1+u_n)*T0_n  and  1+c > 0.5*(1+u_n)
                 const float lhs = (t0 - n.x) + (c * t0 - n.v * n.x);
