@@ -571,7 +571,7 @@ struct AdjPolicyExact {
 // rewritten as Ta = c0 + wxm*Ta(ix-1) + wxp*Ta(ix+1) + wym*Ta(iy-1) + wyp*Ta(iy+1)
 // with FP32 weights computed in FP64 (w = {wxm, wxp, wym, wyp}, c0 separate).
 #ifndef SA_ADJ32_LEAD
-#define SA_ADJ32_LEAD 3
+#define SA_ADJ32_LEAD 2
 #endif
 struct AdjPolicyW32 {
     using V = float;
