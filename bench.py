@@ -320,6 +320,45 @@ def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx):
             "dtype": "f64"}
 
 
+def per_solve_timing(w, svel, nev=4):
+    """The plain per-solve form: FP64, one forward and one adjoint call per
+    event through the single-solve C ABI with host arrays, as the reference's
+    forward_for_event calls eikonal::FSM_UW_PS_lonlat_2d and
+    FSM_O1_JSE_lonlat_2d (src/preproc.cpp:88-127), receiver interpolation and
+    residuals on the host."""
+    from surfattpp_b200 import eikonal
+    m11, m12, m22 = w.media()
+    ev = w.events()
+    X, Y = w.xx_deg, w.yy_deg
+    dx, dy = X[1] - X[0], Y[1] - Y[0]
+
+    def bilinear(T, x, y):
+        i = np.clip(((x - X[0]) / dx).astype(int), 0, X.size - 2)
+        j = np.clip(((y - Y[0]) / dy).astype(int), 0, Y.size - 2)
+        r, q = (x - X[i]) / dx, (y - Y[j]) / dy
+        return ((1 - r) * (1 - q) * T[j, i] + r * (1 - q) * T[j, i + 1]
+                + (1 - r) * q * T[j + 1, i] + r * q * T[j + 1, i + 1])
+
+    rng = np.random.default_rng(11)
+    keep = np.sort(rng.choice(w.n_events, size=min(nev, w.n_events), replace=False))
+    t0 = time.perf_counter()
+    for e in keep:
+        ip = int(ev["iper"][e])
+        a0, b0, c0 = m11[ip], m22[ip], -m12[ip]
+        T = eikonal.FSM_UW_PS_lonlat_2d(X, Y, a0, b0, c0, 1.0 / svel[ip], ev["evlo"][e],
+                                        ev["evla"][e])
+        r = ev["rec_idx"][ev["rec_ptr"][e]:ev["rec_ptr"][e + 1]]
+        o = slice(ev["rec_ptr"][e], ev["rec_ptr"][e + 1])
+        xr, yr = ev["stlo"][r], ev["stla"][r]
+        sadj = ev["weight"][o] * (bilinear(T, xr, yr) - ev["tt_obs"][o])
+        Ta = eikonal.FSM_O1_JSE_lonlat_2d(X, Y, a0, b0, c0, T, xr, yr, sadj)
+        eikonal.mask_uniform_grid(X, Y, Ta, ev["evlo"][e], ev["evla"][e])
+    dt = time.perf_counter() - t0
+    return {"value": keep.size / dt, "unit": UNIT, "events": int(keep.size), "dtype": "f64",
+            "note": "one FP64 forward + adjoint solve per call (single-solve C ABI, host "
+                    "arrays, wall clock)"}
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -428,6 +467,7 @@ def main():
     if world == 1 and not a.no_extras:
         extra["misfit_gradient"] = misfit_gradient_timing(a, w, plan, tt, wt, dev, stream)
         extra["fp64_plain"] = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx)
+        extra["fp64_per_solve"] = per_solve_timing(w, svel)
         extra["pde_smooth"] = pde_smooth_timing(a, w, dev, stream, peaks()[0])
         extra["topo_media"] = topo_media_timing(dev, stream)
 
