@@ -404,9 +404,11 @@ __device__ __forceinline__ float fsm_update_delta_flat(float u, float t0, float 
         const bool ok = nxn.has && nyn.has && disc >= 0.f && fabsf(al) >= 1e-30f;
         const float sq = sqrtf(fmaxf(disc, 0.f));
         const float qq = -0.5f * (be + copysignf(sq, be));
+        // the second root as ga / qq also when qq == 0: then it is +-inf or
+        // NaN and fails the tests below, and the first root is the only one
         float Dr[2];
         Dr[0] = SA_FDIV(qq, al);
-        Dr[1] = (qq != 0.f) ? SA_FDIV(ga, qq) : Dr[0];
+        Dr[1] = SA_FDIV(ga, qq);
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const float D = Dr[r];
@@ -414,7 +416,9 @@ __device__ __forceinline__ float fsm_update_delta_flat(float u, float t0, float 
             const float Ty = fmaf(B1, D, B0);
             const float char_x = ISO ? Tx : aij * Tx - cij * Ty;
             const float char_y = ISO ? Ty : bij * Ty - cij * Tx;
-            const bool take = ok && -sx * char_x >= 0.f && -sy * char_y >= 0.f;
+            // both characteristic components point away from the neighbours
+            // (a NaN root makes both NaN and fails)
+            const bool take = ok && fminf(-sx * char_x, -sy * char_y) >= 0.f;
             best = take ? fminf(best, ux + D) : best;
         }
     }
@@ -426,12 +430,13 @@ __device__ __forceinline__ float fsm_update_delta_flat(float u, float t0, float 
         const float g1 = fmaf(g, n.v, g);
         const float rden = SA_FDIV(1.f, g - s * kk);
         const bool ok = okd && n.has;
+        // (1+c)*t0 >= (1+u_n)*T0_n  and  1+c > 0.5*(1+u_n)
+        const float kn = t0 - fmaf(n.v, n.x, n.x);
+        const float half = fmaf(0.5f, n.v, -0.5f);
 #pragma unroll
         for (int sgn = 0; sgn < 2; sgn++) {
             const float c = n.v + ((sgn == 0 ? dis : -dis) - g1) * rden;
-            // (1+c)*t0 >= (1+u_n)*T0_n  and  1+c > 0.5*(1+u_n)
-            const float lhs = (t0 - n.x) + (c * t0 - n.v * n.x);
-            const bool take = ok && lhs >= 0.f && c > 0.5f * n.v - 0.5f;
+            const bool take = ok && fmaf(c, t0, kn) >= 0.f && c > half;
             best = take ? fminf(best, c) : best;
         }
     };
