@@ -25,6 +25,7 @@ EXPORTED = (
     "sa_eik_fwd_field", "sa_eik_adj_field", "sa_mask_uniform_grid",
     "sa_plan_create", "sa_plan_destroy", "sa_plan_set_graph", "sa_plan_forward_adjoint",
     "sa_forward_for_events", "sa_plan_debug_fields", "sa_plan_kernel_timing", "sa_plan_kernel_ms",
+    "sa_plan_autotune", "sa_plan_set_tune", "sa_plan_get_tune",
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
     "sa_depthkernel_columns_group",
     "sa_eik_fwd_field_noalloc",
@@ -82,6 +83,10 @@ def lib():
     L.sa_plan_debug_fields.argtypes = [_vp, _vp, _vp]
     L.sa_plan_kernel_timing.argtypes = [_vp, i]
     L.sa_plan_kernel_ms.argtypes = [_vp, C.POINTER(C.c_float)]
+    L.sa_plan_autotune.argtypes = [_vp] * 7 + [i, _vp, C.POINTER(C.c_float), C.POINTER(i),
+                                              C.POINTER(i), _vp]
+    L.sa_plan_set_tune.argtypes = [_vp, i, i]
+    L.sa_plan_get_tune.argtypes = [_vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.sa_forward_for_events.argtypes = [_vp, i, i, i, i, _dp, _dp, _dp, _vp, _vp, _vp, i, _dp,
                                         _dp, _ip, _ip, _ip, i, _dp, _dp, _dp, _dp, i, _dp, _dp,
                                         C.POINTER(d), _ip, _ip]

@@ -92,7 +92,14 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     return L;
 }
 
-template <class S, bool ISO>
+// Launch variants of the FP32 kernel (kBatchVariants, chosen per plan by
+// sa_plan_autotune): bit 0 = unrolled forward step (else one rolled copy),
+// bit 1 = FP32 adjoint loads 3 steps ahead (else 2).  The FP64 kernel has
+// variant 0 only.
+__host__ __device__ constexpr bool variant_fwd_rolled(int v) { return (v & 1) == 0; }
+__host__ __device__ constexpr int variant_adj_lead(int v) { return (v & 2) ? 3 : 2; }
+
+template <class S, bool ISO, int VAR>
 __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo& si, int ip,
                                             int src, S* tau, S* tst, Q4<S>* pk,
                                             unsigned char* flags, int2* rng, double* T,
@@ -103,7 +110,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     const int lane = threadIdx.x & 31;
     const double fun0_64 = bilinear64(B.fun64 + (size_t)ip * n, nx, si.idx0, si.idy0, si.r1, si.r2);
     using Pol = typename std::conditional<sizeof(S) == sizeof(double), FwdPolicy64<ISO>,
-                                          FwdPolicyDelta32<ISO>>::type;
+                                          FwdPolicyDelta32<ISO, variant_fwd_rolled(VAR)>>::type;
     Pol P;
     P.nx = nx;
     P.ny = ny;
@@ -190,7 +197,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     return fun0_64;
 }
 
-template <class S, bool ISO>
+template <class S, bool ISO, int VAR>
 __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? SA_MINB64 : SA_MINB32)
 batch_kernel(BatchArgs<S> B) {
     const int lane = threadIdx.x & 31;
@@ -224,8 +231,8 @@ batch_kernel(BatchArgs<S> B) {
 
         if (B.mode != MODE_ADJ_ONLY) {
             int iters = 0;
-            fwd_solve<S, ISO>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_fl, P_rng, P_T,
-                              iters, status);
+            fwd_solve<S, ISO, VAR>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_fl, P_rng,
+                                   P_T, iters, status);
             if (lane == 0 && B.out.fwd_iters) B.out.fwd_iters[e] = iters;
             if (B.out.T_out)
                 for (size_t k = lane; k < n; k += 32) B.out.T_out[(size_t)e * n + k] = P_T[k];
@@ -383,7 +390,7 @@ batch_kernel(BatchArgs<S> B) {
                     P_rng[ny + iy] = make_int2(0x7fffffff, -1);
                 }
                 __syncwarp();
-                AdjPolicyW32 Q;
+                AdjPolicyW32<variant_adj_lead(VAR)> Q;
                 Q.nx = nx;
                 Q.ny = ny;
                 Q.W = P_W;

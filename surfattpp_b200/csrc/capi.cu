@@ -9,6 +9,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -81,6 +83,9 @@ struct sa_ctx {
     LayerConstCache lc;
     PeriodCache pc;
     DArr<double> red;   // reduction scratch of the optimizer entry points
+    // launch configuration chosen by sa_plan_autotune per grid size:
+    // (nx, ny, precision) -> (variant, active slots; 0 = all)
+    std::map<std::array<int, 3>, std::array<int, 2>> tune;
 };
 
 namespace {
@@ -125,6 +130,8 @@ struct sa_plan {
     size_t sort_bytes = 0;
     int nslots = 0;
     size_t slot_bytes = 0;
+    int variant = 0;      // FP32 batch-kernel launch variant (batch.cuh)
+    int active = 0;       // event slots in use (0 = all nslots)
     double* dbg_T = nullptr;
     double* dbg_Ta = nullptr;
     bool use_graph = true;
@@ -448,8 +455,9 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
     d.ev.stlo = P->stlo.p;
     d.ev.stla = P->stla.p;
     d.ev.cos_stla = P->cos_stla.p;
-    d.sc.nslots = P->nslots;
+    d.sc.nslots = (P->active > 0 && P->active < P->nslots) ? P->active : P->nslots;
     d.sc.slot_bytes = P->slot_bytes;
+    d.variant = P->prec == SA_FP32 ? P->variant : 0;
     d.sc.base = P->scratch.p;
     d.sc.queue = P->queue.p;
     d.maxr = P->maxr;
@@ -529,11 +537,99 @@ extern "C" int sa_plan_create(sa_ctx* ctx, int precision, int nx, int ny, int np
         delete P;
         return rc;
     }
+    // a configuration tuned earlier for this grid size
+    const auto it = ctx->tune.find({nx, ny, precision});
+    if (it != ctx->tune.end()) {
+        P->variant = it->second[0];
+        P->active = it->second[1];
+    }
     *out = P;
     return SA_OK;
 }
 
 extern "C" void sa_plan_destroy(sa_plan* plan) { delete plan; }
+
+// Launch-configuration autotuner.  Candidates: every FP32 launch variant
+// (rolled / unrolled forward step x adjoint load lead 2 / 3; FP64: the one
+// kernel) x all or three quarters of the resident event slots.  Each
+// candidate runs the plan's own evaluation twice, the second timed with
+// CUDA events around the batch kernel; the fastest is kept for this plan and
+// for plans of the same grid size created later on this context.  FP64
+// results do not depend on the choice (only the atomic accumulation order of
+// adj_s varies); the FP32 variants run the same arithmetic, but the compiler
+// may fuse multiply-adds differently in each, so their results differ by
+// FP32 rounding.
+extern "C" int sa_plan_autotune(sa_plan* P, const double* svel, const double* m11,
+                                const double* m12, const double* m22, const double* tt_obs,
+                                const double* weight, int calc_adj, double* adj_s,
+                                float* ms_out, int* n_out, int* choice, void* stream) {
+    if (!P) return SA_ERR_ARG;
+    sa_ctx* ctx = P->ctx;
+    if (!svel) return fail(ctx, SA_ERR_ARG, "svel is required");
+    if ((m11 == nullptr) != (m22 == nullptr) || (m11 == nullptr) != (m12 == nullptr))
+        return fail(ctx, SA_ERR_ARG, "m11, m12, m22 must be all set or all NULL");
+    if (P->npair > 0 && (!tt_obs || !weight)) return fail(ctx, SA_ERR_ARG, "tt_obs/weight");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const int nvar = P->prec == SA_FP32 ? kBatchVariants : 1;
+    const int slots[2] = {0, std::max(1, P->nslots * 3 / 4)};
+    const int ncand = 2 * nvar;
+    const bool had_timing = P->timing;
+    if (!P->tk0) {
+        SA_CUDA(cudaEventCreate(&P->tk0));
+        SA_CUDA(cudaEventCreate(&P->tk1));
+    }
+    P->timing = true;
+    float best = 0.f;
+    int best_c = 0;
+    for (int c = 0; c < ncand; c++) {
+        P->variant = c % nvar;
+        P->active = slots[c / nvar];
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; rep++) {
+            const int rc = plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj,
+                                        nullptr, adj_s, nullptr, nullptr, nullptr, nullptr, st);
+            if (rc) {
+                P->timing = had_timing;
+                return rc;
+            }
+        }
+        SA_CUDA(cudaEventSynchronize(P->tk1));
+        SA_CUDA(cudaEventElapsedTime(&ms, P->tk0, P->tk1));
+        if (ms_out) ms_out[c] = ms;
+        if (c == 0 || ms < best) {
+            best = ms;
+            best_c = c;
+        }
+    }
+    P->timing = had_timing;
+    P->variant = best_c % nvar;
+    P->active = slots[best_c / nvar];
+    P->have_graph = false;
+    ctx->tune[{P->nx, P->ny, P->prec}] = {P->variant, P->active};
+    if (n_out) *n_out = ncand;
+    if (choice) *choice = best_c;
+    return SA_OK;
+}
+
+extern "C" int sa_plan_set_tune(sa_plan* P, int variant, int active_slots) {
+    if (!P) return SA_ERR_ARG;
+    const int nvar = P->prec == SA_FP32 ? kBatchVariants : 1;
+    if (variant < 0 || variant >= nvar || active_slots < 0)
+        return fail(P->ctx, SA_ERR_ARG, "sa_plan_set_tune: variant or active_slots out of range");
+    P->variant = variant;
+    P->active = active_slots;
+    P->have_graph = false;
+    return SA_OK;
+}
+
+extern "C" int sa_plan_get_tune(sa_plan* P, int* variant, int* active_slots, int* nslots) {
+    if (!P) return SA_ERR_ARG;
+    if (variant) *variant = P->variant;
+    if (active_slots) *active_slots = P->active > 0 ? std::min(P->active, P->nslots) : P->nslots;
+    if (nslots) *nslots = P->nslots;
+    return SA_OK;
+}
 
 extern "C" int sa_plan_set_graph(sa_plan* plan, int enable) {
     if (!plan) return SA_ERR_ARG;

@@ -33,16 +33,28 @@ size_t batch32_slot_bytes(int nx, int ny, int maxr) {
 int batch32_max_slots(int device) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<float, true>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<float, true, 0>, 128, 0);
     if (per_sm < 1) per_sm = 1;
     return nsm * per_sm * 4;
 }
 
+namespace {
+template <int VAR>
+void launch_variant(const BatchDesc& d, const BatchArgs<float>& B, int blocks, cudaStream_t st) {
+    if (d.iso) batch_kernel<float, true, VAR><<<blocks, 128, 0, st>>>(B);
+    else batch_kernel<float, false, VAR><<<blocks, 128, 0, st>>>(B);
+}
+}  // namespace
+
 cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st) {
     const BatchArgs<float> B = make_batch_args<float>(d);
     const int blocks = (d.sc.nslots + 3) / 4;
-    if (d.iso) batch_kernel<float, true><<<blocks, 128, 0, st>>>(B);
-    else batch_kernel<float, false><<<blocks, 128, 0, st>>>(B);
+    switch (d.variant) {
+        case 1: launch_variant<1>(d, B, blocks, st); break;
+        case 2: launch_variant<2>(d, B, blocks, st); break;
+        case 3: launch_variant<3>(d, B, blocks, st); break;
+        default: launch_variant<0>(d, B, blocks, st); break;
+    }
     return cudaGetLastError();
 }
 

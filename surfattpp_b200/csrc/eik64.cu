@@ -96,7 +96,7 @@ size_t batch64_slot_bytes(int nx, int ny, int maxr) {
 int batch64_max_slots(int device) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<double, true>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<double, true, 0>, 128, 0);
     if (per_sm < 1) per_sm = 1;
     return nsm * per_sm * 4;
 }
@@ -137,8 +137,8 @@ template cudaError_t launch_geometry<float>(int, int, int, const double*, const 
 cudaError_t launch_batch64(const BatchDesc& d, cudaStream_t st) {
     const BatchArgs<double> B = make_batch_args<double>(d);
     const int blocks = (d.sc.nslots + 3) / 4;
-    if (d.iso) batch_kernel<double, true><<<blocks, 128, 0, st>>>(B);
-    else batch_kernel<double, false><<<blocks, 128, 0, st>>>(B);
+    if (d.iso) batch_kernel<double, true, 0><<<blocks, 128, 0, st>>>(B);
+    else batch_kernel<double, false, 0><<<blocks, 128, 0, st>>>(B);
     return cudaGetLastError();
 }
 

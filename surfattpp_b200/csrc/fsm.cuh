@@ -147,15 +147,14 @@ struct MetricCell<S, true> {};
 #ifndef SA_FWD_LEAD
 #define SA_FWD_LEAD 1
 #endif
-#ifndef SA_FWD_ROLLED
-#define SA_FWD_ROLLED 1
-#endif
-template <class S, bool ISO>
+// ROLLED: one copy of the sweep step with register moves (the default) or
+// the step unrolled with statically rotated buffers (systolic.cuh).
+template <class S, bool ISO, bool ROLLED = true>
 struct FwdBase {
     using V = S;
     using X = S;
     static constexpr int kLead = SA_FWD_LEAD;
-    static constexpr bool kRolled = SA_FWD_ROLLED;
+    static constexpr bool kRolled = ROLLED;
     struct Cell {
         S v;    // field before this update
         S x;    // T0 of the cell
@@ -452,9 +451,9 @@ __device__ __forceinline__ float fsm_update_delta_flat(float u, float t0, float 
 #endif
 
 // FP32 forward: field u = tau - 1, increment-form update.
-template <bool ISO>
-struct FwdPolicyDelta32 : FwdBase<float, ISO> {
-    using Base = FwdBase<float, ISO>;
+template <bool ISO, bool ROLLED = true>
+struct FwdPolicyDelta32 : FwdBase<float, ISO, ROLLED> {
+    using Base = FwdBase<float, ISO, ROLLED>;
     using Cell = typename Base::Cell;
     using Base::row_fixed;
     using Base::fix_x0;
@@ -575,13 +574,12 @@ struct AdjPolicyExact {
 // Adjoint sweep policy, FP32 weight form: the same Gauss-Seidel update
 // rewritten as Ta = c0 + wxm*Ta(ix-1) + wxp*Ta(ix+1) + wym*Ta(iy-1) + wyp*Ta(iy+1)
 // with FP32 weights computed in FP64 (w = {wxm, wxp, wym, wyp}, c0 separate).
-#ifndef SA_ADJ32_LEAD
-#define SA_ADJ32_LEAD 2
-#endif
+// LEAD: how many steps ahead the sweep loads (2 by default).
+template <int LEAD = 2>
 struct AdjPolicyW32 {
     using V = float;
     using X = float;
-    static constexpr int kLead = SA_ADJ32_LEAD;
+    static constexpr int kLead = LEAD;
     static constexpr bool kRolled = false;
     struct Cell {
         float v;

@@ -39,7 +39,11 @@ struct BatchDesc {
     Scratch sc;
     int maxr;
     int mode;
+    int variant;   // FP32 launch variant (batch.cuh), 0 = default
 };
+
+// Number of FP32 batch-kernel launch variants (batch.cuh).
+constexpr int kBatchVariants = 4;
 
 size_t batch64_slot_bytes(int nx, int ny, int maxr);
 int batch64_max_slots(int device);

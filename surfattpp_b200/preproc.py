@@ -69,6 +69,32 @@ class ForwardAdjointPlan:
         _capi.check(self.ctx.h, _capi.lib().sa_plan_kernel_ms(self.h, C.byref(ms)))
         return ms.value
 
+    def autotune(self, svel, tt_obs, weight, calc_adj=True, m11=None, m12=None, m22=None,
+                 adj_s=None, stream=None):
+        """Pick the fastest batch-kernel launch configuration on this plan's own
+        workload (sa_plan_autotune); kept for this plan and later plans of the
+        same grid size on its context.  Returns dict(ms=[per candidate],
+        choice=index, variant, active_slots, nslots)."""
+        ms = (C.c_float * 8)()
+        n, ch = C.c_int(0), C.c_int(0)
+        rc = _capi.lib().sa_plan_autotune(self.h, ptr(svel), ptr(m11), ptr(m12), ptr(m22),
+                                          ptr(tt_obs), ptr(weight), int(bool(calc_adj)),
+                                          ptr(adj_s), ms, C.byref(n), C.byref(ch), stream)
+        _capi.check(self.ctx.h, rc)
+        return dict(ms=list(ms)[:n.value], choice=ch.value, **self.tune())
+
+    def set_tune(self, variant, active_slots=0):
+        """Use a known launch configuration (sa_plan_set_tune)."""
+        _capi.check(self.ctx.h, _capi.lib().sa_plan_set_tune(self.h, int(variant),
+                                                             int(active_slots)))
+
+    def tune(self):
+        """Current launch configuration: variant, active_slots, nslots."""
+        v, a, n = C.c_int(0), C.c_int(0), C.c_int(0)
+        _capi.check(self.ctx.h, _capi.lib().sa_plan_get_tune(self.h, C.byref(v), C.byref(a),
+                                                             C.byref(n)))
+        return dict(variant=v.value, active_slots=a.value, nslots=n.value)
+
     def debug_fields(self, T_out=None, Ta_out=None):
         _capi.lib().sa_plan_debug_fields(self.h, ptr(T_out), ptr(Ta_out))
 
