@@ -101,19 +101,18 @@ def _stations(rng, xx, yy, nsta, margin_cells=2):
 
 
 def _all_pairs_events(stlo, stla, nper):
-    """Every station is a source for every period; all others are receivers."""
+    """Every station is a source for every period (station-major, then
+    period); all other stations, in order, are its receivers."""
     nsta = stlo.size
-    evlo, evla, iper, ptr, idx = [], [], [], [0], []
-    for s in range(nsta):
-        for p in range(nper):
-            evlo.append(stlo[s])
-            evla.append(stla[s])
-            iper.append(p)
-            rec = [r for r in range(nsta) if r != s]
-            idx.extend(rec)
-            ptr.append(len(idx))
-    return (np.array(evlo), np.array(evla), np.array(iper, np.int32), np.array(ptr, np.int32),
-            np.array(idx, np.int32))
+    ne = nsta * nper
+    src = np.repeat(np.arange(nsta), nper)
+    iper = np.tile(np.arange(nper, dtype=np.int32), nsta)
+    ptr = (np.arange(ne + 1, dtype=np.int64) * (nsta - 1)).astype(np.int32)
+    # receivers of source s: 0..s-1, s+1..nsta-1
+    r = np.tile(np.arange(nsta - 1, dtype=np.int32), ne)
+    idx = r + (r >= np.repeat(src, nsta - 1)).astype(np.int32)
+    return (np.asarray(stlo)[src].astype(float), np.asarray(stla)[src].astype(float), iper, ptr,
+            idx.astype(np.int32))
 
 
 def checker_pattern(nx, ny, nz, nxw, nyw, nzw):
@@ -191,6 +190,31 @@ def config3(seed=1003, nsta=400, nper=20, n=301):
     return Workload(f"C3 batched {n}x{n}x{z.size}, {nper} periods, {nsta} stations, "
                     f"{nsta * nper} solves", xx, yy, z, vs, periods, stlo, stla, evlo, evla,
                     iper, ptr, idx, tt, np.ones(idx.size), meta=dict(vs_start=vs0))
+
+
+def config5(seed=1005, nsta=1000, nper=30, n=601):
+    """Full-inversion case: 601x601x50 at 0.005 deg (0-98 km), GRF +-6 %
+    (15 km) on the gradient, 1000 stations, 30 periods 1-60 s: 30000 forward +
+    adjoint solves per misfit gradient.  tt_obs are straight-ray times at a
+    per-period reference velocity (the inversion benchmark replaces them with
+    the engine's synthetic times in the GRF model)."""
+    rng = np.random.default_rng(seed)
+    xx, yy = _grid(102.0, 24.0, (n, n), 0.005)
+    z = np.arange(0.0, 98.0 + 1e-9, 2.0)
+    vs0 = gradient_model(n, n, z)
+    dx_km = 0.005 * np.pi / 180.0 * R_EARTH
+    vs = vs0 * (1.0 + grf_perturbation(rng, n, n, z.size, dx_km, 2.0, 15.0, 0.06))
+    periods = np.geomspace(1.0, 60.0, nper)
+    stlo, stla = _stations(rng, xx, yy, nsta)
+    evlo, evla, iper, ptr, idx = _all_pairs_events(stlo, stla, nper)
+    cref = 2.9 + 0.9 * (np.log(periods) - np.log(1.0)) / (np.log(60.0) - np.log(1.0))
+    src_of_rec = np.repeat(np.repeat(np.arange(nsta), nper), np.diff(ptr))
+    per_of_rec = np.repeat(iper, np.diff(ptr))
+    d = _gc_km(stlo[src_of_rec], stla[src_of_rec], stlo[idx], stla[idx])
+    tt = d / cref[per_of_rec]
+    return Workload(f"C5 inversion {n}x{n}x{z.size}, {nper} periods, {nsta} stations, "
+                    f"{nsta * nper} solves per gradient", xx, yy, z, vs, periods, stlo, stla,
+                    evlo, evla, iper, ptr, idx, tt, np.ones(idx.size), meta=dict(vs_start=vs0))
 
 
 def fractal_topography(rng, lon, lat, relief_km=4.0, slope=-2.0):
