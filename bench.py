@@ -364,7 +364,9 @@ def per_solve_timing(w, svel, nev=4):
 
 def run_inversion(a):
     """The full inversion loop on the device (Inversion::run_inversion,
-    src/inversion.cpp:106-160): misfit gradient with FP32 sweeps, PDE kernel
+    src/inversion.cpp:106-160): misfit gradient with FP32 sweeps (through the
+    torch.autograd.Function backward; forward fields recomputed per event,
+    never stored), PDE kernel
     smoothing, FP64 L-BFGS with the strong-Wolfe line search, multiplicative
     model update.  Observed times are the engine's FP32 synthetic times in the
     GRF model; the inversion starts from the 1-D gradient.  Reports wall time
@@ -392,7 +394,8 @@ def run_inversion(a):
     del o, sv
     smooth = dict(ygrid=w.yy_deg, zgrid=w.zgrid, dx=0.005, dy=0.005, dz=2.0, sigma_h=0.025,
                   sigma_v=6.0)
-    inv = inversion.Inversion(g, tt_obs, wt, smooth=smooth, niter=a.inversion)
+    # the gradient taken through the torch.autograd.Function backward
+    inv = inversion.Inversion(g, tt_obs, wt, smooth=smooth, niter=a.inversion, autograd=True)
     vs0 = t(w.meta["vs_start"])
     inv.run_forward_adjoint(vs0)          # graph capture and first-touch, untimed
     count = [0]

@@ -138,6 +138,7 @@ def _fn():
         def forward(ctx, vs3d, grad, tt_obs, weight):
             vs = vs3d.detach().contiguous()
             out = grad.run(vs, tt_obs, weight)
+            grad.last = out      # status / svel / adj_s of this evaluation
             ctx.save_for_backward(out["ker_vs"])
             return out["chi"][0].clone()
 
@@ -170,8 +171,10 @@ class Inversion:
 
     def __init__(self, grad: MisfitGradient, tt_obs, weight, smooth=None, niter=10,
                  optim="lbfgs", step_length=0.02, max_sub_niter=10, c1=0.1, c2=0.9,
-                 maxshrink=0.8, min_derr=0.0, data_weight=1.0):
-        """smooth = dict(ygrid, zgrid, dx, dy, dz, sigma_h, sigma_v) or None."""
+                 maxshrink=0.8, min_derr=0.0, data_weight=1.0, autograd=False):
+        """smooth = dict(ygrid, zgrid, dx, dy, dz, sigma_h, sigma_v) or None.
+        autograd: take the kernel as the gradient of TravelTimeMisfit through
+        torch.autograd (the same evaluation behind a backward pass)."""
         self.g = grad
         self.tt, self.wt = tt_obs, weight
         self.smooth = smooth
@@ -179,6 +182,7 @@ class Inversion:
         self.step_length, self.max_sub_niter = step_length, int(max_sub_niter)
         self.c1, self.c2, self.maxshrink, self.min_derr = c1, c2, maxshrink, min_derr
         self.w = data_weight
+        self.autograd = bool(autograd)
         self.misfit, self.alphas, self.sub_iters, self.restarts = [], [], [], 0
         self._out = None
 
@@ -187,13 +191,20 @@ class Inversion:
         returns (misfit, ker_curr, gradient)."""
         import torch
         from . import postproc
-        out = self.g.run(vs, self.tt, self.wt, out=self._out)
-        self._out = out
+        if self.autograd:
+            v = vs.detach().clone().requires_grad_(True)
+            c = TravelTimeMisfit.apply(self.g, v, self.tt, self.wt)
+            c.backward()
+            out = self.g.last
+            ker = v.grad
+        else:
+            out = self.g.run(vs, self.tt, self.wt, out=self._out)
+            self._out = out
+            ker = out["ker_vs"]
         torch.cuda.synchronize()
         if int(out["status"][0]) != 0:
             raise _capi.SAError(int(out["status"][0]), "forward/adjoint evaluation failed")
         chi = float(out["chi"][0])
-        ker = out["ker_vs"]
         ker_curr = ker * self.w
         sm = ker.clone()
         if self.smooth is not None:

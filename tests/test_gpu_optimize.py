@@ -131,7 +131,8 @@ def _oracle_inversion(orc, w, ev, vs0, smooth, niter, step=0.02, max_sub=10):
 
 
 @pytest.mark.slow
-def test_lbfgs_inversion_follows_oracle(gpu, orc):
+@pytest.mark.parametrize("autograd", [False, True])
+def test_lbfgs_inversion_follows_oracle(gpu, orc, autograd):
     import torch
     from surfattpp_b200 import inversion, preproc
     from surfattpp_b200 import workloads as W
@@ -150,7 +151,9 @@ def test_lbfgs_inversion_follows_oracle(gpu, orc):
                                       ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
                                       ev["stla"], precision="fp64")
     g = inversion.MisfitGradient(plan, w.zgrid, w.periods)
-    inv = inversion.Inversion(g, _t(ev["tt_obs"]), _t(ev["weight"]), smooth=smooth, niter=niter)
+    # autograd: the kernel as the backward of TravelTimeMisfit (same evaluation)
+    inv = inversion.Inversion(g, _t(ev["tt_obs"]), _t(ev["weight"]), smooth=smooth, niter=niter,
+                              autograd=autograd)
     vs = inv.run(_t(vs0))
     torch.cuda.synchronize()
     assert inv.alphas == ral and inv.sub_iters == rsub
