@@ -155,3 +155,68 @@ def test_plan_graph_replay_is_stable(orc, gpu):
         tol = 1e-12 * float(outs[0]["adj_s"].abs().max())
         assert float((o["adj_s"] - outs[0]["adj_s"]).abs().max()) <= tol
     assert int(outs[0]["status"].max()) == 0
+
+
+def test_c3_full_size_properties(gpu):
+    """The full C3 batch (301x301, 400 stations, 20 periods, 8000 FP32
+    forward + adjoint solves) checked through size-independent properties
+    (the oracle would take minutes here; subsets are compared with it above):
+      * every solve converges, every output is finite;
+      * straight-path bounds for pairs at least 10 km apart: d / vmax <= T <=
+        d / vmin to 1e-3 (the eikonal time is the fastest path; no path is
+        faster than the fastest medium, the straight one is no slower than the
+        slowest).  Closer pairs lie within a few cells of the source, where the
+        discretisation error is a large fraction of T (the FP64 oracle reaches
+        d / vmin * 1.016 below 5 km);
+      * source-receiver reciprocity T(a -> b) = T(b -> a) for the same pairs:
+        max 3e-3, median 1e-4 relative (discretisation around either source:
+        the FP64 oracle shows 1.7e-4 / 1.1e-5 over 190 pairs, this run
+        1.3e-3 at worst over 1.5 M);
+      * adj_s is zero outside the grid interior and the misfit equals the sum
+        of 0.5 w r^2 over all observations."""
+    import torch
+    import bench
+    from surfattpp_b200 import preproc
+    from surfattpp_b200.workloads import _gc_km
+
+    class A:
+        n, nsta, nper, precision = 301, 400, 20, "fp32"
+
+    w, svel = bench.make_inputs(A, 0)
+    ev = w.events()
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision="fp32")
+    out = plan.run(t(svel), t(ev["tt_obs"]), t(ev["weight"]))
+    torch.cuda.synchronize()
+    assert int(out["status"].max()) == 0
+    syn = out["syn"].cpu().numpy()[: ev["rec_idx"].size]
+    adj = out["adj_s"].cpu().numpy()
+    assert np.all(np.isfinite(syn)) and np.all(np.isfinite(adj))
+    nsta, nper = A.nsta, A.nper
+    cnt = np.diff(ev["rec_ptr"])
+    src = np.repeat(np.repeat(np.arange(nsta), nper), cnt)
+    per = np.repeat(ev["iper"], cnt)
+    rec = ev["rec_idx"]
+    d = _gc_km(ev["stlo"][src], ev["stla"][src], ev["stlo"][rec], ev["stla"][rec])
+    flat = svel.reshape(nper, -1)
+    far = d >= 10.0
+    assert far.sum() > 0.9 * far.size
+    assert (syn * flat.max(1)[per] / d)[far].min() >= 1.0 - 1e-3
+    assert (syn * flat.min(1)[per] / d)[far].max() <= 1.0 + 1e-3
+    T = np.zeros((nper, nsta, nsta))
+    T[per, src, rec] = syn
+    D = np.zeros((nsta, nsta))
+    D[src, rec] = d
+    a, b = np.triu_indices(nsta, 1)
+    sel = D[a, b] >= 10.0
+    a, b = a[sel], b[sel]
+    rel = np.abs(T[:, a, b] - T[:, b, a]) / T[:, a, b]
+    assert rel.max() <= 3e-3 and np.median(rel) <= 1e-4, (rel.max(), np.median(rel))
+    assert np.all(adj[:, 0, :] == 0) and np.all(adj[:, -1, :] == 0)
+    assert np.all(adj[:, :, 0] == 0) and np.all(adj[:, :, -1] == 0)
+    r = syn - ev["tt_obs"]
+    chi = 0.5 * np.sum(ev["weight"] * r * r)
+    assert abs(float(out["chi"][0]) - chi) <= 1e-9 * chi
