@@ -85,9 +85,10 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     L.sadj = take(r * sizeof(double));
     L.syn = take(r * sizeof(double));
     L.flags = take(n);   // sweep flags (systolic.cuh), forward then adjoint
-    // per-row x ranges (systolic.cuh): [0, ny) flag bit 0, [ny, 2 ny) cells
-    // changed in the current iteration
-    L.rng = take(2 * (size_t)ny * sizeof(int2));
+    // per-row x ranges (systolic.cuh): [0, ny) cells that can change in the
+    // current sweep, [ny, 2 ny) cells changed in the current iteration,
+    // [2 ny, 3 ny) the adjoint's ranges for the next sweep
+    L.rng = take(3 * (size_t)ny * sizeof(int2));
     L.total = o;
     return L;
 }
@@ -306,11 +307,11 @@ batch_kernel(BatchArgs<S> B) {
                     const double v0 = interior ? 100.0 : 0.0;   // :446-449
                     P_Ta[k] = v0;
                     P_Tst[k] = v0;
-                    P_fl[k] = 1;
                 }
                 for (int iy = lane; iy < ny; iy += 32) {
                     P_rng[iy] = make_int2(1, nx - 2);
                     P_rng[ny + iy] = make_int2(0x7fffffff, -1);
+                    P_rng[2 * ny + iy] = make_int2(0x7fffffff, -1);
                 }
                 __syncwarp();
                 AdjPolicyExact Q;
@@ -322,9 +323,9 @@ batch_kernel(BatchArgs<S> B) {
                 Q.dd = P_DD;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_Tst;
-                Q.flags = P_fl;
                 Q.rng = P_rng;
                 Q.crng = P_rng + ny;
+                Q.rng2 = P_rng + 2 * ny;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
@@ -383,11 +384,11 @@ batch_kernel(BatchArgs<S> B) {
                     const float v0 = interior ? 100.f : 0.f;
                     P_Ta[k] = v0;
                     P_tst[k] = v0;
-                    P_fl[k] = 1;
                 }
                 for (int iy = lane; iy < ny; iy += 32) {
                     P_rng[iy] = make_int2(1, nx - 2);
                     P_rng[ny + iy] = make_int2(0x7fffffff, -1);
+                    P_rng[2 * ny + iy] = make_int2(0x7fffffff, -1);
                 }
                 __syncwarp();
                 AdjPolicyW32<variant_adj_lead(VAR)> Q;
@@ -397,9 +398,9 @@ batch_kernel(BatchArgs<S> B) {
                 Q.C0 = P_C0;
                 Q.Ta = P_Ta;
                 Q.Ta_start = P_tst;
-                Q.flags = P_fl;
                 Q.rng = P_rng;
                 Q.crng = P_rng + ny;
+                Q.rng2 = P_rng + 2 * ny;
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;

@@ -155,6 +155,7 @@ struct FwdBase {
     using X = S;
     static constexpr int kLead = SA_FWD_LEAD;
     static constexpr bool kRolled = ROLLED;
+    static constexpr bool kFlags = true;   // per-cell skip flags (systolic.cuh)
     struct Cell {
         S v;    // field before this update
         S x;    // T0 of the cell
@@ -493,6 +494,7 @@ struct AdjPolicyExact {
     using X = float;      // no auxiliary neighbour data
     static constexpr int kLead = 2;
     static constexpr bool kRolled = false;
+    static constexpr bool kFlags = false;   // ranges from changes (systolic.cuh)
     struct Cell {
         double v;
         float x;
@@ -503,9 +505,9 @@ struct AdjPolicyExact {
     };
     int nx, ny;
     double dx, dy;
-    unsigned char* flags;
     int2* rng;
     int2* crng;
+    int2* rng2;          // next sweep's ranges (flag-free march)
     const Q4<double>* aq;
     const double2* dd;
     double* Ta;
@@ -525,13 +527,12 @@ struct AdjPolicyExact {
         c.q = ld4(aq + k);
         c.de = dd[k];
         c.vs = last ? Ta_start[k] : 0.0;
-        c.fl = flags[k];
+        c.fl = 0u;
         return c;
     }
     __device__ Cell load_nb(int k) const {
         Cell c{};
         c.v = Ta[k];
-        c.fl = flags[k];
         return c;
     }
     // um / dm: upwind / downwind x neighbour in sweep order (likewise uy /
@@ -568,7 +569,6 @@ struct AdjPolicyExact {
         if (write_v) Ta[k] = v;
         if (write_start) Ta_start[k] = v;
     }
-    __device__ void store_flag(int k, unsigned f) const { flags[k] = (unsigned char)f; }
 };
 
 // Adjoint sweep policy, FP32 weight form: the same Gauss-Seidel update
@@ -581,6 +581,7 @@ struct AdjPolicyW32 {
     using X = float;
     static constexpr int kLead = LEAD;
     static constexpr bool kRolled = false;
+    static constexpr bool kFlags = false;   // ranges from changes (systolic.cuh)
     struct Cell {
         float v;
         float x;
@@ -590,9 +591,9 @@ struct AdjPolicyW32 {
         unsigned fl;
     };
     int nx, ny;
-    unsigned char* flags;
     int2* rng;
     int2* crng;
+    int2* rng2;          // next sweep's ranges (flag-free march)
     const Q4<float>* W;
     const float* C0;
     float* Ta;
@@ -612,13 +613,12 @@ struct AdjPolicyW32 {
         c.w = ld4(W + k);
         c.c0 = C0[k];
         c.vs = last ? Ta_start[k] : 0.f;
-        c.fl = flags[k];
+        c.fl = 0u;
         return c;
     }
     __device__ Cell load_nb(int k) const {
         Cell c{};
         c.v = Ta[k];
-        c.fl = flags[k];
         return c;
     }
     // neighbours in sweep order, mapped back as in AdjPolicyExact::update
@@ -644,7 +644,6 @@ struct AdjPolicyW32 {
         if (write_v) Ta[k] = v;
         if (write_start) Ta_start[k] = v;
     }
-    __device__ void store_flag(int k, unsigned f) const { flags[k] = (unsigned char)f; }
 };
 
 }  // namespace sa

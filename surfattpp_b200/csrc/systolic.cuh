@@ -113,21 +113,24 @@ __device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t,
     X up_x = __shfl_up_sync(FULL_MASK, L.prev_x, 1);
     V dn_v = __shfl_down_sync(FULL_MASK, nx1.v, 1);
     X dn_x = __shfl_down_sync(FULL_MASK, nx1.x, 1);
-    // left neighbour changed: own bit of the last ballot; upper: lane-1's bit
-    // (the strip's first lane reads bit 1 of the row above, current only
-    // where that row changed in this sweep)
-    unsigned up_chg = lane > 0 ? (L.bal >> (lane - 1)) & 1u : 0u;
     if (L.eup) {
         up_v = ecur.v;
         up_x = ecur.x;
-        up_chg = (c >= L.uf && c <= L.ul) ? (ecur.fl >> 1) & 1u : 0u;
     }
     if (L.edn) {
         dn_v = ecur.v;
         dn_x = ecur.x;
     }
-    const bool dirty = valid && (((cur.fl | (L.bal >> lane) | up_chg) & 1u) != 0u);
-    const bool work = __any_sync(FULL_MASK, dirty);
+    bool work = true;
+    if constexpr (P::kFlags) {
+        // left neighbour changed: own bit of the last ballot; upper: lane-1's
+        // bit (the strip's first lane reads bit 1 of the row above, current
+        // only where that row changed in this sweep)
+        unsigned up_chg = lane > 0 ? (L.bal >> (lane - 1)) & 1u : 0u;
+        if (L.eup) up_chg = (c >= L.uf && c <= L.ul) ? (ecur.fl >> 1) & 1u : 0u;
+        const bool dirty = valid && (((cur.fl | (L.bal >> lane) | up_chg) & 1u) != 0u);
+        work = __any_sync(FULL_MASK, dirty);
+    }
     bool chg = false;
     int ix = 0;
     if (valid) {
@@ -154,27 +157,29 @@ __device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t,
     const unsigned nbal = __ballot_sync(FULL_MASK, chg);
     // flags of the previous cell (r', c-1): changed at its visit; a later
     // neighbour (right = this cell, lower = lane+1's cell of this step) changed
-    if (L.act && c >= 1 && c <= NC) {
-        const int ixp = p.col(c - 1, xd);
-        const unsigned lower = (lane + 1 < L.nr_strip) ? (nbal >> (lane + 1)) & 1u : 0u;
-        const unsigned f = (((L.bal >> lane) & 1u) << 1) | ((nbal >> lane) & 1u) | lower;
-        if (f != L.pfl) p.store_flag(L.ioff + ixp, f);
-        if (f & 1u) {
-            L.rmin = min(L.rmin, ixp);
-            L.rmax = max(L.rmax, ixp);
+    if constexpr (P::kFlags) {
+        if (L.act && c >= 1 && c <= NC) {
+            const int ixp = p.col(c - 1, xd);
+            const unsigned lower = (lane + 1 < L.nr_strip) ? (nbal >> (lane + 1)) & 1u : 0u;
+            const unsigned f = (((L.bal >> lane) & 1u) << 1) | ((nbal >> lane) & 1u) | lower;
+            if (f != L.pfl) p.store_flag(L.ioff + ixp, f);
+            if (f & 1u) {
+                L.rmin = min(L.rmin, ixp);
+                L.rmax = max(L.rmax, ixp);
+            }
         }
-    }
-    if (L.eup && chg) {
-        p.store_flag(L.eoff + ix, ecur.fl | 1u);
-        L.umin = min(L.umin, ix);
-        L.umax = max(L.umax, ix);
+        if (L.eup && chg) {
+            p.store_flag(L.eoff + ix, ecur.fl | 1u);
+            L.umin = min(L.umin, ix);
+            L.umax = max(L.umax, ix);
+        }
+        if (valid) L.pfl = cur.fl;
     }
     if ((nbal >> (L.nr_strip - 1)) & 1u) {
         const int cl = t - (L.nr_strip - 1);
         L.lf = min(L.lf, cl);
         L.ll = max(L.ll, cl);
     }
-    if (valid) L.pfl = cur.fl;
     L.bal = nbal;
 }
 
@@ -193,6 +198,15 @@ __device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t,
 // start-of-iteration copy; every other cell adds an exact zero.  All of
 // this is exact: the cells not visited are exactly those the full march
 // would have left bit-identical and whose sums terms are zero.
+//
+// Without flags (P::kFlags false: short updates, where the per-cell
+// bookkeeping costs more than the updates it saves) every cell of the march
+// is updated, and the ranges come from changes instead: a cell can only
+// change in the next sweep if one of its four neighbours changed in this one
+// (every cell that could change in this sweep was visited in it), so the
+// next sweep's range of row r is the union of this sweep's changed ranges of
+// rows r-1, r, r+1 widened by one column (p.rng2, swapped in at the end of
+// the sweep).
 //
 // P::kLead = how many steps ahead a lane loads its row (1 for the long
 // forward update, more for the short adjoint update).
@@ -318,12 +332,47 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
                 if (t + NB - 1 - 31 > lastd && L.bal == 0u) break;
             }
         }
+        if constexpr (!P::kFlags) {
+            // next sweep's ranges: this row's changes widened by a column, in
+            // this row and the rows above and below
+            const bool any = L.cmin <= L.cmax;
+            const int lo = any ? max(L.cmin - 1, p.col(0, 1)) : 0x7fffffff;
+            const int hi = any ? min(L.cmax + 1, p.col(NC - 1, 1)) : -1;
+            int nlo = lo, nhi = hi;
+            const int alo = __shfl_up_sync(FULL_MASK, lo, 1);
+            const int ahi = __shfl_up_sync(FULL_MASK, hi, 1);
+            const int blo = __shfl_down_sync(FULL_MASK, lo, 1);
+            const int bhi = __shfl_down_sync(FULL_MASK, hi, 1);
+            if (lane > 0) {
+                nlo = min(nlo, alo);
+                nhi = max(nhi, ahi);
+            }
+            if (lane < 31) {
+                nlo = min(nlo, blo);
+                nhi = max(nhi, bhi);
+            }
+            if (act && nlo <= nhi) {
+                int2 r = p.rng2[iy];
+                r.x = min(r.x, nlo);
+                r.y = max(r.y, nhi);
+                p.rng2[iy] = r;
+            }
+            __syncwarp();
+            // the rows outside the strip
+            if (any && (L.eup || L.edn)) {
+                const int iy_o = L.eup ? iy_up : p.row(rp + 1, yd);
+                int2 r = p.rng2[iy_o];
+                r.x = min(r.x, lo);
+                r.y = max(r.y, hi);
+                p.rng2[iy_o] = r;
+            }
+        }
         // every cell of the row that had bit 0 set was visited: the range is
         // replaced; lane 0 then adds where it set bit 0 in the row above.
         // Cells changed since the iteration began: added to, or (after the
         // last sweep, whose copy makes start == current) cleared.
         if (act) {
-            p.rng[iy] = make_int2(L.rmin, L.rmax);
+            if constexpr (P::kFlags) p.rng[iy] = make_int2(L.rmin, L.rmax);
             if (last) {
                 p.crng[iy] = make_int2(0x7fffffff, -1);
             } else if (L.cmin <= L.cmax) {
@@ -334,7 +383,7 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
             }
         }
         __syncwarp();
-        if (L.eup && L.umin <= L.umax) {
+        if (P::kFlags && L.eup && L.umin <= L.umax) {
             int2 r = p.rng[iy_up];
             r.x = min(r.x, L.umin);
             r.y = max(r.y, L.umax);
@@ -342,6 +391,13 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         }
         uf = L.lf;
         ul = L.ll;
+        __syncwarp();
+    }
+    if constexpr (!P::kFlags) {
+        int2* nxt = p.rng2;
+        p.rng2 = p.rng;
+        p.rng = nxt;
+        for (int iy = lane; iy < p.ny; iy += 32) p.rng2[iy] = make_int2(0x7fffffff, -1);
         __syncwarp();
     }
 }
