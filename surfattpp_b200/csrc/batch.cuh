@@ -142,6 +142,7 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     P.flags = flags;
     P.rng = rng;
     P.crng = rng + ny;
+    P.rng2 = rng + 2 * ny;
     P.fix_x0 = si.fix_x0;
     P.fix_x1 = si.fix_x1;
     // rows with |(yy - y0)/dy| <= 1 (src/eikonal_solver.cpp:118-129, :162):
@@ -166,11 +167,12 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
         const S v = (fixed ? S(1) : S(10)) - off;
         tau[k] = v;
         tst[k] = v;
-        flags[k] = 1;
+        if (Pol::kFlags) flags[k] = 1;
     }
     for (int iy = lane; iy < ny; iy += 32) {
         rng[iy] = make_int2(0, nx - 1);
         rng[ny + iy] = make_int2(0x7fffffff, -1);   // crng: nothing changed yet
+        rng[2 * ny + iy] = make_int2(0x7fffffff, -1);
     }
     __syncwarp();
     iters = 0;

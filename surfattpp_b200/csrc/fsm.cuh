@@ -155,7 +155,10 @@ struct FwdBase {
     using X = S;
     static constexpr int kLead = SA_FWD_LEAD;
     static constexpr bool kRolled = ROLLED;
-    static constexpr bool kFlags = true;   // per-cell skip flags (systolic.cuh)
+    // per-cell skip flags (systolic.cuh) where the update is expensive enough
+    // to pay for them: the FP64 update (IEEE division and sqrt); the FP32
+    // march updates every cell of its range (10 % faster on C3)
+    static constexpr bool kFlags = sizeof(S) == sizeof(double);
     struct Cell {
         S v;    // field before this update
         S x;    // T0 of the cell
@@ -167,6 +170,7 @@ struct FwdBase {
     unsigned char* flags;  // per event
     int2* rng;           // per row: x range of flag bit 0 (systolic.cuh)
     int2* crng;          // per row: x range changed in this iteration
+    int2* rng2;          // next sweep's ranges (flag-free march)
     const Q4<S>* pk;     // per event
     const Q4<S>* mt;     // per period (general metric) or null
     const S* a_row;      // iso: [ny]
@@ -204,7 +208,7 @@ struct FwdBase {
             c.m.c = m.z;
         }
         c.vs = last ? tau_start[k] : S(0);
-        c.fl = flags[k];
+        c.fl = kFlags ? flags[k] : 0u;
         return c;
     }
     __device__ S ca(const Cell& c) const {
@@ -220,7 +224,7 @@ struct FwdBase {
         Cell c{};
         c.v = tau[k];
         c.x = pk[k].x;
-        c.fl = flags[k];
+        c.fl = kFlags ? flags[k] : 0u;
         return c;
     }
     __device__ void store(int k, S v, bool write_v, bool write_start) const {
