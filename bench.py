@@ -125,13 +125,13 @@ class Clocks:
 
 # DRAM bytes moved per algorithmic byte by batch_kernel<float>, from
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the same
-# kernel on the 151x151 / 3000-event case (53.641 GB moved for 73.430 GB of
+# kernel on the 151x151 / 3000-event case (50.645 GB moved for 73.430 GB of
 # algorithmic bytes; profiles/batch_kernel_fp32_c3_151x151_full.md).  The
 # algorithmic bytes count every cell of every sweep the reference performs;
 # the kernel skips cells that provably stay unchanged, so it moves less.
 # Traffic scales with cell updates, so a full launch moves algorithmic x this
 # ratio.
-TRAFFIC_PER_ALGO_BYTE = {"fp32": 53.641351e9 / 73.429994e9}
+TRAFFIC_PER_ALGO_BYTE = {"fp32": 50.645161e9 / 73.429994e9}
 
 
 def peaks():
