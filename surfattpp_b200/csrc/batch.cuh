@@ -84,7 +84,7 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     L.Ta = take(n * sizeof(S));
     L.sadj = take(r * sizeof(double));
     L.syn = take(r * sizeof(double));
-    L.flags = take(n);   // sweep flags (systolic.cuh), forward then adjoint
+    L.flags = take(n);   // per-cell sweep flags of the FP64 forward (systolic.cuh)
     // per-row x ranges (systolic.cuh): [0, ny) cells that can change in the
     // current sweep, [ny, 2 ny) cells changed in the current iteration,
     // [2 ny, 3 ny) the adjoint's ranges for the next sweep
