@@ -220,3 +220,39 @@ def test_c3_full_size_properties(gpu):
     r = syn - ev["tt_obs"]
     chi = 0.5 * np.sum(ev["weight"] * r * r)
     assert abs(float(out["chi"][0]) - chi) <= 1e-9 * chi
+
+
+def test_c3_full_size_fp32_against_fp64(gpu):
+    """FP32 accuracy on the whole C3 batch (8000 solves at 301x301): the FP64
+    plan is the reference's arithmetic (<= 1e-12 of the oracle in the parity
+    tests above), so it serves as the reference at full size.  Bars: max
+    travel-time error 1e-4 s, adj_s 1e-4 relative L2, misfit 1e-4 relative."""
+    import torch
+    import bench
+    from surfattpp_b200 import preproc
+
+    class A:
+        n, nsta, nper, precision = 301, 400, 20, "fp32"
+
+    w, svel = bench.make_inputs(A, 0)
+    ev = w.events()
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                          ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                          ev["stla"], precision=prec)
+        out = plan.run(t(svel), t(ev["tt_obs"]), t(ev["weight"]))
+        torch.cuda.synchronize()
+        assert int(out["status"].max()) == 0
+        res[prec] = {k: v.cpu().numpy().copy() for k, v in out.items()}
+        plan.close()
+    n = ev["rec_idx"].size
+    err = np.abs(res["fp32"]["syn"][:n] - res["fp64"]["syn"][:n]).max()
+    assert err <= 1e-4, err
+    a32, a64 = res["fp32"]["adj_s"], res["fp64"]["adj_s"]
+    l2 = np.linalg.norm(a32 - a64) / np.linalg.norm(a64)
+    assert l2 <= 1e-4, l2
+    c32, c64 = res["fp32"]["chi"][0], res["fp64"]["chi"][0]
+    assert abs(c32 - c64) <= 1e-4 * abs(c64)
