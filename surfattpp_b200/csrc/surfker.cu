@@ -1,1238 +1,10 @@
-// Dispersion and depth-kernel engine: surfdisp96 (Rayleigh/Love phase or
-// group velocity root search) per surface column and sregn96_hti (Rayleigh
-// eigenfunctions and depth kernels) per (column, period), plus the kernel
-// combination of preproc::combine_kernels.
-//
-// Compiled with -fmad=false and IEEE division/sqrt: the FP64 and REAL*4
-// arithmetic of src/surfker/surfdisp96.f and src/surfker/sregn96.f90 is kept
-// operation for operation, including the REAL*4 islands (model arrays, gtsolh,
-// sngl() arguments, default-kind literals).  Transcendentals are CUDA's
-// (sin/cos/exp/log within 1-2 ulp of the C library); the layer flattening
-// factors that involve REAL*4 powers are precomputed per layer on the host.
-#include <cmath>
-
-#include "launch.h"
+// Dispersion and depth-kernel kernels: surfdisp96 per surface column,
+// sregn96_hti depth kernels per (column, period), the kernel combination of
+// preproc::combine_kernels, and the host-side layer constants.  Compiled with
+// -fmad=false (see surfker_dev.cuh).
+#include "surfker_dev.cuh"
 
 namespace sa {
-namespace sk {
-
-constexpr int MMAX = 64;     // layers (nz + 1) supported per column
-constexpr int KMAX = 64;     // periods per column
-
-// Per-layer constants of the earth-flattening transforms.  They depend on
-// the layer thicknesses only, which every column shares.
-struct LayerConst {
-    int mmax;
-    // surfdisp96 sphere() (surfdisp96.f:502-574)
-    float sd_d[MMAX];        // flattened thickness (d(mmax) = 0 afterwards)
-    double sd_tmp[MMAX];     // velocity factor (ar+ar)/(r0+r1)
-    float sd_rhofac[MMAX];   // btp**(-2.275) (Rayleigh), REAL*4 power
-    float sd_rhofac_love[MMAX];  // btp**(-5) (Love)
-    // sregn96 bldsph() (sregn96.f90:129-183)
-    double rg_zd[MMAX];      // flattened thickness (zd(mmax) = 0)
-    double rg_vtp[MMAX];
-    double rg_rtp[MMAX];     // tmp**(-2.275), FP64 power
-    double rg_dtp[MMAX];
-    float thk[MMAX];         // unflattened float thickness (build_disp_req)
-};
-
-// Routines reached from several call sites.  Kept inline: an out-of-line
-// build (__noinline__) ran the phase kernels ~10 % faster but returned wrong
-// group-velocity dU/dvp kernels (dU/dvs and dU/drho correct, cause not
-// found), so it is not used.
-#ifndef SK_NOINLINE
-#define SK_NOINLINE inline
-#endif
-
-__device__ __forceinline__ double dsign1(double x) { return copysign(1.0, x); }
-
-// Brocher relations, scalar forms (include/utils.h:185-187, :223-225)
-__device__ __forceinline__ double vs2vp(double vs) {
-    return 0.9409 + 2.0947 * vs - 0.8206 * vs * vs + 0.2683 * vs * vs * vs - 0.0251 * vs * vs * vs * vs;
-}
-__device__ __forceinline__ double vp2rho(double vp) {
-    return 1.6612 * vp - 0.4721 * vp * vp + 0.0671 * vp * vp * vp - 0.0043 * vp * vp * vp * vp
-         + 0.000106 * vp * vp * vp * vp * vp;
-}
-// include/utils.h:198-212
-__device__ __forceinline__ double drho_dalpha(double vp) {
-    return 1.6612 - 2 * 0.4721 * vp + 3 * 0.0671 * vp * vp - 4 * 0.0043 * vp * vp * vp
-         + 5 * 0.000106 * vp * vp * vp * vp;
-}
-__device__ __forceinline__ double dalpha_dbeta(double vs) {
-    return 2.0947 - 2 * 0.8206 * vs + 3 * 0.2683 * vs * vs - 4 * 0.0251 * vs * vs * vs;
-}
-
-// Float layer model of one column: build_disp_req (src/surfdisp.cpp:60-108)
-// with the Brocher branch of SurfGrid::fwdsurf (src/surf_grid.cpp:214-226).
-__device__ inline void column_model(const double* vs1d, int nz, const LayerConst& L, float* vp,
-                                    float* vs, float* rho) {
-    for (int kk = 0; kk < nz; ++kk) {
-        const double b = vs1d[kk];
-        const double a = vs2vp(b);
-        const double r = vp2rho(a);
-        vs[kk] = (float)b;
-        vp[kk] = (float)a;
-        rho[kk] = (float)r;
-    }
-    vs[nz] = vs[nz - 1];
-    vp[nz] = vp[nz - 1];
-    rho[nz] = rho[nz - 1];
-}
-
-// ---------------------------------------------------------------------------
-// surfdisp96
-// ---------------------------------------------------------------------------
-struct SDModel {
-    int mmax, llw;
-    float d[MMAX], a[MMAX], b[MMAX], rho[MMAX];
-    double del1st;
-};
-
-struct VarOut {
-    double w, cosp, exa, a0, cpcq, cpy, cpz, cqw, cqx, xy, xz, wy, wz;
-};
-
-// surfdisp96.f:904-1021
-__device__ inline VarOut var(double p, double q, double ra, double rb, double wvno, double xka,
-                             double xkb, double dpth) {
-    VarOut o;
-    double pex = 0.0, sex = 0.0;
-    double sinp = 0.0, w = 0.0, x = 0.0, cosp = 0.0;
-    double sinq = 0.0, y = 0.0, z = 0.0, cosq = 0.0;
-    if (wvno < xka) {
-        sinp = sin(p);
-        w = sinp / ra;
-        x = -(ra * sinp);
-        cosp = cos(p);
-    } else if (wvno == xka) {
-        cosp = 1.0;
-        w = dpth;
-        x = 0.0;
-    } else if (wvno > xka) {
-        pex = p;
-        double fac = 0.0;
-        if (p < 16) fac = exp(-2.0 * p);
-        cosp = (1.0 + fac) * 0.5;
-        sinp = (1.0 - fac) * 0.5;
-        w = sinp / ra;
-        x = ra * sinp;
-    }
-    if (wvno < xkb) {
-        sinq = sin(q);
-        y = sinq / rb;
-        z = -(rb * sinq);
-        cosq = cos(q);
-    } else if (wvno == xkb) {
-        cosq = 1.0;
-        y = dpth;
-        z = 0.0;
-    } else if (wvno > xkb) {
-        sex = q;
-        double fac = 0.0;
-        if (q < 16) fac = exp(-2.0 * q);
-        cosq = (1.0 + fac) * 0.5;
-        sinq = (1.0 - fac) * 0.5;
-        y = sinq / rb;
-        z = rb * sinq;
-    }
-    o.exa = pex + sex;
-    o.a0 = 0.0;
-    if (o.exa < 60.0) o.a0 = exp(-o.exa);
-    o.cpcq = cosp * cosq;
-    o.cpy = cosp * y;
-    o.cpz = cosp * z;
-    o.cqw = cosq * w;
-    o.cqx = cosq * x;
-    o.xy = x * y;
-    o.xz = x * z;
-    o.wy = w * y;
-    o.wz = w * z;
-    o.w = w;
-    o.cosp = cosp;
-    return o;
-}
-
-// surfdisp96.f:1054-1098 fused with the row-vector product of dltar4
-// (ee(i) = sum_j e(j)*ca(j,i), :868-874).
-__device__ inline void dnka_apply(const double* e, double* ee, double wvno2, double gam,
-                                  double gammk, double rho, const VarOut& v) {
-    const double one = 1.0, two = 2.0;
-    const double gamm1 = gam - one;
-    const double twgm1 = gam + gamm1;
-    const double gmgmk = gam * gammk;
-    const double gmgm1 = gam * gamm1;
-    const double gm1sq = gamm1 * gamm1;
-    const double rho2 = rho * rho;
-    const double a0pq = v.a0 - v.cpcq;
-    double ca[5][5];
-    ca[0][0] = v.cpcq - two * gmgm1 * a0pq - gmgmk * v.xz - wvno2 * gm1sq * v.wy;
-    ca[0][1] = (wvno2 * v.cpy - v.cqx) / rho;
-    ca[0][2] = -((twgm1 * a0pq + gammk * v.xz + wvno2 * gamm1 * v.wy) / rho);
-    ca[0][3] = (v.cpz - wvno2 * v.cqw) / rho;
-    ca[0][4] = -((two * wvno2 * a0pq + v.xz + wvno2 * wvno2 * v.wy) / rho2);
-    ca[1][0] = (gmgmk * v.cpz - gm1sq * v.cqw) * rho;
-    ca[1][1] = v.cpcq;
-    ca[1][2] = gammk * v.cpz - gamm1 * v.cqw;
-    ca[1][3] = -v.wz;
-    ca[1][4] = ca[0][3];
-    ca[3][0] = (gm1sq * v.cpy - gmgmk * v.cqx) * rho;
-    ca[3][1] = -v.xy;
-    ca[3][2] = gamm1 * v.cpy - gammk * v.cqx;
-    ca[3][3] = ca[1][1];
-    ca[3][4] = ca[0][1];
-    ca[4][0] = -((two * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * v.xz + gm1sq * gm1sq * v.wy) * rho2);
-    ca[4][1] = ca[3][0];
-    ca[4][2] = -((gammk * gamm1 * twgm1 * a0pq + gam * gammk * gammk * v.xz + gamm1 * gm1sq * v.wy) * rho);
-    ca[4][3] = ca[1][0];
-    ca[4][4] = ca[0][0];
-    const double t = -two * wvno2;
-    ca[2][0] = t * ca[4][2];
-    ca[2][1] = t * ca[3][2];
-    ca[2][2] = v.a0 + two * (v.cpcq - ca[0][0]);
-    ca[2][3] = t * ca[1][2];
-    ca[2][4] = t * ca[0][2];
-#pragma unroll
-    for (int i = 0; i < 5; i++) {
-        double cr = 0.0;
-#pragma unroll
-        for (int j = 0; j < 5; j++) cr = cr + e[j] * ca[j][i];
-        ee[i] = cr;
-    }
-}
-
-// surfdisp96.f:1025-1050
-__device__ __forceinline__ void normc(double* ee, int n) {
-    double t1 = 0.0;
-    for (int i = 0; i < n; i++)
-        if (fabs(ee[i]) > t1) t1 = fabs(ee[i]);
-    if (t1 < 1.e-40) t1 = 1.0;
-    for (int i = 0; i < n; i++) {
-        double t2 = ee[i];
-        t2 = t2 / t1;
-        ee[i] = t2;
-    }
-}
-
-// surfdisp96.f:801-901
-__device__ SK_NOINLINE double dltar4(const SDModel& M, double wvno, double omga) {
-    const int mmax = M.mmax;
-    double omega = omga;
-    if (omega < 1.0e-4) omega = 1.0e-4;
-    const double wvno2 = wvno * wvno;
-    double xka = omega / (double)M.a[mmax - 1];
-    double xkb = omega / (double)M.b[mmax - 1];
-    double wvnop = wvno + xka;
-    double wvnom = fabs(wvno - xka);
-    double ra = sqrt(wvnop * wvnom);
-    wvnop = wvno + xkb;
-    wvnom = fabs(wvno - xkb);
-    double rb = sqrt(wvnop * wvnom);
-    double t = (double)M.b[mmax - 1] / omega;
-    double gammk = 2.0 * t * t;
-    double gam = gammk * wvno2;
-    const double gamm1 = gam - 1.0;
-    double rho1 = (double)M.rho[mmax - 1];
-    double e[5], ee[5];
-    e[0] = rho1 * rho1 * (gamm1 * gamm1 - gam * gammk * ra * rb);
-    e[1] = -(rho1 * ra);
-    e[2] = rho1 * (gamm1 - gammk * ra * rb);
-    e[3] = rho1 * rb;
-    e[4] = wvno2 - ra * rb;
-    for (int m = mmax - 2; m >= M.llw - 1; m--) {
-        xka = omega / (double)M.a[m];
-        xkb = omega / (double)M.b[m];
-        t = (double)M.b[m] / omega;
-        gammk = 2.0 * t * t;
-        gam = gammk * wvno2;
-        wvnop = wvno + xka;
-        wvnom = fabs(wvno - xka);
-        ra = sqrt(wvnop * wvnom);
-        wvnop = wvno + xkb;
-        wvnom = fabs(wvno - xkb);
-        rb = sqrt(wvnop * wvnom);
-        const double dpth = (double)M.d[m];
-        rho1 = (double)M.rho[m];
-        const double p = ra * dpth;
-        const double q = rb * dpth;
-        const VarOut v = var(p, q, ra, rb, wvno, xka, xkb, dpth);
-        dnka_apply(e, ee, wvno2, gam, gammk, rho1, v);
-        normc(ee, 5);
-        for (int i = 0; i < 5; i++) e[i] = ee[i];
-    }
-    if (M.llw != 1) {
-        xka = omega / (double)M.a[0];
-        wvnop = wvno + xka;
-        wvnom = fabs(wvno - xka);
-        ra = sqrt(wvnop * wvnom);
-        const double dpth = (double)M.d[0];
-        rho1 = (double)M.rho[0];
-        const double p = ra * dpth;
-        const double znul = 1.0e-05;
-        const VarOut v = var(p, znul, ra, znul, wvno, xka, znul, dpth);
-        const double w0 = -(rho1 * v.w);
-        return v.cosp * e[0] + w0 * e[1];
-    }
-    return e[0];
-}
-
-// surfdisp96.f:737-797
-__device__ SK_NOINLINE double dltar1(const SDModel& M, double wvno, double omega) {
-    const int mmax = M.mmax;
-    double beta1 = (double)M.b[mmax - 1];
-    double rho1 = (double)M.rho[mmax - 1];
-    double xkb = omega / beta1;
-    double wvnop = wvno + xkb;
-    double wvnom = fabs(wvno - xkb);
-    double rb = sqrt(wvnop * wvnom);
-    double e1 = rho1 * rb;
-    double e2 = 1.0 / (beta1 * beta1);
-    for (int m = mmax - 2; m >= M.llw - 1; m--) {
-        beta1 = (double)M.b[m];
-        rho1 = (double)M.rho[m];
-        const double xmu = rho1 * beta1 * beta1;
-        xkb = omega / beta1;
-        wvnop = wvno + xkb;
-        wvnom = fabs(wvno - xkb);
-        rb = sqrt(wvnop * wvnom);
-        const double q = (double)M.d[m] * rb;
-        double sinq, y, z, cosq;
-        if (wvno < xkb) {
-            sinq = sin(q);
-            y = sinq / rb;
-            z = -(rb * sinq);
-            cosq = cos(q);
-        } else if (wvno == xkb) {
-            cosq = 1.0;
-            y = (double)M.d[m];
-            z = 0.0;
-        } else {
-            double fac = 0.0;
-            if (q < 16) fac = exp(-2.0 * q);
-            cosq = (1.0 + fac) * 0.5;
-            sinq = (1.0 - fac) * 0.5;
-            y = sinq / rb;
-            z = rb * sinq;
-        }
-        const double e10 = e1 * cosq + e2 * xmu * z;
-        const double e20 = e1 * y / xmu + e2 * cosq;
-        double xnor = fabs(e10);
-        const double ynor = fabs(e20);
-        if (ynor > xnor) xnor = ynor;
-        if (xnor < 1.e-40) xnor = 1.0;
-        e1 = e10 / xnor;
-        e2 = e20 / xnor;
-    }
-    return e1;
-}
-
-__device__ __forceinline__ double dltar(const SDModel& M, double wvno, double omega, int kk) {
-    return kk == 1 ? dltar1(M, wvno, omega) : dltar4(M, wvno, omega);
-}
-
-// surfdisp96.f:578-711 (nevill with half inlined)
-__device__ SK_NOINLINE double nevill(const SDModel& M, double t, double c1, double c2, double del1,
-                                double del2, int ifunc, double twopi) {
-    double x[20], y[20];
-    const double omega = twopi / t;
-    double c3 = 0.5 * (c1 + c2);
-    double del3 = dltar(M, omega / c3, omega, ifunc);
-    int nev = 1;
-    int nctrl = 1;
-    int m = 1;
-    const double p01 = (double)0.01f;
-    for (;;) {
-        nctrl = nctrl + 1;
-        if (nctrl >= 100) break;
-        if (c3 < fmin(c1, c2) || c3 > fmax(c1, c2)) {
-            nev = 0;
-            c3 = 0.5 * (c1 + c2);
-            del3 = dltar(M, omega / c3, omega, ifunc);
-        }
-        const double s13 = del1 - del3;
-        const double s32 = del3 - del2;
-        if (dsign1(del3) * dsign1(del1) < 0.0) {
-            c2 = c3;
-            del2 = del3;
-        } else {
-            c1 = c3;
-            del1 = del3;
-        }
-        if (fabs(c1 - c2) <= 1.e-6 * c1) break;
-        if (dsign1(s13) != dsign1(s32)) nev = 0;
-        const double ss1 = fabs(del1);
-        const double s1 = p01 * ss1;
-        const double ss2 = fabs(del2);
-        const double s2 = p01 * ss2;
-        if (s1 > ss2 || s2 > ss1 || nev == 0) {
-            c3 = 0.5 * (c1 + c2);
-            del3 = dltar(M, omega / c3, omega, ifunc);
-            nev = 1;
-            m = 1;
-        } else {
-            if (nev == 2) {
-                x[m] = c3;
-                y[m] = del3;
-            } else {
-                x[0] = c1;
-                y[0] = del1;
-                x[1] = c2;
-                y[1] = del2;
-                m = 1;
-            }
-            bool bad = false;
-            for (int kk = 1; kk <= m; kk++) {
-                const int j = m - kk + 1;
-                const double denom = y[m] - y[j - 1];
-                if (fabs(denom) < 1.0e-10 * fabs(y[m])) {
-                    bad = true;
-                    break;
-                }
-                x[j - 1] = (-(y[j - 1] * x[j]) + y[m] * x[j - 1]) / denom;
-            }
-            if (!bad) {
-                c3 = x[0];
-                del3 = dltar(M, omega / c3, omega, ifunc);
-                nev = 2;
-                m = m + 1;
-                if (m > 10) m = 10;
-            } else {
-                c3 = 0.5 * (c1 + c2);
-                del3 = dltar(M, omega / c3, omega, ifunc);
-                nev = 1;
-                m = 1;
-            }
-        }
-    }
-    return c3;
-}
-
-// surfdisp96.f:403-498
-__device__ SK_NOINLINE int getsol(SDModel& M, double t1, double& c1, double clow, double dc, double cm,
-                             float betmx, int ifunc, int ifirst) {
-    const double twopi = 2.0 * 3.141592653589793;
-    double omega = twopi / t1;
-    double wvno = omega / c1;
-    double del1 = dltar(M, wvno, omega, ifunc);
-    if (ifirst == 1) M.del1st = del1;
-    const double plmn = dsign1(M.del1st) * dsign1(del1);
-    int idir;
-    if (ifirst == 1) idir = +1;
-    else if (plmn >= 0.0) idir = +1;
-    else idir = -1;
-    for (int guard = 0; guard < 100000; guard++) {
-        double c2;
-        if (idir > 0) c2 = c1 + dc;
-        else c2 = c1 - dc;
-        if (c2 <= clow) {
-            idir = +1;
-            c1 = clow;
-            continue;
-        }
-        omega = twopi / t1;
-        wvno = omega / c2;
-        const double del2 = dltar(M, wvno, omega, ifunc);
-        if (dsign1(del1) != dsign1(del2)) {
-            c1 = nevill(M, t1, c1, c2, del1, del2, ifunc, twopi);
-            if (c1 > (double)betmx) return -1;
-            return 1;
-        }
-        c1 = c2;
-        del1 = del2;
-        if (c1 < cm) return -1;
-        if (c1 >= ((double)betmx + dc)) return -1;
-    }
-    return -1;
-}
-
-// surfdisp96.f:380-401 (REAL*4)
-__device__ inline float gtsolh(float a, float b) {
-    float c = 0.95f * b;
-    for (int i = 0; i < 5; i++) {
-        const float gamma = b / a;
-        const float kappa = c / b;
-        const float k2 = kappa * kappa;
-        const float gk2 = (gamma * kappa) * (gamma * kappa);
-        const float fac1 = sqrtf(1.0f - gk2);
-        const float fac2 = sqrtf(1.0f - k2);
-        const float t = 2.0f - k2;
-        const float fr = t * t - 4.0f * fac1 * fac2;
-        float frp = -(4.0f * (2.0f - k2) * kappa) + 4.0f * fac2 * gamma * gamma * kappa / fac1
-                  + 4.0f * fac1 * kappa / fac2;
-        frp = frp / b;
-        c = c - fr / frp;
-    }
-    return c;
-}
-
-// surfdisp96.f:57-373 for one column.  vp/vs/rho: unflattened float model
-// (mmax layers).  Returns 0, or 1 when the fundamental-mode search fails.
-__device__ int surfdisp96(const LayerConst& L, const float* vpm, const float* vsm,
-                          const float* rhom, int iflsph, int iwave, int mode, int igr, int kmax,
-                          const double* t, double* cg) {
-    SDModel M;
-    const int mmax = L.mmax;
-    M.mmax = mmax;
-    float vmin = vsm[0];
-    for (int i = 1; i < mmax; i++) vmin = fminf(vmin, vsm[i]);
-    float ddc0;
-    if (vmin < 1.0f) ddc0 = 0.001f;
-    else if (vmin < 2.0f) ddc0 = 0.002f;
-    else ddc0 = 0.005f;
-    const float h0 = 0.005f;
-    M.llw = 1;
-    if (vsm[0] <= 0.0f) M.llw = 2;
-    for (int i = 0; i < mmax; i++) {
-        if (iflsph == 1) {   // sphere(0,0): velocities and thickness flattened
-            M.d[i] = L.sd_d[i];
-            M.a[i] = (float)(vpm[i] * L.sd_tmp[i]);
-            M.b[i] = (float)(vsm[i] * L.sd_tmp[i]);
-        } else {
-            M.d[i] = L.thk[i];
-            M.a[i] = vpm[i];
-            M.b[i] = vsm[i];
-        }
-        M.rho[i] = rhom[i];
-    }
-    M.del1st = 0.0;
-    const double one = 1.0e-2;
-    int jmn = 1, jsol = 1;
-    float betmx = -1.e20f, betmn = 1.e20f;
-    for (int i = 0; i < mmax; i++) {
-        if (M.b[i] > 0.01f && M.b[i] < betmn) {
-            betmn = M.b[i];
-            jmn = i + 1;
-            jsol = 1;
-        } else if (M.b[i] <= 0.01f && M.a[i] < betmn) {
-            betmn = M.a[i];
-            jmn = i + 1;
-            jsol = 0;
-        }
-        if (M.b[i] > betmx) betmx = M.b[i];
-    }
-    const int ifunc = (iwave == 1) ? 1 : 2;
-    if (iflsph == 1)   // sphere(ifunc,1): density mapping
-        for (int i = 0; i < mmax; i++)
-            M.rho[i] = rhom[i] * (ifunc == 1 ? L.sd_rhofac_love[i] : L.sd_rhofac[i]);
-    double c[KMAX], cb[KMAX];
-    const float ddc = ddc0;
-    const float sone = 1.500f;
-    const float h = h0;
-    const double onea = (double)sone;
-    float cc1;
-    if (jsol == 0) cc1 = betmn;
-    else cc1 = gtsolh(M.a[jmn - 1], M.b[jmn - 1]);
-    cc1 = 0.95f * cc1;
-    cc1 = 0.90f * cc1;
-    const double cc = (double)cc1;
-    const double dc = fabs((double)ddc);
-    double c1 = cc;
-    const double cm = cc;
-    double clow = cc;
-    for (int i = 0; i < kmax; i++) {
-        cb[i] = 0.0;
-        c[i] = 0.0;
-    }
-    int ift = 999;
-    for (int iq = 1; iq <= mode; iq++) {
-        int kfail = -1;
-        for (int k = 1; k <= kmax; k++) {
-            if (k >= ift) {
-                kfail = k;
-                break;
-            }
-            double t1 = t[k - 1];
-            float t1a, t1b = 0.0f;
-            if (igr > 0) {
-                t1a = (float)(t1 / (double)(1.0f + h));
-                t1b = (float)(t1 / (double)(1.0f - h));
-                t1 = (double)t1a;
-            } else {
-                t1a = (float)t1;
-            }
-            int ifirst;
-            if (k == 1 && iq == 1) {
-                c1 = cc;
-                clow = cc;
-                ifirst = 1;
-            } else if (k == 1 && iq > 1) {
-                c1 = c[0] + one * dc;
-                clow = c1;
-                ifirst = 1;
-            } else if (k > 1 && iq > 1) {
-                ifirst = 0;
-                clow = c[k - 1] + one * dc;
-                c1 = c[k - 2];
-                if (c1 < clow) c1 = clow;
-            } else {
-                ifirst = 0;
-                c1 = c[k - 2] - onea * dc;
-                clow = cm;
-            }
-            int iret = getsol(M, t1, c1, clow, dc, cm, betmx, ifunc, ifirst);
-            if (iret == -1) {
-                kfail = k;
-                break;
-            }
-            c[k - 1] = c1;
-            if (igr > 0) {
-                t1 = (double)t1b;
-                ifirst = 0;
-                clow = cb[k - 1] + one * dc;
-                c1 = c1 - onea * dc;
-                iret = getsol(M, t1, c1, clow, dc, cm, betmx, ifunc, ifirst);
-                if (iret == -1) c1 = c[k - 1];
-                cb[k - 1] = c1;
-            } else {
-                c1 = 0.0;
-            }
-            const float cc0 = (float)c[k - 1];
-            const float ccg = (float)c1;
-            if (igr == 0) {
-                cg[k - 1] = cc0;
-            } else {
-                const float gvel =
-                    (1.0f / t1a - 1.0f / t1b) / (1.0f / (t1a * cc0) - 1.0f / (t1b * ccg));
-                cg[k - 1] = gvel;
-            }
-        }
-        if (kfail < 0) continue;
-        for (int i = kfail; i <= kmax; i++) cg[i - 1] = 0.0;
-        if (iq <= 1) return 1;
-        ift = kfail;
-    }
-    return 0;
-}
-
-// ---------------------------------------------------------------------------
-// sregn96_hti (sregn96.f90:1745-1849), Rayleigh, no fluid layers required
-// (the fluid branches are kept for completeness).
-// ---------------------------------------------------------------------------
-struct cx {
-    double re, im;
-};
-__device__ __forceinline__ cx C(double r, double i = 0.0) { return {r, i}; }
-__device__ __forceinline__ cx operator+(cx a, cx b) { return {a.re + b.re, a.im + b.im}; }
-__device__ __forceinline__ cx operator-(cx a, cx b) { return {a.re - b.re, a.im - b.im}; }
-__device__ __forceinline__ cx operator-(cx a) { return {-a.re, -a.im}; }
-__device__ __forceinline__ cx operator*(cx a, cx b) {
-    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
-}
-__device__ __forceinline__ cx operator*(double s, cx a) { return {s * a.re, s * a.im}; }
-__device__ __forceinline__ cx operator*(cx a, double s) { return {a.re * s, a.im * s}; }
-__device__ __forceinline__ cx operator-(double s, cx a) { return {s - a.re, -a.im}; }
-__device__ __forceinline__ cx operator/(cx a, double s) { return {a.re / s, a.im / s}; }
-// gfortran's range-reduced complex division
-__device__ __forceinline__ cx operator/(cx a, cx b) {
-    const double ar = a.re, ai = a.im, br = b.re, bi = b.im;
-    if (fabs(br) < fabs(bi)) {
-        const double ratio = br / bi;
-        const double div = (br * ratio) + bi;
-        return {((ar * ratio) + ai) / div, ((ai * ratio) - ar) / div};
-    }
-    const double ratio = bi / br;
-    const double div = (bi * ratio) + br;
-    return {((ai * ratio) + ar) / div, (ai - (ar * ratio)) / div};
-}
-__device__ __forceinline__ cx operator/(double s, cx b) { return C(s) / b; }
-__device__ __forceinline__ double cabs_(cx a) { return hypot(a.re, a.im); }
-__device__ __forceinline__ cx csqrt_real(double x) {
-    if (x < 0.0) return {0.0, sqrt(-x)};
-    return {sqrt(x), 0.0};
-}
-__device__ __forceinline__ cx cexp_(cx a) {
-    const double e = exp(a.re);
-    return {e * cos(a.im), e * sin(a.im)};
-}
-__device__ __forceinline__ cx conj_(cx a) { return {a.re, -a.im}; }
-
-struct RW {
-    int mmax;
-    bool allfluid;
-    double zd[MMAX], zrho[MMAX], za[MMAX], zb[MMAX], xmu[MMAX], xlam[MMAX];
-    double ur[MMAX], uz[MMAX], tz[MMAX], tr[MMAX];
-    double dcda[MMAX], dcdb[MMAX], dcdr[MMAX], dcdh[MMAX], dcdgc[MMAX];
-    double exe[MMAX], exa[MMAX];
-    double cd[MMAX][5], vv[MMAX][4];
-    unsigned char iwat[MMAX];
-    cx ra, rb;
-    cx e[4][4], einv[4][4];
-};
-
-struct VarSv {
-    double cosp, cosq, rsinp, rsinq, sinpr, sinqr, pex, svex;
-};
-// sregn96.f90:827-911
-__device__ SK_NOINLINE VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
-    VarSv o;
-    const double lim = (double)1.0e-5f;
-    o.svex = 0.0;
-    const double pr = p.re, pi = p.im, qr = q.re, qi = q.im;
-    o.pex = pr;
-    const cx epp = C(cos(pi), sin(pi)) / 2.0;
-    const cx epm = conj_(epp);
-    const double pfac = (pr < 30.0) ? exp(-(2.0 * pr)) : 0.0;
-    o.cosp = (epp + pfac * epm).re;
-    const cx sinp = epp - pfac * epm;
-    o.rsinp = (rp * sinp).re;
-    if (fabs(pr) < lim && cabs_(rp) < lim) o.sinpr = zd;
-    else o.sinpr = (sinp / rp).re;
-    if (iwat == 1) {
-        o.cosq = 1.0;
-        o.rsinq = 0.0;
-        o.sinqr = 0.0;
-    } else {
-        o.svex = qr;
-        const cx eqp = C(cos(qi), sin(qi)) / 2.0;
-        const cx eqm = conj_(eqp);
-        const double svfac = (qr < 30.0) ? exp(-(2.0 * qr)) : 0.0;
-        o.cosq = (eqp + svfac * eqm).re;
-        const cx sinq = eqp - svfac * eqm;
-        o.rsinq = (rsv * sinq).re;
-        if (fabs(qr) < lim && cabs_(rsv) < lim) o.sinqr = zd;
-        else o.sinqr = (sinq / rsv).re;
-    }
-    return o;
-}
-
-// sregn96.f90:491-647 fused with the product ee(i) = sum_j cd(m+1,j)*ca(j,i)
-__device__ SK_NOINLINE void dnka_rg(double ca[5][5], double cosp, double rsinp, double sinpr,
-                               double cossv, double rsinsv, double sinsvr, float rho, float b,
-                               int iwat, double ex, double exa, double wvno, double wvno2,
-                               double om2) {
-    if (iwat == 1) {
-        for (int j = 0; j < 5; j++)
-            for (int i = 0; i < 5; i++) ca[i][j] = 0.0;
-        const double dfac = (ex > 35.0) ? 0.0 : exp(-ex);
-        ca[2][2] = dfac;
-        ca[0][0] = cosp;
-        ca[4][4] = cosp;
-        ca[0][1] = -(rsinp / (rho * om2));
-        ca[1][0] = -(rho * sinpr * om2);
-        ca[1][1] = cosp;
-        ca[3][3] = cosp;
-        ca[3][4] = ca[0][1];
-        ca[4][3] = ca[1][0];
-        return;
-    }
-    const double a0 = (exa < 60.0) ? exp(-exa) : 0.0;
-    const double cpcq = cosp * cossv;
-    const double cpy = cosp * sinsvr;
-    const double cpz = cosp * rsinsv;
-    const double cqw = cossv * sinpr;
-    const double cqx = cossv * rsinp;
-    const double xy = rsinp * sinsvr;
-    const double xz = rsinp * rsinsv;
-    const double wy = sinpr * sinsvr;
-    const double wz = sinpr * rsinsv;
-    const float rho2 = rho * rho;
-    const double gam = (double)(2.0f * b * b) * wvno2 / om2;
-    const double gam2 = gam * gam;
-    const double gamm1 = gam - 1.0;
-    const double gamm2 = gamm1 * gamm1;
-    const double cqww2 = cqw * wvno2;
-    const double cqxw2 = cqx / wvno2;
-    const double gg1 = gam * gamm1;
-    const double a0c = 2.0 * (a0 - cpcq);
-    const double xz2 = xz / wvno2;
-    const double gxz2 = gam * xz2;
-    const double g2xz2 = gam2 * xz2;
-    const double a0cgg1 = a0c * (gam + gamm1);
-    const double wy2 = wy * wvno2;
-    const double g2wy2 = gamm2 * wy2;
-    const double g1wy2 = gamm1 * wy2;
-    const double rom2 = (double)rho * om2;
-    double temp = a0c * gg1 + g2xz2 + g2wy2;
-    ca[2][2] = a0 + temp + temp;
-    ca[0][0] = cpcq - temp;
-    ca[0][1] = (-cqx + wvno2 * cpy) / rom2;
-    temp = 0.5 * a0cgg1 + gxz2 + g1wy2;
-    ca[0][2] = wvno * temp / rom2;
-    ca[0][3] = (-cqww2 + cpz) / rom2;
-    temp = wvno2 * (a0c + wy2) + xz;
-    ca[0][4] = -(temp / ((double)rho2 * om2 * om2));
-    ca[1][0] = (-(gamm2 * cqw) + gam2 * cpz / wvno2) * (double)rho * om2;
-    ca[1][1] = cpcq;
-    ca[1][2] = (gamm1 * cqww2 - gam * cpz) / wvno;
-    ca[1][3] = -wz;
-    ca[1][4] = ca[0][3];
-    temp = 0.5 * a0cgg1 * gg1 + gam2 * gxz2 + gamm2 * g1wy2;
-    ca[2][0] = -(2.0 * temp * (double)rho * om2 / wvno);
-    ca[2][1] = -(wvno * (gam * cqxw2 - gamm1 * cpy) * 2.0);
-    ca[2][3] = -2.0 * ca[1][2];
-    ca[2][4] = -2.0 * ca[0][2];
-    ca[3][0] = (-(gam2 * cqxw2) + gamm2 * cpy) * (double)rho * om2;
-    ca[3][1] = -xy;
-    ca[3][2] = -(ca[2][1] / 2.0);
-    ca[3][3] = ca[1][1];
-    ca[3][4] = ca[0][1];
-    temp = gamm2 * (a0c * gam2 + g2wy2) + gam2 * g2xz2;
-    ca[4][0] = -((double)rho2 * om2 * om2 * temp / wvno2);
-    ca[4][1] = ca[3][0];
-    ca[4][2] = -(ca[2][0] / 2.0);
-    ca[4][3] = ca[1][0];
-    ca[4][4] = ca[0][0];
-}
-
-// sregn96.f90:649-825 (jbdry = 0, inp = 1)
-__device__ SK_NOINLINE void evalg(RW& W, int m, cx* gbr, double wvno, double om, double om2,
-                             double wvno2) {
-    const double xka = om / W.za[m - 1];
-    const double xkb = (W.zb[m - 1] > 0.0) ? om / W.zb[m - 1] : 0.0;
-    W.ra = csqrt_real(wvno2 - xka * xka);
-    W.rb = csqrt_real(wvno2 - xkb * xkb);
-    const cx ra = W.ra, rb = W.rb;
-    double gam = W.zb[m - 1] * wvno / om;
-    gam = 2.0 * (gam * gam);
-    const double gamm1 = gam - 1.0;
-    const double zr = W.zrho[m - 1];
-    cx(&E)[4][4] = W.e;
-    cx(&EI)[4][4] = W.einv;
-    if (W.iwat[m - 1] == 0) {
-        E[0][0] = C(wvno);
-        E[0][1] = rb;
-        E[0][2] = C(wvno);
-        E[0][3] = -rb;
-        E[1][0] = ra;
-        E[1][1] = C(wvno);
-        E[1][2] = -ra;
-        E[1][3] = C(wvno);
-        E[2][0] = C(zr * om2 * gamm1);
-        E[2][1] = (zr * om2 * gam) * rb / wvno;
-        E[2][2] = C(zr * om2 * gamm1);
-        E[2][3] = -((zr * om2 * gam) * rb / wvno);
-        E[3][0] = (zr * om2 * gam) * ra / wvno;
-        E[3][1] = C(zr * om2 * gamm1);
-        E[3][2] = -((zr * om2 * gam) * ra / wvno);
-        E[3][3] = C(zr * om2 * gamm1);
-        EI[0][0] = C(0.5 * gam / wvno);
-        EI[0][1] = -((0.5 * gamm1) / ra);
-        EI[0][2] = C(-(0.5 / (zr * om2)));
-        EI[0][3] = (0.5 * wvno) / ((zr * om2) * ra);
-        EI[1][0] = -((0.5 * gamm1) / rb);
-        EI[1][1] = C(0.5 * gam / wvno);
-        EI[1][2] = (0.5 * wvno) / ((zr * om2) * rb);
-        EI[1][3] = C(-(0.5 / (zr * om2)));
-        EI[2][0] = C(0.5 * gam / wvno);
-        EI[2][1] = (0.5 * gamm1) / ra;
-        EI[2][2] = C(-(0.5 / (zr * om2)));
-        EI[2][3] = -((0.5 * wvno) / ((zr * om2) * ra));
-        EI[3][0] = (0.5 * gamm1) / rb;
-        EI[3][1] = C(0.5 * gam / wvno);
-        EI[3][2] = -((0.5 * wvno) / ((zr * om2) * rb));
-        EI[3][3] = C(-(0.5 / (zr * om2)));
-        if (gbr) {
-            gbr[0] = ((zr * zr) * om2 * om2) * (-((gam * gam) * ra * rb) + C(wvno2 * gamm1 * gamm1));
-            gbr[1] = -((zr * (wvno2 * ra)) * om2);
-            gbr[2] = -(((zr * (-((gam * ra) * rb) + C(wvno2 * gamm1))) * om2) * wvno);
-            gbr[3] = (zr * (wvno2 * rb)) * om2;
-            gbr[4] = wvno2 * (C(wvno2) - ra * rb);
-            const cx den = -((((zr * zr) * om2 * om2 * wvno2) * ra) * rb);
-            for (int k = 0; k < 5; k++) gbr[k] = (0.25 * gbr[k]) / den;
-        }
-    } else {
-        if (gbr) {
-            if (W.allfluid) {
-                gbr[0] = 0.5 / ra;
-                gbr[1] = C(0.5) / C(-(zr * om2));
-                gbr[2] = C(0.0);
-                gbr[3] = C(0.0);
-                gbr[4] = C(0.0);
-            } else {
-                gbr[0] = C(0.0);
-                gbr[1] = C(0.0);
-                gbr[2] = C(0.0);
-                gbr[3] = ((0.5 * zr) * om2) / ra;
-                gbr[4] = C(-0.5);
-            }
-        }
-        for (int i = 0; i < 4; i++)
-            for (int j = 0; j < 4; j++) {
-                E[i][j] = C(0.0);
-                EI[i][j] = C(0.0);
-            }
-        E[0][0] = ra;
-        E[0][1] = -ra;
-        E[1][0] = C(-(zr * om2));
-        E[1][1] = C(-(zr * om2));
-        EI[0][0] = 0.5 / ra;
-        EI[0][1] = C(-(0.5 / (zr * om2)));
-        EI[1][0] = -(0.5 / ra);
-        EI[1][1] = C(-(0.5 / (zr * om2)));
-    }
-}
-
-__device__ __forceinline__ double normc_ex(double* ee, int nmat) {
-    double t1 = 0.0;
-    for (int i = 0; i < nmat; i++)
-        if (fabs(ee[i]) > t1) t1 = fabs(ee[i]);
-    if (t1 < 1.e-40) t1 = 1.0;
-    for (int i = 0; i < nmat; i++) {
-        double t2 = ee[i];
-        t2 = t2 / t1;
-        ee[i] = t2;
-    }
-    return log(t1);
-}
-
-// sregn96.f90:401-489
-__device__ inline void up(RW& W, double omega, double wvno) {
-    const double wvno2 = wvno * wvno;
-    const double om2 = omega * omega;
-    cx gbr[5];
-    evalg(W, W.mmax, gbr, wvno, omega, om2, wvno2);
-    for (int j = 0; j < 5; j++) W.cd[W.mmax - 1][j] = gbr[j].re;
-    W.exe[W.mmax - 1] = 0.0;
-    double exsum = 0.0;
-    double ca[5][5], ee[5];
-    for (int m = W.mmax - 1; m >= 1; m--) {
-        const double xka = omega / W.za[m - 1];
-        const double xkb = (W.zb[m - 1] > 0.0) ? omega / W.zb[m - 1] : 0.0;
-        const cx rp = csqrt_real(wvno2 - xka * xka);
-        const cx rsv = csqrt_real(wvno2 - xkb * xkb);
-        const VarSv v = varsv(rp * W.zd[m - 1], rsv * W.zd[m - 1], rp, rsv, W.iwat[m - 1],
-                              W.zd[m - 1]);
-        dnka_rg(ca, v.cosp, v.rsinp, v.sinpr, v.cosq, v.rsinq, v.sinqr, (float)W.zrho[m - 1],
-                (float)W.zb[m - 1], W.iwat[m - 1], v.pex, v.pex + v.svex, wvno, wvno2, om2);
-        for (int i = 0; i < 5; i++) {
-            double cr = 0.0;
-            for (int j = 0; j < 5; j++) cr = cr + W.cd[m][j] * ca[j][i];
-            ee[i] = cr;
-        }
-        const double exn = normc_ex(ee, 5);
-        exsum = exsum + v.pex + v.svex + exn;
-        W.exe[m - 1] = exsum;
-        for (int i = 0; i < 5; i++) W.cd[m - 1][i] = ee[i];
-    }
-}
-
-// sregn96.f90:913-987
-__device__ inline void hska(double AA[4][4], double cosp, double rsinp, double sinpr,
-                            double tcossv, double trsinsv, double tsinsvr, float rho, float b,
-                            int iwat, double pex, double svex, double wvno, double wvno2,
-                            double om2) {
-    const double rom2 = (double)rho * om2;
-    if (iwat == 1) {
-        for (int i = 0; i < 4; i++)
-            for (int j = 0; j < 4; j++) AA[i][j] = 0.0;
-        const double dfac = (pex > 35.0) ? 0.0 : exp(-pex);
-        AA[0][0] = dfac;
-        AA[3][3] = dfac;
-        AA[1][1] = cosp;
-        AA[2][2] = cosp;
-        AA[1][2] = -(rsinp / rom2);
-        AA[2][1] = -(rom2 * sinpr);
-        return;
-    }
-    const double dfac = ((pex - svex) > 70.0) ? 0.0 : exp(svex - pex);
-    const double cossv = dfac * tcossv;
-    const double rsinsv = dfac * trsinsv;
-    const double sinsvr = dfac * tsinsvr;
-    const double gam = (double)(2.0f * b * b) * wvno2 / om2;
-    const double gamm1 = gam - 1.0;
-    AA[0][0] = cossv + gam * (cosp - cossv);
-    AA[0][1] = -(wvno * gamm1 * sinpr) + gam * rsinsv / wvno;
-    AA[0][2] = -(wvno * (cosp - cossv) / rom2);
-    AA[0][3] = (wvno2 * sinpr - rsinsv) / rom2;
-    AA[1][0] = gam * rsinp / wvno - wvno * gamm1 * sinsvr;
-    AA[1][1] = cosp - gam * (cosp - cossv);
-    AA[1][2] = (-rsinp + wvno2 * sinsvr) / rom2;
-    AA[1][3] = -AA[0][2];
-    AA[2][0] = rom2 * gam * gamm1 * (cosp - cossv) / wvno;
-    AA[2][1] = rom2 * (-(gamm1 * gamm1 * sinpr) + gam * gam * rsinsv / wvno2);
-    AA[2][2] = AA[1][1];
-    AA[2][3] = -AA[0][1];
-    AA[3][0] = rom2 * (gam * gam * rsinp / wvno2 - gamm1 * gamm1 * sinsvr);
-    AA[3][1] = -AA[2][0];
-    AA[3][2] = -AA[1][0];
-    AA[3][3] = AA[0][0];
-}
-
-// sregn96.f90:989-1059
-__device__ inline void down(RW& W, double omega, double wvno) {
-    const double om2 = omega * omega;
-    const double wvno2 = wvno * wvno;
-    for (int i = 0; i < 4; i++) W.vv[0][i] = (i == 0) ? 1.0 : 0.0;
-    W.exa[0] = 0.0;
-    double exsum = 0.0;
-    double AA[4][4], aa0[4];
-    for (int m = 1; m <= W.mmax - 1; m++) {
-        const double xka = omega / W.za[m - 1];
-        const double xkb = (W.zb[m - 1] > 0.0) ? omega / W.zb[m - 1] : 0.0;
-        const cx rp = csqrt_real(wvno2 - xka * xka);
-        const cx rsv = csqrt_real(wvno2 - xkb * xkb);
-        const VarSv v = varsv(rp * W.zd[m - 1], rsv * W.zd[m - 1], rp, rsv, W.iwat[m - 1],
-                              W.zd[m - 1]);
-        hska(AA, v.cosp, v.rsinp, v.sinpr, v.cosq, v.rsinq, v.sinqr, (float)W.zrho[m - 1],
-             (float)W.zb[m - 1], W.iwat[m - 1], v.pex, v.svex, wvno, wvno2, om2);
-        for (int i = 0; i < 4; i++) {
-            double cc = 0.0;
-            for (int j = 0; j < 4; j++) cc = cc + AA[i][j] * W.vv[m - 1][j];
-            aa0[i] = cc;
-        }
-        const double ex2 = normc_ex(aa0, 4);
-        exsum = exsum + v.pex + ex2;
-        W.exa[m] = exsum;
-        for (int i = 0; i < 4; i++) W.vv[m][i] = aa0[i];
-    }
-}
-
-// sregn96.f90:193-399
-__device__ inline void svfunc(RW& W, double omega, double wvno) {
-    up(W, omega, wvno);
-    down(W, omega, wvno);
-    const double f1213 = -W.cd[0][1];
-    W.ur[0] = W.cd[0][2] / W.cd[0][1];
-    W.uz[0] = 1.0;
-    W.tz[0] = 0.0;
-    W.tr[0] = 0.0;
-    for (int i = 2; i <= W.mmax; i++) {
-        const double* cdi = W.cd[i - 1];
-        const double cd1 = cdi[0], cd2 = cdi[1], cd3 = cdi[2], cd4 = -cdi[2], cd5 = cdi[3],
-                     cd6 = cdi[4];
-        const double* vvi = W.vv[i - 1];
-        const double tz1 = -vvi[3], tz2 = -vvi[2], tz3 = vvi[1], tz4 = vvi[0];
-        const double uu1 = tz2 * cd6 - tz3 * cd5 + tz4 * cd4;
-        const double uu2 = -(tz1 * cd6) + tz3 * cd3 - tz4 * cd2;
-        const double uu3 = tz1 * cd5 - tz2 * cd3 + tz4 * cd1;
-        const double uu4 = -(tz1 * cd4) + tz2 * cd2 - tz3 * cd1;
-        const double ext = W.exa[i - 1] + W.exe[i - 1] - W.exe[0];
-        if (ext > -80.0 && ext < 80.0) {
-            const double fact = exp(ext);
-            W.ur[i - 1] = uu1 * fact / f1213;
-            W.uz[i - 1] = uu2 * fact / f1213;
-            W.tz[i - 1] = uu3 * fact / f1213;
-            W.tr[i - 1] = uu4 * fact / f1213;
-        } else {
-            W.ur[i - 1] = 0.0;
-            W.uz[i - 1] = 0.0;
-            W.tz[i - 1] = 0.0;
-            W.tr[i - 1] = 0.0;
-        }
-    }
-    if (!W.allfluid) {
-        int jwat = 0;
-        for (int i = 1; i <= W.mmax; i++) {
-            if (W.iwat[i - 1] > 0) jwat = i;
-            else break;
-        }
-        for (int i = 1; i <= jwat; i++) {
-            W.ur[i - 1] = 0.0;
-            W.tr[i - 1] = 0.0;
-        }
-    }
-}
-
-// sregn96.f90:1326-1404
-__device__ inline cx ffunc(cx nub, double dm) {
-    if (cabs_(nub) < 1.0e-08) return C(dm);
-    const cx argcd = nub * dm;
-    const cx exqq = (argcd.re < 40.0) ? cexp_(-(2.0 * argcd)) : C(0.0);
-    return (1.0 - exqq) / (2.0 * nub);
-}
-__device__ inline cx gfunc(cx nub, double dm) {
-    const cx argcd = nub * dm;
-    if (argcd.re < 75.0) return cexp_(-argcd) * dm;
-    return C(0.0, 0.0);
-}
-__device__ inline cx h1func(cx nua, cx nub, double dm) {
-    if (cabs_(nub + nua) < 1.0e-08) return C(dm);
-    const cx argcd = (nua + nub) * dm;
-    const cx exqq = (argcd.re < 40.0) ? cexp_(-argcd) : C(0.0);
-    return (1.0 - exqq) / (nub + nua);
-}
-__device__ inline cx h2func(cx nua, cx nub, double dm) {
-    if (cabs_(nub - nua) < 1.0e-08) return C(dm);
-    cx argcd = nua * dm;
-    const cx exqp = (argcd.re < 40.0) ? cexp_(-argcd) : C(0.0);
-    argcd = nub * dm;
-    const cx exqq = (argcd.re < 40.0) ? cexp_(-argcd) : C(0.0);
-    return (exqq - exqp) / (nua - nub);
-}
-
-// The six energy integrals of one layer (sregn96.f90:1205-1324 called with
-// (1,1),(1,3),(2,2),(2,4),(3,3),(4,4)); evalg is evaluated once per layer
-// (its outputs are the same for every (i, j)).
-__device__ SK_NOINLINE void layer_integrals(RW& W, int m, int typelyr, double om, double om2,
-                                       double wvno, double wvno2, double* I) {
-    evalg(W, m, nullptr, wvno, om, om2, wvno2);
-    const cx ra = W.ra, rb = W.rb;
-    const double zd = W.zd[m - 1];
-    auto e = [&](int a, int b) { return W.e[a - 1][b - 1]; };
-    auto ei = [&](int a, int b) { return W.einv[a - 1][b - 1]; };
-    const int II[6] = {1, 1, 2, 2, 3, 4};
-    const int JJ[6] = {1, 3, 2, 4, 3, 4};
-    if (W.iwat[m - 1] == 1) {
-        cx kmpu = C(0.0), km1pd = C(0.0), FA = C(0.0), GA = C(0.0);
-        if (typelyr < 0) {
-            kmpu = ei(1, 1) * W.uz[m] + ei(1, 2) * W.tz[m];
-        } else if (typelyr == 0) {
-            km1pd = ei(2, 1) * W.uz[m - 1] + ei(2, 2) * W.tz[m - 1];
-            kmpu = ei(1, 1) * W.uz[m] + ei(1, 2) * W.tz[m];
-            FA = ffunc(ra, zd);
-            GA = gfunc(ra, zd);
-        } else {
-            km1pd = ei(2, 1) * W.uz[m - 1] + ei(2, 2) * W.tz[m - 1];
-        }
-        for (int q = 0; q < 6; q++) {
-            const int i = II[q], j = JJ[q];
-            cx c;
-            if (typelyr < 0) c = e(i, 1) * e(j, 1) * kmpu * kmpu / (2.0 * ra);
-            else if (typelyr == 0)
-                c = e(i, 1) * e(j, 1) * kmpu * kmpu * FA
-                  + (e(i, 1) * e(j, 2) + e(i, 2) * e(j, 1)) * kmpu * km1pd * GA
-                  + e(i, 2) * e(j, 2) * km1pd * km1pd * FA;
-            else c = e(i, 2) * e(j, 2) * km1pd * km1pd / (2.0 * ra);
-            I[q] = c.re;
-        }
-        return;
-    }
-    const double urm = W.ur[m - 1], uzm = W.uz[m - 1], tzm = W.tz[m - 1], trm = W.tr[m - 1];
-    if (typelyr < 0) {
-        const cx kmpu = ei(1, 1) * urm + ei(1, 2) * uzm + ei(1, 3) * tzm + ei(1, 4) * trm;
-        const cx kmsu = ei(2, 1) * urm + ei(2, 2) * uzm + ei(2, 3) * tzm + ei(2, 4) * trm;
-        for (int q = 0; q < 6; q++) {
-            const int i = II[q], j = JJ[q];
-            const cx c = e(i, 1) * e(j, 1) * kmpu * kmpu / (2.0 * ra)
-                       + (e(i, 1) * e(j, 2) + e(i, 2) * e(j, 1)) * kmpu * kmsu / (ra + rb)
-                       + e(i, 2) * e(j, 2) * kmsu * kmsu / (2.0 * rb);
-            I[q] = c.re;
-        }
-    } else if (typelyr == 0) {
-        const double urp = W.ur[m], uzp = W.uz[m], tzp = W.tz[m], trp = W.tr[m];
-        const cx km1pd = ei(3, 1) * urm + ei(3, 2) * uzm + ei(3, 3) * tzm + ei(3, 4) * trm;
-        const cx km1sd = ei(4, 1) * urm + ei(4, 2) * uzm + ei(4, 3) * tzm + ei(4, 4) * trm;
-        const cx kmpu = ei(1, 1) * urp + ei(1, 2) * uzp + ei(1, 3) * tzp + ei(1, 4) * trp;
-        const cx kmsu = ei(2, 1) * urp + ei(2, 2) * uzp + ei(2, 3) * tzp + ei(2, 4) * trp;
-        const cx FA = ffunc(ra, zd);
-        const cx GA = gfunc(ra, zd);
-        const cx FB = ffunc(rb, zd);
-        const cx GB = gfunc(rb, zd);
-        const cx H1 = h1func(ra, rb, zd);
-        const cx H2 = h2func(ra, rb, zd);
-        for (int q = 0; q < 6; q++) {
-            const int i = II[q], j = JJ[q];
-            const cx c = e(i, 1) * e(j, 1) * kmpu * kmpu * FA
-                       + e(i, 3) * e(j, 3) * km1pd * km1pd * FA
-                       + e(i, 2) * e(j, 2) * kmsu * kmsu * FB
-                       + e(i, 4) * e(j, 4) * km1sd * km1sd * FB
-                       + H1 * ((e(i, 1) * e(j, 2) + e(i, 2) * e(j, 1)) * kmpu * kmsu
-                               + (e(i, 3) * e(j, 4) + e(i, 4) * e(j, 3)) * km1pd * km1sd)
-                       + H2 * ((e(i, 1) * e(j, 4) + e(i, 4) * e(j, 1)) * kmpu * km1sd
-                               + (e(i, 2) * e(j, 3) + e(i, 3) * e(j, 2)) * km1pd * kmsu)
-                       + GA * (e(i, 1) * e(j, 3) + e(i, 3) * e(j, 1)) * kmpu * km1pd
-                       + GB * (e(i, 2) * e(j, 4) + e(i, 4) * e(j, 2)) * kmsu * km1sd;
-            I[q] = c.re;
-        }
-    } else {
-        const cx km1pd = ei(3, 1) * urm + ei(3, 2) * uzm + ei(3, 3) * tzm + ei(3, 4) * trm;
-        const cx km1sd = ei(4, 1) * urm + ei(4, 2) * uzm + ei(4, 3) * tzm + ei(4, 4) * trm;
-        for (int q = 0; q < 6; q++) {
-            const int i = II[q], j = JJ[q];
-            const cx c = e(i, 3) * e(j, 3) * km1pd * km1pd / (2.0 * ra)
-                       + (e(i, 3) * e(j, 4) + e(i, 4) * e(j, 3)) * km1pd * km1sd / (ra + rb)
-                       + e(i, 4) * e(j, 4) * km1sd * km1sd / (2.0 * rb);
-            I[q] = c.re;
-        }
-    }
-}
-
-// sregn96.f90:1061-1203 (getmat :1538-1590) followed by the 1/(U I0) scaling.
-__device__ inline double energy(RW& W, double om, double wvno, double& ugr, double& fac) {
-    double sumi0 = 0.0, sumi1 = 0.0, sumi2 = 0.0, sumi3 = 0.0;
-    const double c = om / wvno;
-    const double om2 = om * om;
-    const double wvno2 = wvno * wvno;
-    for (int m = 1; m <= W.mmax; m++) {
-        double a12 = 0, a14 = 0, a21 = 0, a23 = 0, ah, av, bv, eta, rho, TA, TC, TF, TL, TN;
-        if (W.iwat[m - 1] == 1) {
-            ah = W.za[m - 1];
-            av = W.za[m - 1];
-            bv = 0.0;
-            rho = W.zrho[m - 1];
-            eta = 1.0;
-            TL = 0.0;
-            TN = 0.0;
-            TC = W.zrho[m - 1] * W.za[m - 1] * W.za[m - 1];
-            TA = W.zrho[m - 1] * W.za[m - 1] * W.za[m - 1];
-            TF = TA - 2.0 * TN;
-            a12 = -(wvno * wvno - om * om / (ah * ah)) / (rho * om * om);
-        } else {
-            ah = W.za[m - 1];
-            av = W.za[m - 1];
-            bv = W.zb[m - 1];
-            rho = W.zrho[m - 1];
-            eta = 1.0;
-            TL = W.zrho[m - 1] * W.zb[m - 1] * W.zb[m - 1];
-            TN = W.zrho[m - 1] * W.zb[m - 1] * W.zb[m - 1];
-            TC = W.zrho[m - 1] * W.za[m - 1] * W.za[m - 1];
-            TA = W.zrho[m - 1] * W.za[m - 1] * W.za[m - 1];
-            TF = TA - 2.0 * TN;
-            a12 = -wvno;
-            a14 = 1.0 / TL;
-            a21 = wvno * TF / TC;
-            a23 = 1.0 / TC;
-        }
-        const int typelyr = (m == W.mmax) ? 1 : 0;
-        double I[6];
-        layer_integrals(W, m, typelyr, om, om2, wvno, wvno2, I);
-        const double INT11 = I[0], INT13 = I[1], INT22 = I[2], INT24 = I[3], INT33 = I[4],
-                     INT44 = I[5];
-        if (W.iwat[m - 1] == 1) {
-            const double wr = wvno / (rho * om2);
-            const double URUR = INT22 * (wr * wr);
-            const double UZUZ = INT11;
-            const double URDUZ = -(wvno / (rho * om2)) * a12 * INT22;
-            const double DUZDUZ = a12 * a12 * INT22;
-            sumi0 = sumi0 + rho * (URUR + UZUZ);
-            sumi1 = sumi1 + TA * URUR;
-            sumi2 = sumi2 - TF * URDUZ;
-            sumi3 = sumi3 + TC * DUZDUZ;
-            const double facah = rho * ah * ah * (URUR - 2.0 * eta * URDUZ / wvno);
-            const double facav = rho * av * av * DUZDUZ / wvno2;
-            W.dcda[m - 1] = facah + facav;
-            W.dcdb[m - 1] = 0.0;
-            const double facr = -(0.5 * c * c * (URUR + UZUZ));
-            W.dcdr[m - 1] = 0.5 * (av * facav + ah * facah) + facr * rho;
-            W.dcdgc[m - 1] = 0.0;
-            W.ur[m - 1] = -(wvno * W.tz[m - 1]) / (rho * om2);
-        } else {
-            const double URUR = INT11;
-            const double UZUZ = INT22;
-            const double DURDUR = a12 * a12 * INT22 + 2.0 * a12 * a14 * INT24 + a14 * a14 * INT44;
-            const double DUZDUZ = a21 * a21 * INT11 + 2.0 * a21 * a23 * INT13 + a23 * a23 * INT33;
-            const double URDUZ = a21 * INT11 + a23 * INT13;
-            const double UZDUR = a12 * INT22 + a14 * INT24;
-            sumi0 = sumi0 + rho * (URUR + UZUZ);
-            sumi1 = sumi1 + TL * UZUZ + TA * URUR;
-            sumi2 = sumi2 + TL * UZDUR - TF * URDUZ;
-            sumi3 = sumi3 + TL * DURDUR + TC * DUZDUZ;
-            const double facah = rho * ah * ah * (URUR - 2.0 * eta * URDUZ / wvno);
-            const double facav = rho * av * av * DUZDUZ / wvno2;
-            const double facbh = 0.0;
-            const double facbv =
-                rho * bv * bv * (UZUZ + 2.0 * UZDUR / wvno + DURDUR / wvno2 + 4.0 * eta * URDUZ / wvno);
-            W.dcda[m - 1] = facah + facav;
-            W.dcdb[m - 1] = facbv + facbh;
-            const double facr = -(0.5 * c * c * (URUR + UZUZ));
-            W.dcdr[m - 1] = 0.5 * (av * facav + ah * facah + bv * facbv) + facr * rho;
-            W.dcdgc[m - 1] = rho * bv * bv * (UZUZ + 2.0 * UZDUR / wvno + DURDUR / wvno2)
-                           + rho * bv * bv * (URUR);
-        }
-    }
-    ugr = (wvno * sumi1 + sumi2) / (om * sumi0);
-    const double are = wvno / (2.0 * om * ugr * sumi0);
-    fac = are * c / wvno2;
-    for (int m = 0; m < W.mmax; m++) {
-        W.dcda[m] = W.dcda[m] / (ugr * sumi0);
-        W.dcdb[m] = W.dcdb[m] / (ugr * sumi0);
-        W.dcdr[m] = W.dcdr[m] / (ugr * sumi0);
-        W.dcdgc[m] = W.dcdgc[m] / (ugr * sumi0);
-    }
-    return sumi0;
-}
-
-}  // namespace sk
 
 // ---------------------------------------------------------------------------
 // Kernels
@@ -1335,100 +107,6 @@ depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int 
     }
 }
 
-// surfker::depthkernel_rayleigh_group (src/surfdisp.cpp:203-285) through
-// sregnpu (src/surfker/sregn96.f90:1851-1992): one thread per (column,
-// period); phase kernels at t, t1 = t(1 + 0.005) and t2 = t(1 - 0.005) from
-// the three phase-velocity planes, the finite-difference group kernels and
-// their earth-flattening conversion.  As in the reference, the first term of
-// du/dm reads the kernels left by the last (t2) evaluation.
-__global__ void __launch_bounds__(64, SK_DEPTH_MINB)
-depthkernel_group_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
-                         const double* __restrict__ periods, const double* __restrict__ p1,
-                         const double* __restrict__ p2, const double* __restrict__ cp_plane,
-                         const double* __restrict__ cp1_plane,
-                         const double* __restrict__ cp2_plane, const LayerConst* __restrict__ Lp,
-                         double* sen_vs, double* sen_vp, double* sen_rho) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= (long long)nx * ny * nper) return;
-    const int ip = (int)(gid % nper);
-    const int col = (int)(gid / nper);
-    const int ix = col / ny, iy = col % ny;
-    const LayerConst& L = *Lp;
-    float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];
-    sk::column_model(vs3d + (size_t)col * nz, nz, L, vp, vs, rho);
-    sk::RW W;
-    const int mmax = L.mmax;
-    W.mmax = mmax;
-    W.allfluid = true;
-    for (int i = 0; i < mmax; i++) {
-        W.zb[i] = vs[i];
-        W.za[i] = vp[i];
-        W.zrho[i] = rho[i];
-        W.zd[i] = L.thk[i];
-        W.iwat[i] = (W.zb[i] > 0.0) ? 0 : 1;
-        if (W.zb[i] > 0.0) W.allfluid = false;
-    }
-    for (int i = 0; i < mmax; i++) {   // bldsph
-        W.za[i] = W.za[i] * L.rg_vtp[i];
-        W.zb[i] = W.zb[i] * L.rg_vtp[i];
-        W.zrho[i] = W.zrho[i] * L.rg_rtp[i];
-        W.zd[i] = L.rg_zd[i];
-    }
-    for (int i = 0; i < mmax; i++) {
-        W.xmu[i] = W.zrho[i] * (W.zb[i] * W.zb[i]);
-        W.xlam[i] = W.zrho[i] * (W.za[i] * W.za[i]) - 2.0 * W.xmu[i];
-    }
-    const size_t pix = (size_t)ip * nx * ny + ix + (size_t)nx * iy;
-    const double pi = 3.1415926535897932384626433832795;
-    const double twopi = 2.0 * pi;
-    const double t = periods[ip], t1 = p1[ip], t2 = p2[ip];
-    const double cp = cp_plane[pix];
-    double ugr, fac;
-    // period t (:1908-1918)
-    double omega = twopi / t;
-    sk::svfunc(W, omega, omega / cp);
-    sk::energy(W, omega, omega / cp, ugr, fac);
-    const double cg = ugr;
-    double a0[sk::MMAX], b0[sk::MMAX], r0[sk::MMAX], a1[sk::MMAX], b1[sk::MMAX], r1[sk::MMAX];
-    for (int k = 0; k < nz; k++) {
-        a0[k] = W.dcda[k];
-        b0[k] = W.dcdb[k];
-        r0[k] = W.dcdr[k];
-    }
-    // period t1 (:1921-1930)
-    omega = twopi / t1;
-    const double c1 = cp1_plane[pix];
-    sk::svfunc(W, omega, omega / c1);
-    sk::energy(W, omega, omega / c1, ugr, fac);
-    for (int k = 0; k < nz; k++) {
-        a1[k] = W.dcda[k];
-        b1[k] = W.dcdb[k];
-        r1[k] = W.dcdr[k];
-    }
-    // period t2 (:1933-1942); W.dc* now hold this evaluation
-    omega = twopi / t2;
-    const double c2 = cp2_plane[pix];
-    sk::svfunc(W, omega, omega / c2);
-    sk::energy(W, omega, omega / c2, ugr, fac);
-    // :1945-1971
-    const double uc1 = cg / cp;
-    const double ar = 6371.0;
-    omega = twopi / t;
-    const double r = cp / (2.0 * ar * omega);
-    const double tm = sqrt(1.0 + r * r);
-    const double q = 0.5 / (ar * omega);
-    const double tm1 = (q * q) / tm;
-    for (int k = 0; k < nz; k++) {
-        const double dua = uc1 * (2.0 - uc1) * W.dcda[k] - uc1 * uc1 * t * (W.dcda[k] - a1[k]) / (t2 - t1);
-        const double dub = uc1 * (2.0 - uc1) * W.dcdb[k] - uc1 * uc1 * t * (W.dcdb[k] - b1[k]) / (t2 - t1);
-        const double dur = uc1 * (2.0 - uc1) * W.dcdr[k] - uc1 * uc1 * t * (W.dcdr[k] - r1[k]) / (t2 - t1);
-        const size_t i4 = ((size_t)col * nz + k) * nper + ip;
-        sen_vp[i4] = (tm * dua + cg * cp * a0[k] * tm1) * L.rg_vtp[k];
-        sen_vs[i4] = (tm * dub + cg * cp * b0[k] * tm1) * L.rg_vtp[k];
-        sen_rho[i4] = (tm * dur + cg * cp * r0[k] * tm1) * L.rg_rtp[k];
-    }
-}
-
 // preproc::combine_kernels, vs-only branch (src/preproc.cpp:276-304): one
 // thread per (ix, iy, k), periods accumulated in order from zero.
 __global__ void combine_vs_kernel(int nx, int ny, int nz, int nper, const double* __restrict__ adj_s,
@@ -1473,18 +151,6 @@ cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int n
     depthkernel_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
         nx, ny, nz, vs3d, nper, periods, cp, reinterpret_cast<const LayerConst*>(layer_const),
         sen_vs, sen_vp, sen_rho);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_depthkernel_group(int nx, int ny, int nz, const double* vs3d, int nper,
-                                     const double* periods, const double* p1, const double* p2,
-                                     const double* cp, const double* cp1, const double* cp2,
-                                     const void* layer_const, double* sen_vs, double* sen_vp,
-                                     double* sen_rho, cudaStream_t st) {
-    const long long n = (long long)nx * ny * nper;
-    depthkernel_group_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
-        nx, ny, nz, vs3d, nper, periods, p1, p2, cp, cp1, cp2,
-        reinterpret_cast<const LayerConst*>(layer_const), sen_vs, sen_vp, sen_rho);
     return cudaGetLastError();
 }
 
