@@ -2,6 +2,9 @@
 // sregn96_hti depth kernels per (column, period), the kernel combination of
 // preproc::combine_kernels, and the host-side layer constants.  Compiled with
 // -fmad=false (see surfker_dev.cuh).
+// the eigenfunction routines out of line here: the depth kernel then runs
+// 77 -> 72 ms (instruction fetch); the dispersion routines stay inline
+#define SK_NOINLINE_EIG __noinline__
 #include "surfker_dev.cuh"
 
 namespace sa {

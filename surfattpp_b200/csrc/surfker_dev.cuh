@@ -47,6 +47,11 @@ struct LayerConst {
 #ifndef SK_NOINLINE
 #define SK_NOINLINE inline
 #endif
+// The eigenfunction routines (varsv, dnka_rg, evalg, layer_integrals): out of
+// line in surfker.cu (SK_NOINLINE_EIG set there), inline elsewhere.
+#ifndef SK_NOINLINE_EIG
+#define SK_NOINLINE_EIG inline
+#endif
 
 // One out-of-line copy each of the FP64 transcendentals.  The column kernels
 // reach them from dozens of inlined call sites, and inline copies of the
@@ -686,7 +691,7 @@ struct VarSv {
     double cosp, cosq, rsinp, rsinq, sinpr, sinqr, pex, svex;
 };
 // sregn96.f90:827-911
-__device__ SK_NOINLINE VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
+static __device__ SK_NOINLINE_EIG VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
     VarSv o;
     const double lim = (double)1.0e-5f;
     o.svex = 0.0;
@@ -719,7 +724,7 @@ __device__ SK_NOINLINE VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double z
 }
 
 // sregn96.f90:491-647 fused with the product ee(i) = sum_j cd(m+1,j)*ca(j,i)
-__device__ SK_NOINLINE void dnka_rg(double ca[5][5], double cosp, double rsinp, double sinpr,
+static __device__ SK_NOINLINE_EIG void dnka_rg(double ca[5][5], double cosp, double rsinp, double sinpr,
                                double cossv, double rsinsv, double sinsvr, float rho, float b,
                                int iwat, double ex, double exa, double wvno, double wvno2,
                                double om2) {
@@ -798,7 +803,7 @@ __device__ SK_NOINLINE void dnka_rg(double ca[5][5], double cosp, double rsinp, 
 }
 
 // sregn96.f90:649-825 (jbdry = 0, inp = 1)
-__device__ SK_NOINLINE void evalg(RW& W, int m, cx* gbr, double wvno, double om, double om2,
+static __device__ SK_NOINLINE_EIG void evalg(RW& W, int m, cx* gbr, double wvno, double om, double om2,
                              double wvno2) {
     const double xka = om / W.za[m - 1];
     const double xkb = (W.zb[m - 1] > 0.0) ? om / W.zb[m - 1] : 0.0;
@@ -1076,7 +1081,7 @@ __device__ inline cx h2func(cx nua, cx nub, double dm) {
 // The six energy integrals of one layer (sregn96.f90:1205-1324 called with
 // (1,1),(1,3),(2,2),(2,4),(3,3),(4,4)); evalg is evaluated once per layer
 // (its outputs are the same for every (i, j)).
-__device__ SK_NOINLINE void layer_integrals(RW& W, int m, int typelyr, double om, double om2,
+static __device__ SK_NOINLINE_EIG void layer_integrals(RW& W, int m, int typelyr, double om, double om2,
                                        double wvno, double wvno2, double* I) {
     evalg(W, m, nullptr, wvno, om, om2, wvno2);
     const cx ra = W.ra, rb = W.rb;
