@@ -2,9 +2,12 @@
 // sregn96_hti depth kernels per (column, period), the kernel combination of
 // preproc::combine_kernels, and the host-side layer constants.  Compiled with
 // -fmad=false (see surfker_dev.cuh).
-// the eigenfunction routines out of line here: the depth kernel then runs
-// 77 -> 72 ms (instruction fetch); the dispersion routines stay inline
+// Out of line here, to shrink the instruction footprint: the eigenfunction
+// routines (the depth kernel 77 -> 72 ms on C3) and var (the dispersion
+// 141 -> 130 ms).  The other dispersion routines stay inline (out of line
+// they cost more in calls than they save).
 #define SK_NOINLINE_EIG __noinline__
+#define SK_VAR_ATTR __noinline__
 #include "surfker_dev.cuh"
 
 namespace sa {

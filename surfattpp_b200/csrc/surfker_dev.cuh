@@ -52,6 +52,11 @@ struct LayerConst {
 #ifndef SK_NOINLINE_EIG
 #define SK_NOINLINE_EIG inline
 #endif
+// var (the layer sines / exponentials of surfdisp96): out of line in
+// surfker.cu (SK_VAR_ATTR set there), inline elsewhere.
+#ifndef SK_VAR_ATTR
+#define SK_VAR_ATTR inline
+#endif
 
 // One out-of-line copy each of the FP64 transcendentals.  The column kernels
 // reach them from dozens of inlined call sites, and inline copies of the
@@ -122,7 +127,7 @@ struct VarOut {
 };
 
 // surfdisp96.f:904-1021
-__device__ inline VarOut var(double p, double q, double ra, double rb, double wvno, double xka,
+static __device__ SK_VAR_ATTR VarOut var(double p, double q, double ra, double rb, double wvno, double xka,
                              double xkb, double dpth) {
     VarOut o;
     double pex = 0.0, sex = 0.0;
