@@ -3,11 +3,12 @@
 // preproc::combine_kernels, and the host-side layer constants.  Compiled with
 // -fmad=false (see surfker_dev.cuh).
 // Out of line here, to shrink the instruction footprint: the eigenfunction
-// routines (the depth kernel 77 -> 72 ms on C3) and var (the dispersion
-// 141 -> 130 ms).  The other dispersion routines stay inline (out of line
-// they cost more in calls than they save).
+// routines (the depth kernel 77 -> 72 ms on C3), var and dltar4 (the
+// dispersion 141 -> 130 -> 107 ms).  nevill and getsol stay inline (out of
+// line they cost more in calls than they save: 137 / 179 ms).
 #define SK_NOINLINE_EIG __noinline__
 #define SK_VAR_ATTR __noinline__
+#define SK_ATTR_DLTAR4 __noinline__
 #include "surfker_dev.cuh"
 
 namespace sa {

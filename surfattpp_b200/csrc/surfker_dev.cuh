@@ -57,6 +57,10 @@ struct LayerConst {
 #ifndef SK_VAR_ATTR
 #define SK_VAR_ATTR inline
 #endif
+// dltar4: out of line in surfker.cu (SK_ATTR_DLTAR4 set there).
+#ifndef SK_ATTR_DLTAR4
+#define SK_ATTR_DLTAR4 inline
+#endif
 
 // One out-of-line copy each of the FP64 transcendentals.  The column kernels
 // reach them from dozens of inlined call sites, and inline copies of the
@@ -248,7 +252,7 @@ __device__ __forceinline__ void normc(double* ee, int n) {
 }
 
 // surfdisp96.f:801-901
-__device__ SK_NOINLINE double dltar4(const SDModel& M, double wvno, double omga) {
+static __device__ SK_ATTR_DLTAR4 double dltar4(const SDModel& M, double wvno, double omga) {
     const int mmax = M.mmax;
     double omega = omga;
     if (omega < 1.0e-4) omega = 1.0e-4;
