@@ -52,11 +52,6 @@ struct LayerConst {
 #ifndef SK_NOINLINE_EIG
 #define SK_NOINLINE_EIG inline
 #endif
-// var (the layer sines / exponentials of surfdisp96): out of line in
-// surfker.cu (SK_VAR_ATTR set there), inline elsewhere.
-#ifndef SK_VAR_ATTR
-#define SK_VAR_ATTR inline
-#endif
 // dltar4: out of line in surfker.cu (SK_ATTR_DLTAR4 set there).
 #ifndef SK_ATTR_DLTAR4
 #define SK_ATTR_DLTAR4 inline
@@ -131,7 +126,7 @@ struct VarOut {
 };
 
 // surfdisp96.f:904-1021
-static __device__ SK_VAR_ATTR VarOut var(double p, double q, double ra, double rb, double wvno, double xka,
+__device__ inline VarOut var(double p, double q, double ra, double rb, double wvno, double xka,
                              double xkb, double dpth) {
     VarOut o;
     double pex = 0.0, sex = 0.0;
