@@ -3,14 +3,17 @@
 // preproc::combine_kernels, and the host-side layer constants.  Compiled with
 // -fmad=false (see surfker_dev.cuh).
 // Out of line here, to shrink the instruction footprint: the eigenfunction
-// routines (the depth kernel 77 -> 72 ms on C3) and dltar4 (the dispersion
-// 141 -> 103 ms).  var, nevill and getsol stay inline (out of line on top of
+// routines and the complex division (the depth kernel 77 -> 72 -> 68 ms on
+// C3) and dltar4 (the dispersion 141 -> 103 ms).  var, nevill and getsol stay inline (out of line on top of
 // dltar4 they cost more in calls than they save: 107 / 137 / 179 ms).
 #ifndef SK_NOINLINE_EIG
 #define SK_NOINLINE_EIG __noinline__
 #endif
 #ifndef SK_ATTR_DLTAR4
 #define SK_ATTR_DLTAR4 __noinline__
+#endif
+#ifndef SK_CDIV_ATTR
+#define SK_CDIV_ATTR __noinline__
 #endif
 #include "surfker_dev.cuh"
 

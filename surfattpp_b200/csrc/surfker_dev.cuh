@@ -655,7 +655,10 @@ __device__ __forceinline__ cx operator*(cx a, double s) { return {a.re * s, a.im
 __device__ __forceinline__ cx operator-(double s, cx a) { return {s - a.re, -a.im}; }
 __device__ __forceinline__ cx operator/(cx a, double s) { return {a.re / s, a.im / s}; }
 // gfortran's range-reduced complex division
-__device__ __forceinline__ cx operator/(cx a, cx b) {
+#ifndef SK_CDIV_ATTR
+#define SK_CDIV_ATTR __forceinline__
+#endif
+static __device__ SK_CDIV_ATTR cx cdiv_(cx a, cx b) {
     const double ar = a.re, ai = a.im, br = b.re, bi = b.im;
     if (fabs(br) < fabs(bi)) {
         const double ratio = br / bi;
@@ -666,6 +669,7 @@ __device__ __forceinline__ cx operator/(cx a, cx b) {
     const double div = (bi * ratio) + br;
     return {((ai * ratio) + ar) / div, (ai - (ar * ratio)) / div};
 }
+__device__ __forceinline__ cx operator/(cx a, cx b) { return cdiv_(a, b); }
 __device__ __forceinline__ cx operator/(double s, cx b) { return C(s) / b; }
 __device__ __forceinline__ double cabs_(cx a) { return hypot(a.re, a.im); }
 __device__ __forceinline__ cx csqrt_real(double x) {
