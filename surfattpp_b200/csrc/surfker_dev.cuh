@@ -40,10 +40,14 @@ struct LayerConst {
     float thk[MMAX];         // unflattened float thickness (build_disp_req)
 };
 
-// Routines reached from several call sites.  Kept inline: an out-of-line
-// build (__noinline__) ran the phase kernels ~10 % faster but returned wrong
-// group-velocity dU/dvp kernels (dU/dvs and dU/drho correct, cause not
-// found), so it is not used.
+// Inlining of the routines reached from several call sites.  Each unit that
+// includes this header picks per group: surfker.cu takes the transcendentals,
+// dltar4, the eigenfunction routines and the complex division out of line
+// (smaller instruction footprint, bit-identical results); surfker_group.cu
+// keeps everything inline, because the group-velocity kernel returned wrong
+// dU/dvp values with out-of-line routines (dU/dvs, dU/drho right; cause not
+// found).  SK_NOINLINE marks the routines that stay inline everywhere
+// (dltar1, nevill, getsol: out of line they cost more than they save).
 #ifndef SK_NOINLINE
 #define SK_NOINLINE inline
 #endif
