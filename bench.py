@@ -346,9 +346,11 @@ def per_solve_timing(w, svel, nev=4):
                 + (1 - r) * q * T[j + 1, i] + r * q * T[j + 1, i + 1])
 
     rng = np.random.default_rng(11)
-    keep = np.sort(rng.choice(w.n_events, size=min(nev, w.n_events), replace=False))
+    keep = np.sort(rng.choice(w.n_events, size=min(nev + 1, w.n_events), replace=False))
     t0 = time.perf_counter()
-    for e in keep:
+    for i, e in enumerate(keep):
+        if i == 1:               # the first solve warms the path up, untimed
+            t0 = time.perf_counter()
         ip = int(ev["iper"][e])
         a0, b0, c0 = m11[ip], m22[ip], -m12[ip]
         T = eikonal.FSM_UW_PS_lonlat_2d(X, Y, a0, b0, c0, 1.0 / svel[ip], ev["evlo"][e],
@@ -360,7 +362,8 @@ def per_solve_timing(w, svel, nev=4):
         Ta = eikonal.FSM_O1_JSE_lonlat_2d(X, Y, a0, b0, c0, T, xr, yr, sadj)
         eikonal.mask_uniform_grid(X, Y, Ta, ev["evlo"][e], ev["evla"][e])
     dt = time.perf_counter() - t0
-    return {"value": keep.size / dt, "unit": UNIT, "events": int(keep.size), "dtype": "f64",
+    n = max(keep.size - 1, 1)
+    return {"value": n / dt, "unit": UNIT, "events": int(n), "dtype": "f64",
             "note": "one FP64 forward + adjoint solve per call (single-solve C ABI, host "
                     "arrays, wall clock)"}
 
