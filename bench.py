@@ -71,17 +71,27 @@ def workload_config(a, world):
             "grid": [a.n, a.n], "stations": a.nsta, "periods": a.nper,
             "events_per_rank": a.nsta * a.nper, "ranks": world,
             "l2_policy": "per-step working set > L2 (126 MB); no flush",
+            "phase_velocities": "fwdsurf of the 301x301x40 random-field model (device)",
             "graph": True, "precision": a.precision}
 
 
-def make_inputs(a, rank):
+def make_inputs(a, rank, dev=None):
+    """The C3 workload and its own Rayleigh phase velocities: SurfGrid::fwdsurf
+    of the 3-D random-field model, on the device (sa_surfdisp_columns) or,
+    for the CPU reference arm (dev None), by the CPU restatement on every host
+    thread -- the two are bit-identical."""
     from surfattpp_b200 import workloads as W
     w = W.config3(seed=1003 + rank, nsta=a.nsta, nper=a.nper, n=a.n)
-    X, Y = np.meshgrid(w.xx_deg, w.yy_deg)
-    # smooth synthetic phase-velocity planes per period (km/s)
-    svel = np.stack([3.0 + 0.9 * k / max(a.nper - 1, 1)
-                     + 0.1 * np.sin(X * 20 + k) * np.cos(Y * 17) for k in range(a.nper)])
-    return w, svel
+    if dev is None:
+        from oracle import oracle as O
+        sv, st = O.fwdsurf(w.zgrid, w.vs3d, w.periods, nthreads=os.cpu_count() or 1)
+        return w, sv
+    import torch
+    from surfattpp_b200 import surfker
+    sv, st = surfker.fwdsurf(w.zgrid, torch.as_tensor(np.ascontiguousarray(w.vs3d), device=dev),
+                             w.periods)
+    torch.cuda.synchronize()
+    return w, sv.cpu().numpy()
 
 
 class Clocks:
@@ -129,7 +139,7 @@ class Clocks:
 # DRAM bytes moved per algorithmic byte by batch_kernel<float>, from
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the same
 # kernel on the 151x151 / 3000-event case (50.645 GB moved for 73.430 GB of
-# algorithmic bytes; profiles/batch_kernel_fp32_c3_151x151_full.md).  The
+# algorithmic bytes).  The
 # algorithmic bytes count every cell of every sweep the reference performs;
 # the kernel skips cells that provably stay unchanged, so it moves less.
 # Traffic scales with cell updates, so a full launch moves algorithmic x this
@@ -160,10 +170,11 @@ def cpu_baseline(a, w, svel, nev=None):
     """The oracle (port of the reference) on a bounded sample of events with
     every host thread: 24 events per thread by default (about 10 s on the
     301x301 grid, where one FP64 forward + adjoint solve takes ~0.4 s on one
-    core)."""
+    core).  Built on this host with the reference's release flags (-O3
+    -march=native, GNU C++17)."""
     from oracle import oracle as O
     from surfattpp_b200 import workloads as W
-    O.build()
+    O.lib("native")
     rng = np.random.default_rng(7)
     nth = os.cpu_count() or 1
     nev = 24 * nth if nev is None else nev
@@ -172,9 +183,10 @@ def cpu_baseline(a, w, svel, nev=None):
     m11, m12, m22 = sub.media()
     t0 = time.perf_counter()
     O.forward_for_events(sub.xx_deg, sub.yy_deg, svel, m11, m12, m22, sub.events(),
-                         calc_adj=True, nthreads=nth)
+                         calc_adj=True, nthreads=nth, math="native")
     dt = time.perf_counter() - t0
     return {"value": keep.size / dt, "unit": UNIT, "cores": nth, "kind": "port",
+            "flags": "-O3 -DNDEBUG -march=native -std=gnu++17 (the reference's release flags)",
             "sample": f"{keep.size} random events of the same workload, fwd+adj, FP64, "
                       f"{dt:.1f} s"}
 
@@ -184,7 +196,7 @@ def run_reference(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    w, svel = make_inputs(a, 0)
+    w, svel = make_inputs(a, 0, None)
     # each step: 8 events per host thread (~3 s), so --steps 5 ends in well
     # under a minute; the sample has no warm-up state
     nev = 8 * (os.cpu_count() or 1)
@@ -307,8 +319,12 @@ def topo_media_timing(dev, stream):
             float(sig.max())], "ms_total": e0.elapsed_time(e1)}
 
 
-def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx):
-    """The same solves with the FP64 parity path (the reference's arithmetic)."""
+def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx, timed=True):
+    """The same solves with the FP64 parity path (the reference's arithmetic).
+    Also returns its per-event sweep iteration counts, which are the oracle's
+    (the FP64 parity tests assert equality): the roofline's algorithmic work
+    is counted with them."""
+    import torch
     from surfattpp_b200 import preproc
     cs = stream.cuda_stream
     ev = w.events()
@@ -316,14 +332,19 @@ def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx):
                                       ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
                                       ev["stla"], precision="fp64", ctx=ctx, graph=True)
     out = plan.run(sv, tt, wt, stream=cs)
-    plan.run(sv, tt, wt, out=out, stream=cs)
-    import torch
     torch.cuda.synchronize()
-    steps = max(1, min(a.steps, 2))
-    ms = _event_ms(stream, lambda: plan.run(sv, tt, wt, out=out, stream=cs), steps)
+    fi = out["fwd_iters"].cpu().numpy()[:w.n_events].copy()
+    ai = out["adj_iters"].cpu().numpy()[:w.n_events].copy()
+    res = None
+    if timed:
+        plan.run(sv, tt, wt, out=out, stream=cs)
+        torch.cuda.synchronize()
+        steps = max(1, min(a.steps, 2))
+        ms = _event_ms(stream, lambda: plan.run(sv, tt, wt, out=out, stream=cs), steps)
+        res = {"value": w.n_events / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+               "steps": steps, "dtype": "f64"}
     plan.close()
-    return {"value": w.n_events / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
-            "dtype": "f64"}
+    return res, fi, ai
 
 
 def per_solve_timing(w, svel, nev=4):
@@ -378,13 +399,20 @@ def run_inversion(a):
     GRF model; the inversion starts from the 1-D gradient.  Reports wall time
     per L-BFGS iteration and per misfit-gradient evaluation (synchronised)."""
     import torch
-    from surfattpp_b200 import inversion, preproc, surfker
-    from surfattpp_b200 import workloads as W
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
+    print(json.dumps(inversion_timing(a.inversion, dev)), flush=True)
+    return 0
+
+
+def inversion_timing(niter, dev):
+    """run_inversion's measurement: `niter` L-BFGS iterations on C5."""
+    import torch
+    from surfattpp_b200 import inversion, preproc, surfker
+    from surfattpp_b200 import workloads as W
     w = W.config5()
     ev = w.events()
     t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=dev)
@@ -401,7 +429,7 @@ def run_inversion(a):
     smooth = dict(ygrid=w.yy_deg, zgrid=w.zgrid, dx=0.005, dy=0.005, dz=2.0, sigma_h=0.025,
                   sigma_v=6.0)
     # the gradient taken through the torch.autograd.Function backward
-    inv = inversion.Inversion(g, tt_obs, wt, smooth=smooth, niter=a.inversion, autograd=True)
+    inv = inversion.Inversion(g, tt_obs, wt, smooth=smooth, niter=niter, autograd=True)
     vs0 = t(w.meta["vs_start"])
     inv.run_forward_adjoint(vs0)          # graph capture and first-touch, untimed
     count = [0]
@@ -430,11 +458,12 @@ def run_inversion(a):
             "s_per_gradient": dt / max(count[0], 1),
             "misfit": [float(m) for m in inv.misfit], "alphas": inv.alphas,
             "sub_iters": inv.sub_iters, "restarts": inv.restarts, "wall_s": dt}
-    print(json.dumps(line), flush=True)
-    return 0
+    g.close()
+    plan.close()
+    return line
 
 
-def run_c4(a):
+def c4_levels(dev):
     """The uneven batch with topography: per grid level (101^2, 201^2, 401^2
     over one span) the fractal-topography media (SurfGrid::
     build_media_matrix_with_topo on the device), 15 periods with U{50..600}
@@ -444,10 +473,6 @@ def run_c4(a):
     import torch
     from surfattpp_b200 import preproc, surfgrid
     from surfattpp_b200 import workloads as W
-    if int(os.environ.get("RANK", "0")) != 0:
-        return 0
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
     t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=dev)
     levels = []
     for level in (101, 201, 401):
@@ -481,6 +506,16 @@ def run_c4(a):
                        "tuned": {k: tune[k] for k in ("choice", "variant", "active_slots")},
                        "candidates_ms": [round(x, 3) for x in tune["ms"]]})
         plan.close()
+    return levels
+
+
+def run_c4(a):
+    import torch
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    levels = c4_levels(dev)
     tot_ev = sum(l["events"] for l in levels)
     tot_ms = sum(l["kernel_ms"] for l in levels)
     line = {"metric": "(src,period) fwd+adj solves/s, uneven topography batch (three grid levels)",
@@ -517,7 +552,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
     ctx = Context(local)
-    w, svel = make_inputs(a, rank)
+    w, svel = make_inputs(a, rank, dev)
     ev = w.events()
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
@@ -603,9 +638,11 @@ def main():
     d2h = h_adj.numel() * 8 + 8
 
     extra = {}
-    if world == 1 and not a.no_extras:
+    timed64 = world == 1 and not a.no_extras
+    fp64, fi64, ai64 = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx, timed=timed64)
+    if timed64:
         extra["misfit_gradient"] = misfit_gradient_timing(a, w, plan, tt, wt, dev, stream)
-        extra["fp64_plain"] = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx)
+        extra["fp64_plain"] = fp64
         extra["fp64_per_solve"] = per_solve_timing(w, svel)
         extra["pde_smooth"] = pde_smooth_timing(a, w, dev, stream, peaks()[0])
         extra["topo_media"] = topo_media_timing(dev, stream)
@@ -613,7 +650,8 @@ def main():
     if rank == 0:
         peak, peak_kind = peaks()
         bpu_f, bpu_a = (36, 20) if a.precision == "fp32" else (72, 40)
-        algo, nf, na = algorithmic_bytes(w.nx, w.ny, fwd_iters, adj_iters, bpu_f, bpu_a)
+        # work counted with the FP64 (oracle) iteration counts per event
+        algo, nf, na = algorithmic_bytes(w.nx, w.ny, fi64, ai64, bpu_f, bpu_a)
         achieved = algo / (kernel_ms * 1e-3) / 1e9
         total_events = w.n_events * world
         line = {
@@ -640,15 +678,39 @@ def main():
                          "kernel_ms": kernel_ms, "algorithmic_bytes": algo,
                          "peak_kind": peak_kind,
                          "note": "algorithmic bytes: 36 B per forward / 20 B per adjoint "
-                                 "cell update (FP32), x2 for FP64"},
+                                 "cell update (FP32), x2 for FP64, over iterations x 4 sweeps "
+                                 "x cells with the FP64 plan's (= the oracle's) per-event "
+                                 "iteration counts",
+                         "iterations": {"fp64_fwd": int(fi64.sum()), "fp64_adj": int(ai64.sum()),
+                                        "run_fwd": int(fwd_iters.sum()),
+                                        "run_adj": int(adj_iters.sum())}},
             "clocks": clk.summary(),
             "status": status,
         }
         line.update(extra)
+    plan.close()
+    if rank == 0:
+        if timed64:
+            # the other two measured configurations, so that one default run
+            # reports them: the uneven topography batch (per level) and the
+            # full inversion loop on 601x601 (one L-BFGS iteration)
+            import gc
+            gc.collect()
+            torch.cuda.empty_cache()
+            lv = c4_levels(dev)
+            line["c4_uneven_topography"] = {
+                "solves_per_s": sum(l["events"] for l in lv) / (sum(l["kernel_ms"] for l in lv)
+                                                                * 1e-3),
+                "levels": lv}
+            gc.collect()
+            torch.cuda.empty_cache()
+            inv = inversion_timing(1, dev)
+            line["c5_inversion"] = {k: inv[k] for k in ("value", "unit", "config",
+                                                        "s_per_gradient", "gradient_evaluations",
+                                                        "misfit", "alphas", "wall_s")}
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a, w, svel)
         print(json.dumps(line), flush=True)
-    plan.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

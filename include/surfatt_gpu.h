@@ -111,6 +111,18 @@ int sa_plan_forward_adjoint(sa_plan* plan, const double* svel, const double* m11
                             double* chi, int* fwd_iters, int* adj_iters, int* status,
                             void* stream);
 
+/* preproc::forward_for_event (reference src/preproc.cpp:71-148) with the
+ * adjoint source given by the caller instead of the residuals w*(Tsyn - Tobs)
+ * (:111-127): per receiver source_adj [npair] (device).  Every forward field
+ * is recomputed, the adjoint solved with that source, masked and accumulated
+ * into adj_s [nper][ny][nx] (overwritten), i.e. the reference's adjoint
+ * applied to an arbitrary vector on the receiver times -- the
+ * vector-Jacobian product used by an autograd backward.  syn [npair] and
+ * status [ne] may be NULL; no misfit is formed. */
+int sa_plan_adjoint_source(sa_plan* plan, const double* svel, const double* m11,
+                           const double* m12, const double* m22, const double* source_adj,
+                           double* syn, double* adj_s, int* status, void* stream);
+
 /* Host-array convenience over a transient plan (uploads, runs, downloads):
  * the drop-in for one call of preproc::forward_for_event. */
 int sa_forward_for_events(sa_ctx* ctx, int precision, int nx, int ny, int nper,
@@ -355,6 +367,33 @@ int sa_grad_run(sa_grad* grad, const double* vs3d, const double* vp3d, const dou
                 const double* weight, double* ker_vs, double* chi, double* svel_out,
                 double* adj_s_out, int* status, void* stream);
 
+/* Receiver travel times of a vs model: SurfGrid::fwdsurf
+ * (src/surf_grid.cpp:194-245) and the forward solve of every event
+ * (src/preproc.cpp:88-111), no adjoint.  syn [npair] (device out); svel_out
+ * (may be NULL) receives the phase velocities; status as sa_grad_run. */
+int sa_grad_forward(sa_grad* grad, const double* vs3d, double* syn, double* svel_out,
+                    int* status, void* stream);
+
+/* Vector-Jacobian product of sa_grad_forward: for a vector source_adj [npair]
+ * on the receiver times, fwdsurf and every forward field are recomputed, the
+ * adjoint is driven by source_adj (sa_plan_adjoint_source), and the depth
+ * kernels are combined into grad (nx, ny, nz):
+ *   convention 0: the reference's combine_kernels (src/preproc.cpp:276-304),
+ *     i.e. sa_grad_run's ker_vs when source_adj = w*(Tsyn - Tobs): a kernel
+ *     per unit area from dimensionless depth kernels;
+ *   convention 1: a derivative with respect to the vs nodes: times the cell
+ *     area dx R cos(lat) dy R (the adjoint source is divided by it,
+ *     src/eikonal_solver.cpp:366-367), with dc/dvs = K_b/b + K_a/a da/db +
+ *     (rho dc/drho)/rho drho/da da/db formed from the dimensionless sregn96
+ *     kernels, the density kernel corrected for the flattened velocities its
+ *     elastic terms carry once more (src/surfker/sregn96.f90:1132, :1176), and
+ *     the half-space layer added to the deepest node.  The eikonal part stays
+ *     the reference's continuous adjoint.
+ * vp3d NULL = vs2vp(vs3d).  svel_out, adj_s_out, status may be NULL. */
+int sa_grad_vjp(sa_grad* grad, const double* vs3d, const double* vp3d, const double* source_adj,
+                int convention, double* grad_out, double* svel_out, double* adj_s_out,
+                int* status, void* stream);
+
 /* Copies the last run's depth kernels into device arrays sen_vs, sen_vp,
  * sen_rho ((nx, ny, nz, nper) row-major; any may be NULL), on `stream`. */
 int sa_grad_sen(sa_grad* grad, double* sen_vs, double* sen_vp, double* sen_rho, void* stream);
@@ -368,6 +407,16 @@ int sa_grad_sen(sa_grad* grad, double* sen_vs, double* sen_vp, double* sen_rho, 
 int sa_grad_combine(sa_grad* grad, const double* vs3d, const double* vp3d, const double* adj_s,
                     double* ker_vs, void* stream);
 
+/* ---- device math test hook ------------------------------------------------- */
+
+/* No counterpart in the reference.  Evaluates the correctly rounded FP64
+ * functions the dispersion and depth-kernel routines use in place of CUDA's
+ * (and which agree with the C library the reference calls except where the C
+ * library misrounds): f = 0 exp, 1 log, 2 sin, 3 cos, 4 sin and cos (y holds
+ * n (sin, cos) pairs).  x [n], y [n or 2n]: device arrays; enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy stream). */
+int sa_math_eval(int f, size_t n, const double* x, double* y, void* stream);
+
 /* ---- allocation-free entry point ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot allocate device
@@ -375,14 +424,15 @@ int sa_grad_combine(sa_grad* grad, const double* vs3d, const double* vp3d, const
  * pool, hosts that forbid cudaMalloc after start-up, fully reserved device
  * memory): one eikonal::FSM_UW_PS_lonlat_2d solve in FP64 with every
  * intermediate in a fixed 64 MiB device array that each GPU loading this
- * library keeps until exit (grids up to ~460,000 cells; larger ones return
- * SA_ERR_ARG with a message on stderr).  All array arguments are DEVICE
- * pointers: xx_deg [nx], yy_deg [ny], spha/sphb/sphc/fun/T_out [nx*ny];
- * niter and status (may be NULL) are single device ints.  Work is enqueued on
- * `stream` (a cudaStream_t, NULL = legacy stream) after a small synchronous
- * read of the first two grid coordinates.  Calls share the array: calls that
- * overlap on the GPU race and must be serialised.  The first call on a device
- * looks up the array's address; make it before any stream capture. */
+ * library keeps until exit (145 bytes per cell: grids up to 462,400 cells,
+ * e.g. 680 x 680; larger ones return SA_ERR_ARG with a message on stderr).
+ * All array arguments are DEVICE pointers: xx_deg [nx], yy_deg [ny],
+ * spha/sphb/sphc/fun/T_out [nx*ny]; niter and status (may be NULL) are single
+ * device ints.  All work is enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy stream); the call does not wait for the GPU.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised.  The first call
+ * on a device looks up the array's address; make it before any stream
+ * capture. */
 int sa_eik_fwd_field_noalloc(int nx, int ny, const double* xx_deg, const double* yy_deg,
                              const double* spha, const double* sphb, const double* sphc,
                              const double* fun, double x0_deg, double y0_deg, double* T_out,

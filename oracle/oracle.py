@@ -17,7 +17,14 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+# The same restatement with the correctly rounded exp / log / sin / cos of
+# surfattpp_b200/csrc/crmath.cuh in place of the C library's (omath.h): the
+# device column kernels use those functions, so against this build they must
+# agree bit for bit; against the default build they differ only where the C
+# library misrounds.
+_LIB_CR_PATH = os.path.join(_HERE, "_build", "liboracle_cr.so")
 _lib = None
+_lib_cr = None
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -30,13 +37,50 @@ def build() -> str:
     return _LIB_PATH
 
 
-def lib():
-    global _lib
+_lib_native = None
+
+
+def _native_path() -> str:
+    """Per-host location of the -march=native build (keyed by the CPU model
+    and flags, so a library built on another host is never loaded)."""
+    import hashlib
+    try:
+        with open("/proc/cpuinfo") as f:
+            info = [ln for ln in f if ln.startswith(("model name", "flags"))][:2]
+    except OSError:
+        info = []
+    tag = hashlib.sha1("".join(info).encode()).hexdigest()[:12]
+    return os.path.join(_HERE, "_build", f"native-{tag}", "liboracle_native.so")
+
+
+def lib(math: str = "libc"):
+    """The oracle library; math="cr" selects the correctly rounded libm build,
+    math="native" the timing build with the reference's release flags
+    (-O3 -march=native, built on first use on this host)."""
+    global _lib, _lib_cr, _lib_native
+    if math == "native":
+        if _lib_native is None:
+            path = _native_path()
+            if not os.path.exists(path):
+                subprocess.run(["make", "-s", "-C", _HERE, "native", f"NATIVE_OUT={path}"],
+                               check=True)
+            _lib_native = _declare(C.CDLL(path))
+        return _lib_native
+    if math == "cr":
+        if _lib_cr is None:
+            if not os.path.exists(_LIB_CR_PATH):
+                build()
+            _lib_cr = _declare(C.CDLL(_LIB_CR_PATH))
+        return _lib_cr
     if _lib is not None:
         return _lib
     if not os.path.exists(_LIB_PATH):
         build()
-    L = C.CDLL(_LIB_PATH)
+    _lib = _declare(C.CDLL(_LIB_PATH))
+    return _lib
+
+
+def _declare(L):
     i, d = C.c_int, C.c_double
     L.orc_eik_fwd.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, _dp, C.POINTER(i)]
     L.orc_eik_fwd.restype = i
@@ -78,7 +122,6 @@ def lib():
     L.orc_gradient_2_geo.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp]
     L.orc_topo_media.argtypes = [i, i, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]
     L.orc_correct_depth_with_topo.argtypes = [i, i, i, i, _dp, _dp, _dp]
-    _lib = L
     return L
 
 
@@ -127,11 +170,13 @@ def interp2d(xgrid, ygrid, z, xq, yq):
     return out
 
 
-def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, nthreads=1):
+def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, nthreads=1,
+                       math="libc"):
     """preproc::forward_for_event over an event set.
 
     svel/m11/m12/m22: (nper, ny, nx).  ``ev`` is a dict with evlo, evla, iper,
     rec_ptr, rec_idx, stlo, stla, tt_obs, weight (see tests/workloads.py).
+    math: which build runs it (see lib()).
     Returns dict(syn, adj_s, chi, fwd_iters, adj_iters).
     """
     xx, yy = _c(xx_deg), _c(yy_deg)
@@ -143,7 +188,7 @@ def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, n
     chi = C.c_double(0.0)
     fi = np.zeros(max(ne, 1), np.int32)
     ai = np.zeros(max(ne, 1), np.int32)
-    lib().orc_forward_for_events(
+    lib(math).orc_forward_for_events(
         nx, ny, nper, xx, yy, _c(svel), _c(m11), _c(m12), _c(m22), ne,
         _c(ev["evlo"]), _c(ev["evla"]), _c(ev["iper"], np.int32), _c(ev["rec_ptr"], np.int32),
         _c(ev["rec_idx"], np.int32), _c(ev["stlo"]), _c(ev["stla"]), _c(ev["tt_obs"]),
@@ -198,25 +243,25 @@ def sregn96_hti(thk, vp, vs, rho, t, cp, iflsph=1):
     return outs
 
 
-def fwdsurf(zgrid, vs3d, periods, iwave=2, igr=0, nthreads=1):
+def fwdsurf(zgrid, vs3d, periods, iwave=2, igr=0, nthreads=1, math="libc"):
     """SurfGrid::fwdsurf: vs3d (nx, ny, nz) -> svel (nper, ny, nx), status (ny, nx)."""
     nx, ny, nz = vs3d.shape
     p = _c(periods)
     svel = np.zeros((p.size, ny, nx))
     st = np.zeros((ny, nx), np.int32)
-    lib().orc_fwdsurf(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, iwave, igr, svel, st,
+    lib(math).orc_fwdsurf(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, iwave, igr, svel, st,
                       int(nthreads))
     return svel, st
 
 
-def depthkernel_hti(zgrid, vs3d, periods, nthreads=1):
+def depthkernel_hti(zgrid, vs3d, periods, nthreads=1, math="libc"):
     """compute_dispersion_kernel (PH): returns sen_vs, sen_vp, sen_rho (nx,ny,nz,nper), status."""
     nx, ny, nz = vs3d.shape
     p = _c(periods)
     shp = (nx, ny, nz, p.size)
     sv, sp, sr = np.zeros(shp), np.zeros(shp), np.zeros(shp)
     st = np.zeros((ny, nx), np.int32)
-    lib().orc_depthkernel_hti(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
+    lib(math).orc_depthkernel_hti(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
                               int(nthreads))
     return sv, sp, sr, st
 
@@ -316,13 +361,13 @@ def correct_depth_with_topo(zgrid, angle, ker):
     return k
 
 
-def depthkernel_group(zgrid, vs3d, periods, nthreads=1):
+def depthkernel_group(zgrid, vs3d, periods, nthreads=1, math="libc"):
     """Rayleigh group-velocity depth kernels: sen_vs, sen_vp, sen_rho (nx,ny,nz,nper), status."""
     nx, ny, nz = vs3d.shape
     p = _c(periods)
     shp = (nx, ny, nz, p.size)
     sv, sp, sr = np.zeros(shp), np.zeros(shp), np.zeros(shp)
     st = np.zeros((ny, nx), np.int32)
-    lib().orc_depthkernel_group(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
+    lib(math).orc_depthkernel_group(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
                                 int(nthreads))
     return sv, sp, sr, st

@@ -7,6 +7,7 @@
 // that gfortran emits by default.  REAL*4 islands (sngl() arguments, default
 // literals) are kept.
 #include "oracle.h"
+#include "omath.h"
 
 #include <cmath>
 #include <vector>
@@ -44,8 +45,8 @@ inline cx csqrt_real(double x) {   // cdsqrt(dcmplx(x, 0d0)) for real x
     return {std::sqrt(x), 0.0};
 }
 inline cx cexp_(cx a) {
-    const double e = std::exp(a.re);
-    return {e * std::cos(a.im), e * std::sin(a.im)};
+    const double e = om::exp(a.re);
+    return {e * om::cos(a.im), e * om::sin(a.im)};
 }
 inline cx conj_(cx a) { return {a.re, -a.im}; }
 
@@ -105,10 +106,10 @@ VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
     o.svex = 0.0;
     const double pr = p.re, pi = p.im, qr = q.re, qi = q.im;
     o.pex = pr;
-    const cx epp = C(std::cos(pi), std::sin(pi)) / 2.0;
+    const cx epp = C(om::cos(pi), om::sin(pi)) / 2.0;
     const cx epm = conj_(epp);
     double pfac;
-    if (pr < 30.0) pfac = std::exp(-(2.0 * pr));
+    if (pr < 30.0) pfac = om::exp(-(2.0 * pr));
     else pfac = 0.0;
     o.cosp = (epp + pfac * epm).re;
     const cx sinp = epp - pfac * epm;
@@ -121,10 +122,10 @@ VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwat, double zd) {
         o.sinqr = 0.0;
     } else {
         o.svex = qr;
-        const cx eqp = C(std::cos(qi), std::sin(qi)) / 2.0;
+        const cx eqp = C(om::cos(qi), om::sin(qi)) / 2.0;
         const cx eqm = conj_(eqp);
         double svfac;
-        if (qr < 30.0) svfac = std::exp(-(2.0 * qr));
+        if (qr < 30.0) svfac = om::exp(-(2.0 * qr));
         else svfac = 0.0;
         o.cosq = (eqp + svfac * eqm).re;
         const cx sinq = eqp - svfac * eqm;
@@ -144,7 +145,7 @@ void dnka(double ca[5][5], double cosp, double rsinp, double sinpr, double cossv
             for (int i = 0; i < 5; i++) ca[i][j] = 0.0;
         double dfac;
         if (ex > 35.0) dfac = 0.0;
-        else dfac = std::exp(-ex);
+        else dfac = om::exp(-ex);
         ca[2][2] = dfac;
         ca[0][0] = cosp;
         ca[4][4] = cosp;
@@ -157,7 +158,7 @@ void dnka(double ca[5][5], double cosp, double rsinp, double sinpr, double cossv
         return;
     }
     double a0;
-    if (exa < 60.0) a0 = std::exp(-exa);
+    if (exa < 60.0) a0 = om::exp(-exa);
     else a0 = 0.0;
     const double cpcq = cosp * cossv;
     const double cpy = cosp * sinsvr;
@@ -316,7 +317,7 @@ void normc(double* ee, double& ex, int nmat) {
         t2 = t2 / t1;
         ee[i] = t2;
     }
-    ex = std::log(t1);
+    ex = om::log(t1);
 }
 
 // sregn96.f90:401-489
@@ -366,7 +367,7 @@ void hska(double AA[4][4], double cosp, double rsinp, double sinpr, double tcoss
             for (int j = 0; j < 4; j++) AA[i][j] = 0.0;
         double dfac;
         if (pex > 35.0) dfac = 0.0;
-        else dfac = std::exp(-pex);
+        else dfac = om::exp(-pex);
         AA[0][0] = dfac;
         AA[3][3] = dfac;
         AA[1][1] = cosp;
@@ -377,7 +378,7 @@ void hska(double AA[4][4], double cosp, double rsinp, double sinpr, double tcoss
     }
     double dfac;
     if ((pex - svex) > 70.0) dfac = 0.0;
-    else dfac = std::exp(svex - pex);
+    else dfac = om::exp(svex - pex);
     const double cossv = dfac * tcossv;
     const double rsinsv = dfac * trsinsv;
     const double sinsvr = dfac * tsinsvr;
@@ -462,7 +463,7 @@ void svfunc(RW& W, double omega, double wvno) {
         const double uu4 = -(tz1 * cd4) + tz2 * cd2 - tz3 * cd1;
         const double ext = W.exa[i - 1] + W.exe[i - 1] - W.exe[0];
         if (ext > -80.0 && ext < 80.0) {
-            const double fact = std::exp(ext);
+            const double fact = om::exp(ext);
             W.ur[i - 1] = uu1 * fact / f1213;
             W.uz[i - 1] = uu2 * fact / f1213;
             W.tz[i - 1] = uu3 * fact / f1213;

@@ -6,6 +6,7 @@
 // are REAL*4 (float here), unless the routine says `implicit double precision`.
 // Default-kind literals such as 0.01 or .95 are REAL*4 constants.
 #include "oracle.h"
+#include "omath.h"
 
 #include <cmath>
 #include <vector>
@@ -98,10 +99,10 @@ VarOut var(double p, double q, double ra, double rb, double wvno, double xka, do
     double sinp = 0.0, w = 0.0, x = 0.0, cosp = 0.0;
     double sinq = 0.0, y = 0.0, z = 0.0, cosq = 0.0;
     if (wvno < xka) {
-        sinp = std::sin(p);
+        sinp = om::sin(p);
         w = sinp / ra;
         x = -(ra * sinp);
-        cosp = std::cos(p);
+        cosp = om::cos(p);
     } else if (wvno == xka) {
         cosp = 1.0;
         w = dpth;
@@ -109,17 +110,17 @@ VarOut var(double p, double q, double ra, double rb, double wvno, double xka, do
     } else if (wvno > xka) {
         pex = p;
         double fac = 0.0;
-        if (p < 16) fac = std::exp(-2.0 * p);
+        if (p < 16) fac = om::exp(-2.0 * p);
         cosp = (1.0 + fac) * 0.5;
         sinp = (1.0 - fac) * 0.5;
         w = sinp / ra;
         x = ra * sinp;
     }
     if (wvno < xkb) {
-        sinq = std::sin(q);
+        sinq = om::sin(q);
         y = sinq / rb;
         z = -(rb * sinq);
-        cosq = std::cos(q);
+        cosq = om::cos(q);
     } else if (wvno == xkb) {
         cosq = 1.0;
         y = dpth;
@@ -127,7 +128,7 @@ VarOut var(double p, double q, double ra, double rb, double wvno, double xka, do
     } else if (wvno > xkb) {
         sex = q;
         double fac = 0.0;
-        if (q < 16) fac = std::exp(-2.0 * q);
+        if (q < 16) fac = om::exp(-2.0 * q);
         cosq = (1.0 + fac) * 0.5;
         sinq = (1.0 - fac) * 0.5;
         y = sinq / rb;
@@ -135,7 +136,7 @@ VarOut var(double p, double q, double ra, double rb, double wvno, double xka, do
     }
     o.exa = pex + sex;
     o.a0 = 0.0;
-    if (o.exa < 60.0) o.a0 = std::exp(-o.exa);
+    if (o.exa < 60.0) o.a0 = om::exp(-o.exa);
     o.cpcq = cosp * cosq;
     o.cpy = cosp * y;
     o.cpz = cosp * z;
@@ -201,7 +202,7 @@ void normc(double* ee, int n, double& ex) {
         t2 = t2 / t1;
         ee[i] = t2;
     }
-    ex = std::log(t1);
+    ex = om::log(t1);
 }
 
 // surfdisp96.f:801-901
@@ -294,17 +295,17 @@ double dltar1(const Model& M, double wvno, double omega) {
         const double q = static_cast<double>(M.d[m]) * rb;
         double sinq, y, z, cosq;
         if (wvno < xkb) {
-            sinq = std::sin(q);
+            sinq = om::sin(q);
             y = sinq / rb;
             z = -(rb * sinq);
-            cosq = std::cos(q);
+            cosq = om::cos(q);
         } else if (wvno == xkb) {
             cosq = 1.0;
             y = static_cast<double>(M.d[m]);
             z = 0.0;
         } else {
             double fac = 0.0;
-            if (q < 16) fac = std::exp(-2.0 * q);
+            if (q < 16) fac = om::exp(-2.0 * q);
             cosq = (1.0 + fac) * 0.5;
             sinq = (1.0 - fac) * 0.5;
             y = sinq / rb;

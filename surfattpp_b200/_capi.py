@@ -28,7 +28,8 @@ EXPORTED = (
     "sa_plan_autotune", "sa_plan_set_tune", "sa_plan_get_tune",
     "sa_surfdisp_columns", "sa_depthkernel_columns", "sa_combine_kernels_vs",
     "sa_depthkernel_columns_group",
-    "sa_eik_fwd_field_noalloc",
+    "sa_eik_fwd_field_noalloc", "sa_math_eval", "sa_plan_adjoint_source",
+    "sa_grad_forward", "sa_grad_vjp",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen", "sa_grad_combine",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
@@ -96,6 +97,10 @@ def lib():
                                                _vp, _vp]
     L.sa_combine_kernels_vs.argtypes = [_vp, i, i, i, i] + [_vp] * 7 + [_vp]
     L.sa_eik_fwd_field_noalloc.argtypes = [i, i] + [_vp] * 6 + [d, d] + [_vp] * 4
+    L.sa_math_eval.argtypes = [i, C.c_size_t, _vp, _vp, _vp]
+    L.sa_plan_adjoint_source.argtypes = [_vp] * 9 + [_vp]
+    L.sa_grad_forward.argtypes = [_vp] * 5 + [_vp]
+    L.sa_grad_vjp.argtypes = [_vp] * 4 + [i] + [_vp] * 4 + [_vp]
     L.sa_grad_create.argtypes = [_vp, i, _dp, _dp, C.POINTER(_vp)]
     L.sa_grad_destroy.argtypes = [_vp]
     L.sa_grad_run.argtypes = [_vp] + [_vp] * 9 + [_vp]

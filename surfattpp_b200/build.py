@@ -2,6 +2,7 @@
 
 Each translation unit gets the flags its arithmetic contract needs:
   eik64.cu   -fmad=false: FP64 parity path, every operation rounds as written
+  noalloc.cu -fmad=false: its geometry and metric planes round as the plan's
   eik32.cu   fast FP32 division/sqrt, FTZ: the FP32 sweep path
   surfker*.cu -fmad=false: surfdisp96 / sregn96 operation for operation
   postproc.cu -fmad=false: PDE smoothing rounds as the reference's FP64
@@ -27,10 +28,9 @@ UNITS = {
     "eik32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "surfker.cu": ["-fmad=false"],
     "surfker_group.cu": ["-fmad=false"],
-    "kernels.cu": ["-fmad=false"],
     "util.cu": [],
     "capi.cu": ["-Xcompiler", "-ffp-contract=off"],
-    "noalloc.cu": [],
+    "noalloc.cu": ["-fmad=false"],
     "postproc.cu": ["-fmad=false"],
     "optimize.cu": ["-fmad=false"],
     "topo.cu": ["-fmad=false"],

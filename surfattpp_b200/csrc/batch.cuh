@@ -200,9 +200,10 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     return fun0_64;
 }
 
+// Body of the persistent batch kernel (below), shared with the FP64 variant
+// that reads the grid spacing from device memory (eik64.cu).
 template <class S, bool ISO, int VAR>
-__global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? SA_MINB64 : SA_MINB32)
-batch_kernel(BatchArgs<S> B) {
+__device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
     const int lane = threadIdx.x & 31;
     const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (slot >= B.sc.nslots) return;
@@ -246,7 +247,13 @@ batch_kernel(BatchArgs<S> B) {
                     interp2d_pt(g.xx_deg, nx, g.yy_deg, ny, P_T, B.ev.stlo[st], B.ev.stla[st]);
                 if (B.out.syn) B.out.syn[r0 + ir] = ts;
                 P_syn[ir] = ts;
-                P_sadj[ir] = B.ev.weight[r0 + ir] * (ts - B.ev.tt_obs[r0 + ir]);
+                // residual adjoint source (src/preproc.cpp:111-115), or a
+                // caller-given one (the vector-Jacobian product of T_rec)
+                // (a forward-only run reads neither: tt_obs, weight may be NULL)
+                P_sadj[ir] = B.ev.sadj ? B.ev.sadj[r0 + ir]
+                             : B.mode == MODE_FWD
+                                 ? 0.0
+                                 : B.ev.weight[r0 + ir] * (ts - B.ev.tt_obs[r0 + ir]);
             }
             __syncwarp();
             if (B.mode == MODE_FWD_ADJ && lane == 0 && B.out.chi_ev) {
@@ -457,6 +464,12 @@ batch_kernel(BatchArgs<S> B) {
         if (lane == 0 && B.out.status) B.out.status[e] = status;
         __syncwarp();
     }
+}
+
+template <class S, bool ISO, int VAR>
+__global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? SA_MINB64 : SA_MINB32)
+batch_kernel(BatchArgs<S> B) {
+    batch_body<S, ISO, VAR>(B);
 }
 
 template <class S>

@@ -468,7 +468,7 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
 int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double* m12,
                  const double* m22, const double* tt_obs, const double* weight, int calc_adj,
                  double* syn, double* adj_s, double* chi, int* fwd_iters, int* adj_iters,
-                 int* status, cudaStream_t st) {
+                 int* status, cudaStream_t st, const double* sadj = nullptr) {
     sa_ctx* ctx = P->ctx;
     const bool general = m11 != nullptr;
     int rc = plan_media(P, svel, m11, m12, m22, general, st);
@@ -476,8 +476,9 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
     BatchDesc d = plan_desc(P, general);
     d.ev.tt_obs = tt_obs;
     d.ev.weight = weight;
+    d.ev.sadj = sadj;
     d.out.syn = syn;
-    d.out.chi_ev = (calc_adj && chi) ? P->chi_ev.p : nullptr;
+    d.out.chi_ev = (calc_adj && chi && !sadj) ? P->chi_ev.p : nullptr;
     d.out.adj_s = calc_adj ? adj_s : nullptr;
     d.out.fwd_iters = P->fit.p;
     d.out.adj_iters = P->ait.p;
@@ -493,7 +494,7 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
         if (P->timing) SA_CUDA(cudaEventRecord(P->tk0, st));
         SA_CUDA(P->prec == SA_FP64 ? launch_batch64(d, st) : launch_batch32(d, st));
         if (P->timing) SA_CUDA(cudaEventRecord(P->tk1, st));
-        if (calc_adj && chi) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi, st));
+        if (calc_adj && chi && !sadj) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi, st));
         SA_CUDA(launch_fold_status(P->ne, d.out.status, P->worst.p, st));
         const size_t ib = (size_t)P->ne * sizeof(int);
         if (fwd_iters)
@@ -666,25 +667,24 @@ extern "C" int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out
     return SA_OK;
 }
 
-extern "C" int sa_plan_forward_adjoint(sa_plan* P, const double* svel, const double* m11,
-                                       const double* m12, const double* m22,
-                                       const double* tt_obs, const double* weight, int calc_adj,
-                                       double* syn, double* adj_s, double* chi, int* fwd_iters,
-                                       int* adj_iters, int* status, void* stream) {
-    if (!P) return SA_ERR_ARG;
+namespace {
+// One evaluation, replayed from the plan's CUDA graph when the pointers repeat.
+int plan_run(sa_plan* P, const double* svel, const double* m11, const double* m12,
+             const double* m22, const double* tt_obs, const double* weight, const double* sadj,
+             int calc_adj, double* syn, double* adj_s, double* chi, int* fwd_iters,
+             int* adj_iters, int* status, void* stream) {
     sa_ctx* ctx = P->ctx;
     if (!svel) return fail(ctx, SA_ERR_ARG, "svel is required");
     if ((m11 == nullptr) != (m22 == nullptr) || (m11 == nullptr) != (m12 == nullptr))
         return fail(ctx, SA_ERR_ARG, "m11, m12, m22 must be all set or all NULL");
-    if (P->npair > 0 && (!tt_obs || !weight)) return fail(ctx, SA_ERR_ARG, "tt_obs/weight");
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     if (!P->use_graph || P->timing)
         return plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj, syn, adj_s, chi,
-                            fwd_iters, adj_iters, status, st);
+                            fwd_iters, adj_iters, status, st, sadj);
     GraphKey k{};
     const void* ptrs[17] = {svel, m11, m12, m22, tt_obs, weight, syn, adj_s, chi, fwd_iters,
-                            adj_iters, status, P->dbg_T, P->dbg_Ta, nullptr, nullptr, nullptr};
+                            adj_iters, status, P->dbg_T, P->dbg_Ta, sadj, nullptr, nullptr};
     std::memcpy(k.ptr, ptrs, sizeof(ptrs));
     k.calc_adj = calc_adj;
     if (!(P->have_graph && P->key == k)) {
@@ -700,7 +700,7 @@ extern "C" int sa_plan_forward_adjoint(sa_plan* P, const double* svel, const dou
         cudaGraph_t graph = nullptr;
         SA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         rc = plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj, syn, adj_s, chi,
-                          fwd_iters, adj_iters, status, st);
+                          fwd_iters, adj_iters, status, st, sadj);
         cudaError_t ce = cudaStreamEndCapture(st, &graph);
         if (rc) {
             if (graph) cudaGraphDestroy(graph);
@@ -715,6 +715,29 @@ extern "C" int sa_plan_forward_adjoint(sa_plan* P, const double* svel, const dou
     }
     SA_CUDA(cudaGraphLaunch(P->gexec, st));
     return SA_OK;
+}
+}  // namespace
+
+extern "C" int sa_plan_forward_adjoint(sa_plan* P, const double* svel, const double* m11,
+                                       const double* m12, const double* m22,
+                                       const double* tt_obs, const double* weight, int calc_adj,
+                                       double* syn, double* adj_s, double* chi, int* fwd_iters,
+                                       int* adj_iters, int* status, void* stream) {
+    if (!P) return SA_ERR_ARG;
+    if (P->npair > 0 && (!tt_obs || !weight)) return fail(P->ctx, SA_ERR_ARG, "tt_obs/weight");
+    return plan_run(P, svel, m11, m12, m22, tt_obs, weight, nullptr, calc_adj, syn, adj_s, chi,
+                    fwd_iters, adj_iters, status, stream);
+}
+
+extern "C" int sa_plan_adjoint_source(sa_plan* P, const double* svel, const double* m11,
+                                      const double* m12, const double* m22,
+                                      const double* source_adj, double* syn, double* adj_s,
+                                      int* status, void* stream) {
+    if (!P) return SA_ERR_ARG;
+    if (P->npair > 0 && !source_adj) return fail(P->ctx, SA_ERR_ARG, "source_adj is required");
+    if (!adj_s) return fail(P->ctx, SA_ERR_ARG, "adj_s is required");
+    return plan_run(P, svel, m11, m12, m22, nullptr, nullptr, source_adj, 1, syn, adj_s,
+                    nullptr, nullptr, nullptr, status, stream);
 }
 
 namespace {
@@ -1030,6 +1053,8 @@ struct sa_grad {
     int nz = 0;
     DArr<unsigned char> lc;
     DArr<double> periods, svel, adj_s, sen_vs, sen_vp, sen_rho;
+    DArr<double> sen_hs;     // half-space layer kernels (derivative convention)
+    DArr<double> area;       // [ny] cell area dx R cos(lat) dy R, km^2
     DArr<int> colst, worst;
     cudaStream_t side = nullptr;
     cudaEvent_t e_disp = nullptr, e_sen = nullptr;
@@ -1065,6 +1090,13 @@ extern "C" int sa_grad_create(sa_plan* plan, int nz, const double* zgrid, const 
     if (e == cudaSuccess) e = g->sen_rho.alloc(n4);
     if (e == cudaSuccess) e = g->colst.alloc(ncol);
     if (e == cudaSuccess) e = g->worst.alloc(1);
+    if (e == cudaSuccess) {
+        std::vector<double> yr(plan->ny), area(plan->ny);
+        e = cudaMemcpy(yr.data(), plan->yy.p, plan->ny * sizeof(double), cudaMemcpyDeviceToHost);
+        for (int i = 0; i < plan->ny; i++)
+            area[i] = plan->dx * R_EARTH * std::cos(yr[i]) * plan->dy * R_EARTH;
+        if (e == cudaSuccess) e = g->area.upload(area.data(), plan->ny, ctx->stream);
+    }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->e_disp, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->e_sen, cudaEventDisableTiming);
@@ -1115,6 +1147,65 @@ extern "C" int sa_grad_run(sa_grad* g, const double* vs3d, const double* vp3d,
     // combine_kernels (vs-only parametrisation)
     SA_CUDA(launch_combine_vs(nx, ny, nz, nper, adj_s, vs3d, vp3d, g->sen_vs.p, g->sen_vp.p,
                               g->sen_rho.p, ker_vs, st));
+    SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
+    return SA_OK;
+}
+
+extern "C" int sa_grad_forward(sa_grad* g, const double* vs3d, double* syn, double* svel_out,
+                               int* status, void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (!vs3d || !syn) return fail(ctx, SA_ERR_ARG, "vs3d and syn are required");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
+    double* svel = svel_out ? svel_out : g->svel.p;
+    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->periods.p, 1, 2, 0, g->lc.p, svel,
+                                    g->colst.p, st));
+    // forward only: tt_obs / weight are not read (no residuals)
+    int rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, syn,
+                      nullptr, nullptr, nullptr, nullptr, nullptr, st);
+    if (rc) return rc;
+    SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
+    return SA_OK;
+}
+
+extern "C" int sa_grad_vjp(sa_grad* g, const double* vs3d, const double* vp3d,
+                           const double* source_adj, int convention, double* grad,
+                           double* svel_out, double* adj_s_out, int* status, void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (!vs3d || !grad || (P->npair > 0 && !source_adj))
+        return fail(ctx, SA_ERR_ARG, "vs3d, source_adj and grad are required");
+    if (convention != 0 && convention != 1) return fail(ctx, SA_ERR_ARG, "convention 0 or 1");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
+    double* svel = svel_out ? svel_out : g->svel.p;
+    double* adj_s = adj_s_out ? adj_s_out : g->adj_s.p;
+    if (convention == 1) SA_CUDA(g->sen_hs.alloc((size_t)nx * ny * nper * 3));
+    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->periods.p, 1, 2, 0, g->lc.p, svel,
+                                    g->colst.p, st));
+    SA_CUDA(cudaEventRecord(g->e_disp, st));
+    // every forward field recomputed, the adjoint driven by source_adj
+    int rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, source_adj, 1,
+                      nullptr, adj_s, nullptr, nullptr, nullptr, nullptr, st);
+    if (rc) return rc;
+    SA_CUDA(cudaStreamWaitEvent(g->side, g->e_disp, 0));
+    SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p, g->sen_vs.p,
+                               g->sen_vp.p, g->sen_rho.p, g->side,
+                               convention == 1 ? g->sen_hs.p : nullptr));
+    SA_CUDA(cudaEventRecord(g->e_sen, g->side));
+    SA_CUDA(cudaStreamWaitEvent(st, g->e_sen, 0));
+    if (convention == 0)
+        SA_CUDA(launch_combine_vs(nx, ny, nz, nper, adj_s, vs3d, vp3d, g->sen_vs.p, g->sen_vp.p,
+                                  g->sen_rho.p, grad, st));
+    else
+        SA_CUDA(launch_combine_vs_derivative(nx, ny, nz, nper, adj_s, vs3d, vp3d, g->sen_vs.p,
+                                             g->sen_vp.p, g->sen_rho.p, g->sen_hs.p, g->area.p,
+                                             g->lc.p, grad, st));
     SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
     return SA_OK;
 }

@@ -74,7 +74,8 @@ struct Events {
     const double* cos_stla; // [nsta] cos(stla*DEG2RAD) (host C library)
     const double* tt_obs;   // [npair]
     const double* weight;   // [npair]
-    const double* sadj;     // [npair] explicit adjoint sources (mode ADJ_ONLY) or null
+    const double* sadj;     // [npair] explicit adjoint sources (mode ADJ_ONLY; in
+                            // FWD_ADJ they replace w*(Tsyn - Tobs)) or null
     const double* T_in;     // [ne][ny][nx] forward field input (mode ADJ_ONLY) or null
 };
 

@@ -142,4 +142,26 @@ cudaError_t launch_batch64(const BatchDesc& d, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// The FP64 batch kernel with the grid spacing dx, dy taken from device
+// memory (dxdy[0], dxdy[1]) instead of the launch arguments: for callers that
+// form the radian grid on the device and must not read it back to the host
+// (sa_eik_fwd_field_noalloc).
+template <bool ISO>
+__global__ void __launch_bounds__(128, SA_MINB64)
+batch_kernel_dev_spacing(BatchArgs<double> B, const double* __restrict__ dxdy) {
+    BatchArgs<double> Bl = B;
+    Bl.g.dx = dxdy[0];
+    Bl.g.dy = dxdy[1];
+    batch_body<double, ISO, 0>(Bl);
+}
+
+cudaError_t launch_batch64_dev_spacing(const BatchDesc& d, const double* dxdy,
+                                       cudaStream_t st) {
+    const BatchArgs<double> B = make_batch_args<double>(d);
+    const int blocks = (d.sc.nslots + 3) / 4;
+    if (d.iso) batch_kernel_dev_spacing<true><<<blocks, 128, 0, st>>>(B, dxdy);
+    else batch_kernel_dev_spacing<false><<<blocks, 128, 0, st>>>(B, dxdy);
+    return cudaGetLastError();
+}
+
 }  // namespace sa

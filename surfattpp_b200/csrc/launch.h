@@ -62,6 +62,8 @@ cudaError_t launch_geometry(int nx, int ny, int nsrc, const double* siny, const 
                             const double* sdl, T* G, T* Gx, T* Gy, double* G64,
                             cudaStream_t st);
 cudaError_t launch_batch64(const BatchDesc& d, cudaStream_t st);
+// launch_batch64 with the grid spacing read on the device from dxdy[0..1]
+cudaError_t launch_batch64_dev_spacing(const BatchDesc& d, const double* dxdy, cudaStream_t st);
 cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st);
 
 }  // namespace sa
@@ -81,7 +83,8 @@ cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, 
                                     cudaStream_t st);
 cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int nper,
                                const double* periods, const double* cp, const void* layer_const,
-                               double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st);
+                               double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st,
+                               double* sen_hs = nullptr);
 cudaError_t launch_event_cost(int ne, const int* fwd_it, const int* adj_it, unsigned int* key,
                               int* idx, cudaStream_t st);
 size_t sort_events_temp_bytes(int ne);
@@ -127,4 +130,12 @@ cudaError_t launch_combine_vs(int nx, int ny, int nz, int nper, const double* ad
                               const double* vs3d, const double* vp3d, const double* sen_vs,
                               const double* sen_vp, const double* sen_rho, double* ker_vs,
                               cudaStream_t st);
+// the vs gradient as a derivative (area Jacobian, plain dc/dvs, corrected
+// density term, half-space at the deepest node); sen_hs may be NULL
+cudaError_t launch_combine_vs_derivative(int nx, int ny, int nz, int nper, const double* adj_s,
+                                         const double* vs3d, const double* vp3d,
+                                         const double* sen_vs, const double* sen_vp,
+                                         const double* sen_rho, const double* sen_hs,
+                                         const double* area_row, const void* layer_const,
+                                         double* grad, cudaStream_t st);
 }  // namespace sa

@@ -5,27 +5,34 @@
 // real-time or embedded hosts that forbid cudaMalloc after start-up, and
 // hosts whose device memory is fully reserved up front.  For them,
 // sa_eik_fwd_field_noalloc solves one eikonal::FSM_UW_PS_lonlat_2d problem
-// with every intermediate (grid tables, metric and geometry planes, the
-// warp's sweep scratch and the work counter) in the file-scope device array
-// below.  The caller passes device inputs and outputs only.
+// with every intermediate (grid tables, metric and geometry planes, the grid
+// spacing, the warp's sweep scratch and the work counter) in the file-scope
+// device array below.  The caller passes device inputs and outputs only, and
+// the call neither allocates nor synchronises: all of it is enqueued on the
+// caller's stream.
 //
 // Limits and sharing:
 //   * the array is NOALLOC_BYTES (64 MiB) and every GPU that loads the
 //     library holds it until the process exits;
-//   * a grid needs about 144 bytes per cell, so nx*ny is limited to roughly
-//     460,000 cells; larger grids are rejected with SA_ERR_ARG and a message
-//     on stderr;
+//   * a grid needs 145 bytes per cell (56 in the metric and geometry planes,
+//     89 in the sweep scratch), so nx*ny is limited to about 462,000 cells
+//     (680 x 680 fits, 690 x 690 does not); larger grids are rejected with
+//     SA_ERR_ARG and a message on stderr;
 //   * every call shares the array and it keeps the last call's contents, so
 //     calls that overlap on the GPU (different streams or host threads at the
 //     same time) race: serialise them;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture.
+//
+// Compiled with -fmad=false: the grid, metric and geometry planes round as
+// the plan path's host arithmetic does, with correctly rounded sin and cos.
 #include <cmath>
 #include <cstdio>
 #include <mutex>
 
 #include "batch.cuh"
+#include "crmath.cuh"
 #include "launch.h"
 #include "surfatt_gpu.h"
 
@@ -36,8 +43,10 @@ constexpr size_t NOALLOC_BYTES = size_t(64) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 // Offsets of the pieces inside g_noalloc_scratch for an nx x ny grid.
+// The forward solve (MODE_FWD) reads no adjoint metric planes, so none are
+// reserved.
 struct NoAllocLayout {
-    size_t xx, yy, cosy, siny, a_row, a_arow, mt, b_p, a_a, c_a, G, Gx, Gy;
+    size_t xx, yy, cosy, siny, dxdy, mt, G, Gx, Gy;
     size_t ev_src, ev_iper, ev_evlo, ev_evla, ev_ptr, queue, slot, total;
     size_t slot_bytes;
 };
@@ -55,12 +64,8 @@ NoAllocLayout noalloc_layout(int nx, int ny) {
     L.yy = take(ny * sizeof(double));
     L.cosy = take(ny * sizeof(double));
     L.siny = take(ny * sizeof(double));
-    L.a_row = take(ny * sizeof(double));
-    L.a_arow = take(ny * sizeof(double));
+    L.dxdy = take(2 * sizeof(double));
     L.mt = take(4 * n * sizeof(double));
-    L.b_p = take(n * sizeof(double));
-    L.a_a = take(n * sizeof(double));
-    L.c_a = take(n * sizeof(double));
     L.G = take(n * sizeof(double));
     L.Gx = take(n * sizeof(double));
     L.Gy = take(n * sizeof(double));
@@ -77,10 +82,11 @@ NoAllocLayout noalloc_layout(int nx, int ny) {
 }
 
 // Builds everything the batch kernel reads besides the caller's arrays:
-// radian grids, row trigonometry, the forward metric planes from spha, sphb,
-// sphc (src/eikonal_solver.cpp:55-65), the great-circle geometry of the one
-// source (:96-116, device sin/cos/acos) and a one-event list; zeroes the work
-// counter.
+// radian grids and their spacing dx = xx(1) - xx(0), dy = yy(1) - yy(0), row
+// trigonometry, the forward metric planes from spha, sphb, sphc
+// (src/eikonal_solver.cpp:55-65), the great-circle geometry of the one
+// source (:96-116; correctly rounded sin / cos, CUDA's acos) and a one-event
+// list; zeroes the work counter.
 __global__ void noalloc_prep_kernel(int nx, int ny, const double* __restrict__ xx_deg,
                                     const double* __restrict__ yy_deg,
                                     const double* __restrict__ spha,
@@ -99,18 +105,18 @@ __global__ void noalloc_prep_kernel(int nx, int ny, const double* __restrict__ x
     const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     const size_t nth = (size_t)gridDim.x * blockDim.x;
     const double x0 = x0_deg * DEG2RAD, y0 = y0_deg * DEG2RAD;
-    const double sy0 = sin(y0), cy0 = cos(y0);
+    const double sy0 = cr::sin(y0), cy0 = cr::cos(y0);
     for (size_t i = tid; i < (size_t)nx; i += nth) xx[i] = xx_deg[i] * DEG2RAD;
     for (size_t i = tid; i < (size_t)ny; i += nth) {
         const double y = yy_deg[i] * DEG2RAD;
         yy[i] = y;
-        cosy[i] = cos(y);
-        siny[i] = sin(y);
+        cosy[i] = cr::cos(y);
+        siny[i] = cr::sin(y);
     }
     for (size_t k = tid; k < n; k += nth) {
         const int iy = (int)(k / nx), ix = (int)(k % nx);
         const double y = yy_deg[iy] * DEG2RAD;
-        const double cos_y = cos(y), sin_y = sin(y);
+        const double cos_y = cr::cos(y), sin_y = cr::sin(y);
         const double cos2_y = cos_y * cos_y;
         const double R2 = R_EARTH * R_EARTH;
         mt[4 * k + 0] = spha[k] / (R2 * cos2_y);
@@ -118,7 +124,7 @@ __global__ void noalloc_prep_kernel(int nx, int ny, const double* __restrict__ x
         mt[4 * k + 2] = sphc[k] / (R_EARTH * R_EARTH * cos_y);
         mt[4 * k + 3] = 0.0;
         const double dlon = xx_deg[ix] * DEG2RAD - x0;
-        const double cdl = cos(dlon), sdl = sin(dlon);
+        const double cdl = cr::cos(dlon), sdl = cr::sin(dlon);
         const double tmp = sin_y * sy0 + cos_y * cy0 * cdl;
         const double tmp_c = fmax(-1.0, fmin(1.0, tmp));
         G[k] = acos(tmp_c) * R_EARTH;
@@ -132,6 +138,9 @@ __global__ void noalloc_prep_kernel(int nx, int ny, const double* __restrict__ x
         }
     }
     if (tid == 0) {
+        double* dxdy = reinterpret_cast<double*>(base + L.dxdy);
+        dxdy[0] = xx_deg[1] * DEG2RAD - xx_deg[0] * DEG2RAD;
+        dxdy[1] = yy_deg[1] * DEG2RAD - yy_deg[0] * DEG2RAD;
         *reinterpret_cast<int*>(base + L.ev_src) = 0;
         *reinterpret_cast<int*>(base + L.ev_iper) = 0;
         *reinterpret_cast<double*>(base + L.ev_evlo) = x0_deg;
@@ -213,21 +222,16 @@ extern "C" int sa_eik_fwd_field_noalloc(int nx, int ny, const double* xx_deg,
     d.g.yy = reinterpret_cast<const double*>(base + L.yy);
     d.g.cosy = reinterpret_cast<const double*>(base + L.cosy);
     d.g.siny = reinterpret_cast<const double*>(base + L.siny);
-    // dx, dy as the reference forms them: xx(1) - xx(0) of the radian grid
-    double xx2[2], yy2[2];
-    if (cudaMemcpyAsync(xx2, xx_deg, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(yy2, yy_deg, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return SA_ERR_CUDA;
-    d.g.dx = xx2[1] * DEG2RAD - xx2[0] * DEG2RAD;
-    d.g.dy = yy2[1] * DEG2RAD - yy2[0] * DEG2RAD;
+    // dx, dy: formed on the device by the prep kernel (dxdy plane)
+    d.g.dx = 0.0;
+    d.g.dy = 0.0;
     d.nper = 1;
     d.iso = 0;
     d.fun64 = fun;
     d.mt64 = reinterpret_cast<const double*>(base + L.mt);
-    d.b_p64 = reinterpret_cast<const double*>(base + L.b_p);
-    d.a_a64 = reinterpret_cast<const double*>(base + L.a_a);
-    d.c_a64 = reinterpret_cast<const double*>(base + L.c_a);
+    d.b_p64 = nullptr;   // adjoint planes: not read by MODE_FWD
+    d.a_a64 = nullptr;
+    d.c_a64 = nullptr;
     d.G64 = reinterpret_cast<const double*>(base + L.G);
     d.Gx64 = reinterpret_cast<const double*>(base + L.Gx);
     d.Gy64 = reinterpret_cast<const double*>(base + L.Gy);
@@ -246,6 +250,8 @@ extern "C" int sa_eik_fwd_field_noalloc(int nx, int ny, const double* xx_deg,
     d.sc.queue = reinterpret_cast<unsigned int*>(base + L.queue);
     d.maxr = 1;
     d.mode = MODE_FWD;
-    if (launch_batch64(d, st) != cudaSuccess) return SA_ERR_CUDA;
+    if (launch_batch64_dev_spacing(d, reinterpret_cast<const double*>(base + L.dxdy), st) !=
+        cudaSuccess)
+        return SA_ERR_CUDA;
     return SA_OK;
 }

@@ -16,6 +16,9 @@
 #define SK_CDIV_ATTR __noinline__
 #endif
 #include "surfker_dev.cuh"
+#include "surfatt_gpu.h"
+
+#include <algorithm>
 
 namespace sa {
 
@@ -55,6 +58,24 @@ surfdisp_columns_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
     for (int ip = 0; ip < nper; ip++) svel[(size_t)ip * nx * ny + ix + (size_t)nx * iy] = cg[ip];
 }
 
+// The correctly rounded transcendentals on device arrays (sa_math_eval):
+// f = 0 exp, 1 log, 2 sin, 3 cos, 4 sincos (y holds sin, cos pairs); exp,
+// log and sincos through the same out-of-line routines the kernels call.
+__global__ void math_eval_kernel(int f, size_t n, const double* __restrict__ x,
+                                 double* __restrict__ y) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        switch (f) {
+            case 0: y[i] = sk::sk_exp(v); break;
+            case 1: y[i] = sk::sk_log(v); break;
+            case 2: y[i] = cr::sin(v); break;
+            case 3: y[i] = cr::cos(v); break;
+            default: sk::sk_sincos(v, &y[2 * i], &y[2 * i + 1]); break;
+        }
+    }
+}
+
 // SurfGrid::compute_dispersion_kernel (src/surf_grid.cpp:247-305) through
 // depthkernelHTI1d (src/surfdisp.cpp:481-547): one thread per (column, period)
 // runs sregn96_hti at the column's phase velocity cp.
@@ -65,7 +86,7 @@ __global__ void __launch_bounds__(64, SK_DEPTH_MINB)
 depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
                    const double* __restrict__ periods, const double* __restrict__ cp_plane,
                    const LayerConst* __restrict__ Lp, double* sen_vs, double* sen_vp,
-                   double* sen_rho) {
+                   double* sen_rho, double* sen_hs) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= (long long)nx * ny * nper) return;
     const int ip = (int)(gid % nper);
@@ -118,6 +139,15 @@ depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int 
         sen_vp[i4] = W.dcda[k] * L.rg_vtp[k] / tm3;
         sen_rho[i4] = W.dcdr[k] * L.rg_rtp[k] / tm3;
     }
+    // the half-space layer (index nz), which the reference drops: its
+    // velocities are the deepest node's, so a derivative with respect to that
+    // node includes it.  Optional, [(col * nper + ip) * 3 + {vs, vp, rho}].
+    if (sen_hs) {
+        double* h = sen_hs + ((size_t)col * nper + ip) * 3;
+        h[0] = W.dcdb[nz] * L.rg_vtp[nz] / tm3;
+        h[1] = W.dcda[nz] * L.rg_vtp[nz] / tm3;
+        h[2] = W.dcdr[nz] * L.rg_rtp[nz] / tm3;
+    }
 }
 
 // preproc::combine_kernels, vs-only branch (src/preproc.cpp:276-304): one
@@ -146,6 +176,75 @@ __global__ void combine_vs_kernel(int nx, int ny, int nz, int nper, const double
     ker_vs[i3] = k;
 }
 
+// The vs gradient as a derivative (no counterpart in the reference, whose
+// combine_kernels above is an area density built from dimensionless
+// kernels): per (ix, iy, k)
+//   g = -sum_iper adj_s * dA(iy) * dc/dvs,
+//   dc/dvs = K_b / b + K_a / a * da/db + (K_r' / rho) * drho/da * da/db,
+// with K_b, K_a, K_r the sregn96 outputs (b dc/db, a dc/da and its density
+// kernel), dA = dx R cos(lat) dy R the cell area (the adjoint source is
+// divided by it, src/eikonal_solver.cpp:366-367), and K_r' = rho dc/drho:
+// sregn96's dcdr carries the flattened velocities once more on its elastic
+// terms (src/surfker/sregn96.f90:1132, :1176, where facah, facav, facbv are
+// already a dc/da and b dc/db), so K_r' = K_r - (rtp/vtp)/2 *
+// ((a_f - 1) K_a + (b_f - 1) K_b), a_f, b_f the flattened velocities.  The
+// deepest node also takes the half-space layer's terms (sen_hs).
+__device__ inline double dcdvs_term(double kb, double ka, double kr, double vs, double vp,
+                                    double rho, double dab, double dra, double vtp, double rtp) {
+    const double af = vp * vtp, bf = vs * vtp;
+    const double krho = kr - 0.5 * (rtp / vtp) * ((af - 1.0) * ka + (bf - 1.0) * kb);
+    return kb / vs + ka / vp * dab + krho / rho * dra * dab;
+}
+
+__global__ void combine_vs_derivative_kernel(int nx, int ny, int nz, int nper,
+                                             const double* __restrict__ adj_s,
+                                             const double* __restrict__ vs3d,
+                                             const double* __restrict__ vp3d,
+                                             const double* __restrict__ sen_vs,
+                                             const double* __restrict__ sen_vp,
+                                             const double* __restrict__ sen_rho,
+                                             const double* __restrict__ sen_hs,
+                                             const double* __restrict__ area_row,
+                                             const LayerConst* __restrict__ Lp, double* grad) {
+    const size_t i3 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i3 >= (size_t)nx * ny * nz) return;
+    const LayerConst& L = *Lp;
+    const int col = (int)(i3 / nz);
+    const int k = (int)(i3 % nz);
+    const int ix = col / ny, iy = col % ny;
+    const double vs = vs3d[i3];
+    const double vp = vp3d ? vp3d[i3] : sk::vs2vp(vs);
+    const double rho = sk::vp2rho(vp);
+    const double dab = sk::dalpha_dbeta(vs);
+    const double dra = sk::drho_dalpha(vp);
+    double g = 0.0;
+    for (int ip = 0; ip < nper; ip++) {
+        const double att = adj_s[(size_t)ip * nx * ny + ix + (size_t)nx * iy];
+        const size_t i4 = i3 * nper + ip;
+        double d = dcdvs_term(sen_vs[i4], sen_vp[i4], sen_rho[i4], vs, vp, rho, dab, dra,
+                              L.rg_vtp[k], L.rg_rtp[k]);
+        if (k == nz - 1 && sen_hs) {
+            const double* h = sen_hs + ((size_t)col * nper + ip) * 3;
+            d += dcdvs_term(h[0], h[1], h[2], vs, vp, rho, dab, dra, L.rg_vtp[nz], L.rg_rtp[nz]);
+        }
+        g -= att * area_row[iy] * d;
+    }
+    grad[i3] = g;
+}
+
+cudaError_t launch_combine_vs_derivative(int nx, int ny, int nz, int nper, const double* adj_s,
+                                         const double* vs3d, const double* vp3d,
+                                         const double* sen_vs, const double* sen_vp,
+                                         const double* sen_rho, const double* sen_hs,
+                                         const double* area_row, const void* layer_const,
+                                         double* grad, cudaStream_t st) {
+    const size_t n = (size_t)nx * ny * nz;
+    combine_vs_derivative_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+        nx, ny, nz, nper, adj_s, vs3d, vp3d, sen_vs, sen_vp, sen_rho, sen_hs, area_row,
+        reinterpret_cast<const LayerConst*>(layer_const), grad);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, int nper,
                                     const double* periods, int iflsph, int iwave, int igr,
                                     const void* layer_const, double* svel, int* status,
@@ -159,11 +258,12 @@ cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, 
 
 cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int nper,
                                const double* periods, const double* cp, const void* layer_const,
-                               double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st) {
+                               double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st,
+                               double* sen_hs) {
     const long long n = (long long)nx * ny * nper;
     depthkernel_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
         nx, ny, nz, vs3d, nper, periods, cp, reinterpret_cast<const LayerConst*>(layer_const),
-        sen_vs, sen_vp, sen_rho);
+        sen_vs, sen_vp, sen_rho, sen_hs);
     return cudaGetLastError();
 }
 
@@ -240,3 +340,13 @@ int build_layer_const(int nz, const double* zgrid, void* out) {
 }
 
 }  // namespace sa
+
+extern "C" int sa_math_eval(int f, size_t n, const double* x, double* y, void* stream) {
+    if (f < 0 || f > 4 || (n > 0 && (!x || !y))) return SA_ERR_ARG;
+    if (n == 0) return SA_OK;
+    const int threads = 256;
+    const size_t blocks = std::min<size_t>((n + threads - 1) / threads, 148 * 16);
+    sa::math_eval_kernel<<<(unsigned)blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(
+        f, n, x, y);
+    return cudaGetLastError() == cudaSuccess ? SA_OK : SA_ERR_CUDA;
+}

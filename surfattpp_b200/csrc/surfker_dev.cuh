@@ -9,12 +9,15 @@
 // Compiled with -fmad=false and IEEE division/sqrt: the FP64 and REAL*4
 // arithmetic of src/surfker/surfdisp96.f and src/surfker/sregn96.f90 is kept
 // operation for operation, including the REAL*4 islands (model arrays, gtsolh,
-// sngl() arguments, default-kind literals).  Transcendentals are CUDA's
-// (sin/cos/exp/log within 1-2 ulp of the C library); the layer flattening
-// factors that involve REAL*4 powers are precomputed per layer on the host.
+// sngl() arguments, default-kind literals).  exp, log, sin and cos are the
+// correctly rounded ones of crmath.cuh, which agree with the C library the
+// reference calls except where the C library itself misrounds (about 0.1 %
+// of arguments); the layer flattening factors that involve REAL*4 powers are
+// precomputed per layer on the host.
 #pragma once
 #include <cmath>
 
+#include "crmath.cuh"
 #include "launch.h"
 
 namespace sa {
@@ -75,10 +78,9 @@ struct LayerConst {
 #else
 #define SK_MATH_ATTR __forceinline__
 #endif
-static __device__ SK_MATH_ATTR double sk_sin(double x) { return sin(x); }
-static __device__ SK_MATH_ATTR double sk_cos(double x) { return cos(x); }
-static __device__ SK_MATH_ATTR double sk_exp(double x) { return exp(x); }
-static __device__ SK_MATH_ATTR double sk_log(double x) { return log(x); }
+static __device__ SK_MATH_ATTR void sk_sincos(double x, double* s, double* c) { cr::sincos(x, s, c); }
+static __device__ SK_MATH_ATTR double sk_exp(double x) { return cr::exp(x); }
+static __device__ SK_MATH_ATTR double sk_log(double x) { return cr::log(x); }
 
 __device__ __forceinline__ double dsign1(double x) { return copysign(1.0, x); }
 
@@ -137,10 +139,9 @@ __device__ inline VarOut var(double p, double q, double ra, double rb, double wv
     double sinp = 0.0, w = 0.0, x = 0.0, cosp = 0.0;
     double sinq = 0.0, y = 0.0, z = 0.0, cosq = 0.0;
     if (wvno < xka) {
-        sinp = sk_sin(p);
+        sk_sincos(p, &sinp, &cosp);
         w = sinp / ra;
         x = -(ra * sinp);
-        cosp = sk_cos(p);
     } else if (wvno == xka) {
         cosp = 1.0;
         w = dpth;
@@ -155,10 +156,9 @@ __device__ inline VarOut var(double p, double q, double ra, double rb, double wv
         x = ra * sinp;
     }
     if (wvno < xkb) {
-        sinq = sk_sin(q);
+        sk_sincos(q, &sinq, &cosq);
         y = sinq / rb;
         z = -(rb * sinq);
-        cosq = sk_cos(q);
     } else if (wvno == xkb) {
         cosq = 1.0;
         y = dpth;
@@ -334,10 +334,9 @@ __device__ SK_NOINLINE double dltar1(const SDModel& M, double wvno, double omega
         const double q = (double)M.d[m] * rb;
         double sinq, y, z, cosq;
         if (wvno < xkb) {
-            sinq = sk_sin(q);
+            sk_sincos(q, &sinq, &cosq);
             y = sinq / rb;
             z = -(rb * sinq);
-            cosq = sk_cos(q);
         } else if (wvno == xkb) {
             cosq = 1.0;
             y = (double)M.d[m];
@@ -682,7 +681,9 @@ __device__ __forceinline__ cx csqrt_real(double x) {
 }
 __device__ __forceinline__ cx cexp_(cx a) {
     const double e = sk_exp(a.re);
-    return {e * sk_cos(a.im), e * sk_sin(a.im)};
+    double sn, cs;
+    sk_sincos(a.im, &sn, &cs);
+    return {e * cs, e * sn};
 }
 __device__ __forceinline__ cx conj_(cx a) { return {a.re, -a.im}; }
 
@@ -709,7 +710,9 @@ static __device__ SK_NOINLINE_EIG VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwa
     o.svex = 0.0;
     const double pr = p.re, pi = p.im, qr = q.re, qi = q.im;
     o.pex = pr;
-    const cx epp = C(sk_cos(pi), sk_sin(pi)) / 2.0;
+    double spi, cpi;
+    sk_sincos(pi, &spi, &cpi);
+    const cx epp = C(cpi, spi) / 2.0;
     const cx epm = conj_(epp);
     const double pfac = (pr < 30.0) ? sk_exp(-(2.0 * pr)) : 0.0;
     o.cosp = (epp + pfac * epm).re;
@@ -723,7 +726,9 @@ static __device__ SK_NOINLINE_EIG VarSv varsv(cx p, cx q, cx rp, cx rsv, int iwa
         o.sinqr = 0.0;
     } else {
         o.svex = qr;
-        const cx eqp = C(sk_cos(qi), sk_sin(qi)) / 2.0;
+        double sqi, cqi;
+        sk_sincos(qi, &sqi, &cqi);
+        const cx eqp = C(cqi, sqi) / 2.0;
         const cx eqm = conj_(eqp);
         const double svfac = (qr < 30.0) ? sk_exp(-(2.0 * qr)) : 0.0;
         o.cosq = (eqp + svfac * eqm).re;

@@ -10,11 +10,26 @@ per call for Rayleigh phase-velocity data with the vs-only parametrisation:
 Kernel preconditioning and smoothing (src/postproc.cpp) are not applied; the
 result is ``sg.ker_loc[0]`` right after ``preproc::combine_kernels``.
 
-``TravelTimeMisfit`` exposes the same evaluation as a torch.autograd.Function
-of vs3d: forward returns chi, backward returns ``grad_out * ker_vs`` -- the
-reference's adjoint gradient, which is the continuous adjoint of the eikonal
-(not the exact derivative of the discretised chi).  Device memory is held in
-torch tensors; all arithmetic runs in libsurfatt_gpu.so.
+``TravelTimes`` is the torch.autograd.Function vs3d -> receiver travel times
+T_rec: its forward runs fwdsurf and every event's forward solve and stores no
+field; its backward, for an upstream gradient g on T_rec, recomputes the
+phase velocities and every forward field, drives the adjoint with g in place
+of the residuals w (Tsyn - Tobs) (the reference's adjoint applied to g), and
+combines the depth kernels.  ``misfit`` builds chi = 0.5 sum w (T - Tobs)^2
+in torch on top of it; with ``convention="reference"`` its gradient is the
+reference's ker_vs.  ``TravelTimeMisfit`` is the fused form (one pass: forward,
+residuals and adjoint per event) with the same gradient.
+
+Conventions of the vs gradient:
+  * "reference": preproc::combine_kernels -- a kernel per unit area built
+    from sregn96's dimensionless depth kernels;
+  * "derivative": the derivative with respect to the vs nodes (cell-area
+    Jacobian, plain dc/dvs, corrected density kernel, half-space at the
+    deepest node).  Its eikonal part is still the reference's continuous
+    adjoint, which differs from the derivative of the discretised travel
+    times by the discretisation error (about 10 % on the checkerboard case).
+Device memory is held in torch tensors; all arithmetic runs in
+libsurfatt_gpu.so.
 """
 from __future__ import annotations
 
@@ -103,6 +118,35 @@ class MisfitGradient:
         _capi.check(p.ctx.h, rc)
         return ker_vs
 
+    def forward_times(self, vs3d, syn=None, svel=None, stream=None):
+        """Receiver travel times T_rec [npair] of vs3d (sa_grad_forward)."""
+        import torch
+        p = self.plan
+        dev = vs3d.device
+        if syn is None:
+            syn = torch.empty(max(p.npair, 1), dtype=torch.float64, device=dev)
+        st = torch.zeros(1, dtype=torch.int32, device=dev)
+        rc = _capi.lib().sa_grad_forward(self.h, ptr(vs3d), ptr(syn), ptr(svel), ptr(st), stream)
+        _capi.check(p.ctx.h, rc)
+        self.last_status = st
+        return syn[:p.npair]
+
+    def vjp(self, vs3d, source_adj, convention="reference", vp3d=None, grad=None,
+            adj_s=None, stream=None):
+        """The vs gradient of sum(source_adj * T_rec) (sa_grad_vjp); see the
+        module docstring for the conventions."""
+        import torch
+        p = self.plan
+        conv = {"reference": 0, "derivative": 1}[convention]
+        if grad is None:
+            grad = torch.empty((p.nx, p.ny, self.nz), dtype=torch.float64, device=vs3d.device)
+        st = torch.zeros(1, dtype=torch.int32, device=vs3d.device)
+        rc = _capi.lib().sa_grad_vjp(self.h, ptr(vs3d), ptr(vp3d), ptr(source_adj), conv,
+                                     ptr(grad), None, ptr(adj_s), ptr(st), stream)
+        _capi.check(p.ctx.h, rc)
+        self.last_status = st
+        return grad
+
     def sen(self, stream=None):
         """(sen_vs, sen_vp, sen_rho) of the last run as device tensors
         (nx, ny, nz, nper)."""
@@ -116,8 +160,55 @@ class MisfitGradient:
         return tuple(res)
 
 
+class TravelTimes:
+    """T_rec(vs3d) as a torch.autograd.Function (receiver times [npair])."""
+
+    @staticmethod
+    def apply(grad: MisfitGradient, vs3d, convention="reference"):
+        return _tt_fn().apply(vs3d, grad, convention)
+
+
+def misfit(grad: MisfitGradient, vs3d, tt_obs, weight, convention="reference"):
+    """chi = 0.5 sum w (T_rec - Tobs)^2 (src/preproc.cpp:142) in torch on top
+    of TravelTimes; its backward hands w (T - Tobs) to the adjoint, exactly
+    the reference's adjoint source (src/preproc.cpp:111-115)."""
+    T = TravelTimes.apply(grad, vs3d, convention)
+    r = T - tt_obs
+    return 0.5 * (weight * (r * r)).sum()
+
+
+_TT_FN = None
+
+
+def _tt_fn():
+    global _TT_FN
+    if _TT_FN is not None:
+        return _TT_FN
+    import torch
+
+    class _TravelTimes(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, vs3d, grad, convention):
+            vs = vs3d.detach().contiguous()
+            T = grad.forward_times(vs).clone()
+            ctx.grad = grad
+            ctx.convention = convention
+            ctx.save_for_backward(vs)     # the model only: no forward field is kept
+            return T
+
+        @staticmethod
+        def backward(ctx, g):
+            (vs,) = ctx.saved_tensors
+            g = g.detach().to(torch.float64).contiguous()
+            return ctx.grad.vjp(vs, g, ctx.convention), None, None
+
+    _TT_FN = _TravelTimes
+    return _TT_FN
+
+
 class TravelTimeMisfit:
-    """chi(vs3d) with the reference's adjoint gradient as a torch.autograd.Function."""
+    """chi(vs3d) with the reference's adjoint gradient as a torch.autograd.Function
+    (fused: one forward-residual-adjoint pass per event)."""
 
     @staticmethod
     def apply(grad: MisfitGradient, vs3d, tt_obs, weight):
@@ -173,8 +264,10 @@ class Inversion:
                  optim="lbfgs", step_length=0.02, max_sub_niter=10, c1=0.1, c2=0.9,
                  maxshrink=0.8, min_derr=0.0, data_weight=1.0, autograd=False):
         """smooth = dict(ygrid, zgrid, dx, dy, dz, sigma_h, sigma_v) or None.
-        autograd: take the kernel as the gradient of TravelTimeMisfit through
-        torch.autograd (the same evaluation behind a backward pass)."""
+        autograd: take the kernel as the torch.autograd gradient of chi built
+        in torch on TravelTimes (forward: receiver times, nothing stored;
+        backward: every forward field recomputed, the adjoint driven by
+        w (T - Tobs)) -- the reference's kernel, one extra forward pass."""
         self.g = grad
         self.tt, self.wt = tt_obs, weight
         self.smooth = smooth
@@ -193,9 +286,9 @@ class Inversion:
         from . import postproc
         if self.autograd:
             v = vs.detach().clone().requires_grad_(True)
-            c = TravelTimeMisfit.apply(self.g, v, self.tt, self.wt)
+            c = misfit(self.g, v, self.tt, self.wt)
             c.backward()
-            out = self.g.last
+            out = {"status": self.g.last_status, "chi": c.detach().reshape(1)}
             ker = v.grad
         else:
             out = self.g.run(vs, self.tt, self.wt, out=self._out)

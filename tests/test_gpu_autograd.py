@@ -1,0 +1,140 @@
+"""The torch.autograd.Function vs3d -> receiver travel times (TravelTimes)
+and its backward, on the checkerboard case (41x41x30, 10 periods, 250
+events; observed times from the checkerboard model, evaluated at the 1-D
+starting model).
+
+Bars (written here):
+  * forward: T_rec equals the plan's synthetic times and, in FP64, the
+    oracle's (1e-12 relative);
+  * chi = 0.5 sum w (T - Tobs)^2 built in torch on TravelTimes: chi equals
+    sa_grad_run's (1e-12) and its autograd gradient equals sa_grad_run's
+    ker_vs, in FP64, to 1e-12 of max|ker_vs| (adj_s is summed with FP64
+    atomics in completion order, so not bit for bit);
+  * the backward is linear in the upstream gradient (1e-12 of max);
+  * "derivative" convention: central differences of chi (+-1e-2 km/s, on
+    the oracle) agree with the gradient within 30 % on 12 nodes where
+    |ker| > 5 % of its maximum (measured 0.76-1.02 on the oracle: the
+    remaining gap is the continuous adjoint's discretisation error), while
+    the reference convention differs from them by a factor 5-7 (cell area
+    times the dimensionless-kernel conventions).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2(orc):
+    from surfattpp_b200 import workloads as W
+    w = W.config1()
+    m11, m12, m22 = w.media()
+    ev = w.events()
+    sv_true, st = orc.fwdsurf(w.zgrid, w.vs3d, w.periods, nthreads=8)
+    assert st.sum() == 0
+    ev["tt_obs"] = orc.forward_for_events(w.xx_deg, w.yy_deg, sv_true, m11, m12, m22, ev,
+                                          calc_adj=False, nthreads=8)["syn"].copy()
+    return w, ev, w.meta["vs_start"]
+
+
+def _grad(w, ev, precision="fp64"):
+    import torch
+    from surfattpp_b200 import inversion, preproc
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision=precision)
+    g = inversion.MisfitGradient(plan, w.zgrid, w.periods)
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    return plan, g, t(ev["tt_obs"]), t(ev["weight"]), t
+
+
+def test_forward_times_match_oracle(c2, gpu, orc):
+    import torch
+    from surfattpp_b200 import inversion
+    w, ev, vs0 = c2
+    plan, g, tt, wt, t = _grad(w, ev)
+    T = inversion.TravelTimes.apply(g, t(vs0))
+    torch.cuda.synchronize()
+    sv0, _ = orc.fwdsurf(w.zgrid, vs0, w.periods, nthreads=8)
+    m11, m12, m22 = w.media()
+    ref = orc.forward_for_events(w.xx_deg, w.yy_deg, sv0, m11, m12, m22, ev, calc_adj=False,
+                                 nthreads=8)["syn"]
+    got = T.cpu().numpy()
+    assert got.shape == ref.shape
+    assert np.max(np.abs(got - ref) / ref) <= 1e-12
+
+
+def test_misfit_in_torch_reproduces_ker_vs(c2, gpu):
+    import torch
+    from surfattpp_b200 import inversion
+    w, ev, vs0 = c2
+    plan, g, tt, wt, t = _grad(w, ev)
+    out = g.run(t(vs0), tt, wt)
+    torch.cuda.synchronize()
+    ker = out["ker_vs"].clone()
+    chi_ref = float(out["chi"][0])
+    vs = t(vs0).requires_grad_(True)
+    chi = inversion.misfit(g, vs, tt, wt)
+    chi.backward()
+    torch.cuda.synchronize()
+    assert abs(float(chi) - chi_ref) <= 1e-12 * abs(chi_ref)
+    scale = float(ker.abs().max())
+    assert float((vs.grad - ker).abs().max()) <= 1e-12 * scale
+    assert int(g.last_status[0]) == 0
+
+
+def test_backward_is_linear(c2, gpu):
+    import torch
+    w, ev, vs0 = c2
+    plan, g, tt, wt, t = _grad(w, ev)
+    vs = t(vs0)
+    rng = np.random.default_rng(4)
+    g1 = t(rng.standard_normal(plan.npair))
+    g2 = t(rng.standard_normal(plan.npair))
+    a = g.vjp(vs, g1).clone()
+    b = g.vjp(vs, g2).clone()
+    c = g.vjp(vs, 2.0 * g1 + g2).clone()
+    torch.cuda.synchronize()
+    scale = float(c.abs().max())
+    assert float((c - (2.0 * a + b)).abs().max()) <= 1e-12 * scale
+
+
+def test_derivative_convention_against_finite_differences(c2, gpu, orc):
+    import torch
+    from surfattpp_b200 import inversion
+    w, ev, vs0 = c2
+    plan, g, tt, wt, t = _grad(w, ev)
+    grads = {}
+    for conv in ("reference", "derivative"):
+        vs = t(vs0).requires_grad_(True)
+        inversion.misfit(g, vs, tt, wt, convention=conv).backward()
+        torch.cuda.synchronize()
+        grads[conv] = vs.grad.cpu().numpy()
+    ref = grads["reference"]
+    m11, m12, m22 = w.media()
+
+    def chi(v):
+        sv, _ = orc.fwdsurf(w.zgrid, v, w.periods, nthreads=8)
+        o = orc.forward_for_events(w.xx_deg, w.yy_deg, sv, m11, m12, m22, ev, calc_adj=False,
+                                   nthreads=8)
+        r = o["syn"] - ev["tt_obs"]
+        return 0.5 * np.sum(ev["weight"] * r * r)
+
+    big = np.argwhere(np.abs(ref) > 0.05 * np.abs(ref).max())
+    rng = np.random.default_rng(2002)
+    nodes = big[rng.choice(len(big), size=12, replace=False)]
+    h = 1e-2
+    rd, rr = [], []
+    for i, j, k in nodes:
+        vals = []
+        for s in (1.0, -1.0):
+            v = vs0.copy()
+            v[i, j, k] += s * h
+            vals.append(chi(v))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        rd.append(fd / grads["derivative"][i, j, k])
+        rr.append(fd / ref[i, j, k])
+    rd, rr = np.array(rd), np.array(rr)
+    assert np.all((rd > 0.7) & (rd < 1.3)), rd
+    assert np.all(rr > 3.0), rr
