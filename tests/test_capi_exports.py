@@ -31,3 +31,13 @@ def test_library_exports_declared_symbols():
     missing = [n for n in sorted(declared()) if not hasattr(lib, n)]
     assert not missing, missing
     assert set(_capi.EXPORTED) == declared()
+
+
+def test_cpp_adapters_compile_and_link():
+    """tests/cpp/adapters_test.cpp: C++20 adapters in the reference's layouts
+    compile against include/surfatt_gpu.h and link to the library (run on a
+    GPU by test_gpu_cpp_adapters.py)."""
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    subprocess.run(["make", "-s", "-B", "-C", os.path.join(here, "cpp")], check=True)
+    assert os.access(os.path.join(here, "_build", "adapters_test"), os.X_OK)
