@@ -91,6 +91,17 @@ void sa_plan_destroy(sa_plan* plan);
  * pointers repeat (default on). */
 int sa_plan_set_graph(sa_plan* plan, int enable);
 
+/* Deterministic accumulation of adj_s and the misfit (default off): the
+ * reference adds every event's masked Ta * svel^-3 plane to adj_s and its
+ * misfit to chi in event order (src/preproc.cpp:28-31, :142, one MPI rank).
+ * Enabled, each event writes its plane to a buffer and an ordered reduction
+ * adds the planes in event order, so adj_s and chi are reproducible bit for
+ * bit (FP64 plans: equal to the reference's single-rank sums) instead of
+ * being summed with atomics in completion order.  Events then run in chunks
+ * whose planes fit max_bytes of device memory (0 = a quarter of the free
+ * memory). */
+int sa_plan_set_deterministic(sa_plan* plan, int enable, size_t max_bytes);
+
 /* One forward (+ adjoint) evaluation of every event of the plan: replaces
  * preproc::forward_for_event (reference include/preproc.h:14,
  * src/preproc.cpp:71-148) with accumulate_kernels (:19-34), isotropic

@@ -449,6 +449,9 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
                 const MaskBox mb = mask_box(g, B.ev.evlo[e], B.ev.evla[e]);
                 const double* inv3 = B.inv3 + (size_t)ip * n;
                 double* acc = B.out.adj_s ? B.out.adj_s + (size_t)ip * n : nullptr;
+                double* con = B.out.contrib
+                                  ? B.out.contrib + (size_t)(e - B.out.contrib_e0) * n
+                                  : nullptr;
                 for (size_t k = lane; k < n; k += 32) {
                     const int iy = (int)(k / nx), ix = (int)(k % nx);
                     double v = (double)TaS[k];
@@ -456,7 +459,8 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
                     if (!isfinite(v)) finite = false;
                     if (B.out.Ta_out) B.out.Ta_out[(size_t)e * n + k] = v;
                     const double c = v * inv3[k];
-                    if (acc && c != 0.0) atomicAdd(acc + k, c);
+                    if (con) con[k] = c;
+                    else if (acc && c != 0.0) atomicAdd(acc + k, c);
                 }
             }
             if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;

@@ -132,6 +132,14 @@ struct sa_plan {
     size_t slot_bytes = 0;
     int variant = 0;      // FP32 batch-kernel launch variant (batch.cuh)
     int active = 0;       // event slots in use (0 = all nslots)
+    // deterministic accumulation (sa_plan_set_deterministic): events run in
+    // chunks of `chunk`; each writes its contribution plane to `contrib`,
+    // then the chunk is summed into adj_s in event order, per period
+    // (per_ptr[(c * (nper + 1)) + ip] .. into per_ev)
+    bool determ = false;
+    int chunk = 0;
+    DArr<double> contrib;
+    DArr<int> iota, per_ptr, per_ev;
     double* dbg_T = nullptr;
     double* dbg_Ta = nullptr;
     bool use_graph = true;
@@ -490,11 +498,34 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
     SA_CUDA(cudaMemsetAsync(P->queue.p, 0, sizeof(unsigned int), st));
     if (calc_adj && adj_s)
         SA_CUDA(cudaMemsetAsync(adj_s, 0, (size_t)P->nx * P->ny * P->nper * sizeof(double), st));
+    const bool determ = P->determ && calc_adj && adj_s && P->ne > 0;
     if (P->ne > 0) {
         if (P->timing) SA_CUDA(cudaEventRecord(P->tk0, st));
-        SA_CUDA(P->prec == SA_FP64 ? launch_batch64(d, st) : launch_batch32(d, st));
+        if (!determ) {
+            SA_CUDA(P->prec == SA_FP64 ? launch_batch64(d, st) : launch_batch32(d, st));
+        } else {
+            // chunks of events in event order; within a chunk the queue hands
+            // them out in index order, and the ordered reduction adds their
+            // planes to adj_s as the reference's event loop does
+            const size_t n = (size_t)P->nx * P->ny;
+            for (int e0 = 0, c = 0; e0 < P->ne; e0 += P->chunk, c++) {
+                const int e1 = std::min(P->ne, e0 + P->chunk);
+                BatchDesc dc = d;
+                dc.ev.ne = e1 - e0;
+                dc.sc.order = P->iota.p + e0;
+                dc.out.contrib = P->contrib.p;
+                dc.out.contrib_e0 = e0;
+                if (e0 > 0) SA_CUDA(cudaMemsetAsync(P->queue.p, 0, sizeof(unsigned int), st));
+                SA_CUDA(P->prec == SA_FP64 ? launch_batch64(dc, st) : launch_batch32(dc, st));
+                SA_CUDA(launch_ordered_accumulate(n, P->nper, e0,
+                                                  P->per_ptr.p + (size_t)c * (P->nper + 1),
+                                                  P->per_ev.p, P->contrib.p, adj_s, st));
+            }
+        }
         if (P->timing) SA_CUDA(cudaEventRecord(P->tk1, st));
-        if (calc_adj && chi && !sadj) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi, st));
+        if (calc_adj && chi && !sadj)
+            SA_CUDA(determ ? launch_sum_events_ordered(P->ne, P->chi_ev.p, chi, st)
+                           : launch_sum_events(P->ne, P->chi_ev.p, chi, st));
         SA_CUDA(launch_fold_status(P->ne, d.out.status, P->worst.p, st));
         const size_t ib = (size_t)P->ne * sizeof(int);
         if (fwd_iters)
@@ -629,6 +660,51 @@ extern "C" int sa_plan_get_tune(sa_plan* P, int* variant, int* active_slots, int
     if (variant) *variant = P->variant;
     if (active_slots) *active_slots = P->active > 0 ? std::min(P->active, P->nslots) : P->nslots;
     if (nslots) *nslots = P->nslots;
+    return SA_OK;
+}
+
+extern "C" int sa_plan_set_deterministic(sa_plan* P, int enable, size_t max_bytes) {
+    if (!P) return SA_ERR_ARG;
+    sa_ctx* ctx = P->ctx;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    P->have_graph = false;   // the evaluation's launches change
+    if (!enable) {
+        P->determ = false;
+        P->contrib.release();
+        return SA_OK;
+    }
+    const size_t n = (size_t)P->nx * P->ny;
+    if (max_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        SA_CUDA(cudaMemGetInfo(&fr, &tot));
+        max_bytes = fr / 4;
+    }
+    const int ne = std::max(P->ne, 1);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(ne, max_bytes / (n * 8)));
+    std::vector<int> iper(ne, 0);
+    if (P->ne > 0)
+        SA_CUDA(cudaMemcpy(iper.data(), P->iper.p, P->ne * sizeof(int), cudaMemcpyDeviceToHost));
+    const int nchunk = (P->ne + chunk - 1) / chunk;
+    std::vector<int> iota(ne), ptr, ev;
+    for (int e = 0; e < ne; e++) iota[e] = e;
+    for (int c = 0; c < nchunk; c++) {
+        const int e0 = c * chunk, e1 = std::min(P->ne, e0 + chunk);
+        for (int ip = 0; ip < P->nper; ip++) {
+            ptr.push_back((int)ev.size());
+            for (int e = e0; e < e1; e++)
+                if (iper[e] == ip) ev.push_back(e);
+        }
+        ptr.push_back((int)ev.size());
+    }
+    if (ptr.empty()) ptr.push_back(0);
+    if (ev.empty()) ev.push_back(0);
+    SA_CUDA(P->contrib.alloc((size_t)chunk * n));
+    SA_CUDA(P->iota.upload(iota.data(), iota.size(), ctx->stream));
+    SA_CUDA(P->per_ptr.upload(ptr.data(), ptr.size(), ctx->stream));
+    SA_CUDA(P->per_ev.upload(ev.data(), ev.size(), ctx->stream));
+    SA_CUDA(cudaStreamSynchronize(ctx->stream));
+    P->chunk = chunk;
+    P->determ = true;
     return SA_OK;
 }
 

@@ -88,6 +88,11 @@ struct Outputs {
     int* status;        // [ne] (may be null)
     double* T_out;      // [ne][ny][nx] optional full forward field
     double* Ta_out;     // [ne][ny][nx] optional full adjoint field (unmasked)
+    // deterministic accumulation: instead of adding into adj_s, each event
+    // writes its masked Ta * svel^-3 plane to contrib[(e - contrib_e0)*n]
+    // and an ordered reduction sums them in event order (may be null)
+    double* contrib;
+    int contrib_e0;
 };
 
 enum Mode : int { MODE_FWD = 0, MODE_FWD_ADJ = 1, MODE_ADJ_ONLY = 2 };

@@ -69,6 +69,13 @@ cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st);
 }  // namespace sa
 
 namespace sa {
+// deterministic accumulation of one chunk of per-event contributions, and
+// the misfit summed in event order
+cudaError_t launch_ordered_accumulate(size_t n, int nper, int e0, const int* per_ptr,
+                                      const int* per_ev, const double* contrib, double* adj_s,
+                                      cudaStream_t st);
+cudaError_t launch_sum_events_ordered(int ne, const double* chi_ev, double* chi,
+                                      cudaStream_t st);
 cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStream_t st);
 cudaError_t launch_fold_status(int ne, const int* status, int* worst, cudaStream_t st);
 }  // namespace sa

@@ -70,6 +70,47 @@ cudaError_t launch_event_cost(int ne, const int* fwd_it, const int* adj_it, unsi
     return cudaGetLastError();
 }
 
+// Deterministic accumulation (src/preproc.cpp:28-31 in event order): for one
+// chunk of events [e0, e0 + nchunk), adj_s[ip][k] += contrib[e - e0][k] over
+// the chunk's events of period ip in event order (per_ptr / per_ev: the
+// chunk's events grouped by period, ascending).  One thread per (ip, k).
+__global__ void ordered_accumulate_kernel(size_t n, int nper, int e0,
+                                          const int* __restrict__ per_ptr,
+                                          const int* __restrict__ per_ev,
+                                          const double* __restrict__ contrib, double* adj_s) {
+    const size_t gid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (gid >= n * nper) return;
+    const int ip = (int)(gid / n);
+    const size_t k = gid % n;
+    double a = adj_s[gid];
+    for (int j = per_ptr[ip]; j < per_ptr[ip + 1]; j++)
+        a += contrib[(size_t)(per_ev[j] - e0) * n + k];
+    adj_s[gid] = a;
+}
+
+// The misfit in event order, as the reference's event loop adds it
+// (src/preproc.cpp:142).
+__global__ void sum_events_ordered_kernel(int ne, const double* __restrict__ chi_ev, double* chi) {
+    double s = 0.0;
+    for (int i = 0; i < ne; i++) s += chi_ev[i];
+    *chi = s;
+}
+
+cudaError_t launch_ordered_accumulate(size_t n, int nper, int e0, const int* per_ptr,
+                                      const int* per_ev, const double* contrib, double* adj_s,
+                                      cudaStream_t st) {
+    const size_t total = n * nper;
+    ordered_accumulate_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        n, nper, e0, per_ptr, per_ev, contrib, adj_s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_events_ordered(int ne, const double* chi_ev, double* chi,
+                                      cudaStream_t st) {
+    sum_events_ordered_kernel<<<1, 1, 0, st>>>(ne, chi_ev, chi);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sum_events(int ne, const double* chi_ev, double* chi, cudaStream_t st) {
     sum_events_kernel<<<1, 1024, 0, st>>>(ne, chi_ev, chi);
     return cudaGetLastError();

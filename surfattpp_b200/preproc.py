@@ -59,6 +59,13 @@ class ForwardAdjointPlan:
         except Exception:
             pass
 
+    def set_deterministic(self, enable=True, max_bytes=0):
+        """Sum adj_s and chi in event order (reproducible bit for bit; FP64:
+        the reference's single-rank sums) instead of with atomics
+        (sa_plan_set_deterministic)."""
+        rc = _capi.lib().sa_plan_set_deterministic(self.h, int(bool(enable)), int(max_bytes))
+        _capi.check(self.ctx.h, rc)
+
     def kernel_timing(self, enable=True):
         """Record CUDA events around the batch kernel (runs without the graph)."""
         _capi.check(self.ctx.h, _capi.lib().sa_plan_kernel_timing(self.h, int(bool(enable))))

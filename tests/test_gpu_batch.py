@@ -256,3 +256,44 @@ def test_c3_full_size_fp32_against_fp64(gpu):
     assert l2 <= 1e-4, l2
     c32, c64 = res["fp32"]["chi"][0], res["fp64"]["chi"][0]
     assert abs(c32 - c64) <= 1e-4 * abs(c64)
+
+
+@pytest.mark.parametrize("chunk_events", [0, 37])
+def test_deterministic_adj_s_is_the_reference_sum(c1, gpu, orc, chunk_events):
+    """sa_plan_set_deterministic: adj_s and chi summed in event order.  FP64:
+    bit-identical to the oracle's single-thread event loop (the reference on
+    one MPI rank); a second evaluation, and a run in chunks of 37 events,
+    give the same bits."""
+    import torch
+    from surfattpp_b200 import preproc
+    w, svel0, ev, ref = c1
+    m11, m12, m22 = w.media()
+    ref1 = orc.forward_for_events(w.xx_deg, w.yy_deg, svel0, m11, m12, m22, ev, calc_adj=True,
+                                  nthreads=1)
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision="fp64")
+    n = w.nx * w.ny
+    plan.set_deterministic(True, max_bytes=chunk_events * n * 8)
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    sv, tt, wt = t(svel0), t(ev["tt_obs"]), t(ev["weight"])
+    outs = []
+    for _ in range(2):
+        o = plan.run(sv, tt, wt)
+        torch.cuda.synchronize()
+        outs.append((o["adj_s"].cpu().numpy().copy(), float(o["chi"][0])))
+    for adj, chi in outs:
+        assert np.array_equal(adj, ref1["adj_s"])
+        assert chi == ref1["chi"]
+    # FP32 plan: reproducible run to run
+    p32 = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                     ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                     ev["stla"], precision="fp32")
+    p32.set_deterministic(True, max_bytes=chunk_events * n * 8)
+    a = p32.run(sv, tt, wt)["adj_s"].clone()
+    b = p32.run(sv, tt, wt)["adj_s"].clone()
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    plan.close()
+    p32.close()
