@@ -366,6 +366,16 @@ int sa_grad_create(sa_plan* plan, int nz, const double* zgrid, const double* per
                    sa_grad** out);
 void sa_grad_destroy(sa_grad* grad);
 
+/* The data type the handle evaluates (the reference's surfType loop,
+ * src/inversion.cpp:250-296): 0 Rayleigh phase velocities (default), 1
+ * Rayleigh group velocities -- fwdsurf with igr = 1 for the travel times and
+ * the group depth kernels of SurfGrid::compute_dispersion_kernel, itype 1
+ * (depthkernel_rayleigh_group, src/surfdisp.cpp:203-285: phase velocities at
+ * t and t(1 +- 0.005), sregnpu).  The joint misfit and gradient are the
+ * weighted sums over one handle per data type (weights of the reference's
+ * data section). */
+int sa_grad_set_data_type(sa_grad* grad, int igr);
+
 /* Device arrays: vs3d, vp3d (NULL = Brocher vs2vp(vs3d), as the model keeps it
  * for vs-only inversions), ker_vs: (nx, ny, nz) row-major; tt_obs, weight:
  * [npair]; chi: 1 double.  svel_out and adj_s_out ([nper][ny][nx], may be

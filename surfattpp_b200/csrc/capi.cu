@@ -1132,6 +1132,12 @@ struct sa_grad {
     DArr<double> sen_hs;     // half-space layer kernels (derivative convention)
     DArr<double> area;       // [ny] cell area dx R cos(lat) dy R, km^2
     DArr<int> colst, worst;
+    // data type: 0 Rayleigh phase, 1 Rayleigh group (sa_grad_set_data_type).
+    // Group data: svel are group velocities; the depth kernels come from the
+    // phase velocities at t, t(1 + 0.005), t(1 - 0.005) (per3, cps3) and
+    // sregnpu; colst then holds 4 status planes (group, 3 phase runs)
+    int igr = 0;
+    DArr<double> per3, cps3;
     cudaStream_t side = nullptr;
     cudaEvent_t e_disp = nullptr, e_sen = nullptr;
     ~sa_grad() {
@@ -1192,6 +1198,71 @@ extern "C" void sa_grad_destroy(sa_grad* g) {
     delete g;
 }
 
+namespace {
+// The data type's velocities (phase or group) into svel, column statuses
+// into g->colst, on `st`.
+int grad_velocities(sa_grad* g, const double* vs3d, double* svel, cudaStream_t st) {
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    SA_CUDA(launch_surfdisp_columns(P->nx, P->ny, g->nz, vs3d, P->nper, g->periods.p, 1, 2,
+                                    g->igr, g->lc.p, svel, g->colst.p, st));
+    return SA_OK;
+}
+// The data type's depth kernels on `st` (phase: sregn96_hti at svel; group:
+// three phase-velocity runs and sregnpu), sen_hs optional (phase only).
+int grad_depth_kernels(sa_grad* g, const double* vs3d, const double* svel, double* sen_hs,
+                       cudaStream_t st) {
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
+    if (g->igr == 0) {
+        SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p,
+                                   g->sen_vs.p, g->sen_vp.p, g->sen_rho.p, st, sen_hs));
+        return SA_OK;
+    }
+    const size_t plane = (size_t)nx * ny * nper, ncol = (size_t)nx * ny;
+    for (int k = 0; k < 3; k++)
+        SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->per3.p + k * nper, 1, 2, 0,
+                                        g->lc.p, g->cps3.p + k * plane,
+                                        g->colst.p + (k + 1) * ncol, st));
+    SA_CUDA(launch_depthkernel_group(nx, ny, nz, vs3d, nper, g->per3.p, g->per3.p + nper,
+                                     g->per3.p + 2 * nper, g->cps3.p, g->cps3.p + plane,
+                                     g->cps3.p + 2 * plane, g->lc.p, g->sen_vs.p, g->sen_vp.p,
+                                     g->sen_rho.p, st));
+    return SA_OK;
+}
+int grad_ncolst(const sa_grad* g) {
+    return (g->igr ? 4 : 1) * g->plan->nx * g->plan->ny;
+}
+}  // namespace
+
+extern "C" int sa_grad_set_data_type(sa_grad* g, int igr) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (igr != 0 && igr != 1) return fail(ctx, SA_ERR_ARG, "data type: 0 phase, 1 group");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    const int nper = P->nper;
+    const size_t ncol = (size_t)P->nx * P->ny;
+    if (igr == 1) {
+        std::vector<double> hp(nper), t3(3 * (size_t)nper);
+        SA_CUDA(cudaMemcpy(hp.data(), g->periods.p, nper * sizeof(double), cudaMemcpyDeviceToHost));
+        const double dt = 0.01;   // src/surfdisp.cpp:223-228
+        for (int i = 0; i < nper; ++i) {
+            t3[i] = hp[i];
+            t3[nper + i] = hp[i] * (1.0 + 0.5 * dt);
+            t3[2 * nper + i] = hp[i] * (1.0 - 0.5 * dt);
+        }
+        SA_CUDA(g->per3.upload(t3.data(), t3.size(), ctx->stream));
+        SA_CUDA(g->cps3.alloc(3 * ncol * nper));
+        SA_CUDA(g->colst.alloc(4 * ncol));
+        SA_CUDA(cudaMemsetAsync(g->colst.p, 0, 4 * ncol * sizeof(int), ctx->stream));
+        SA_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    g->igr = igr;
+    return SA_OK;
+}
+
 extern "C" int sa_grad_run(sa_grad* g, const double* vs3d, const double* vp3d,
                            const double* tt_obs, const double* weight, double* ker_vs,
                            double* chi, double* svel_out, double* adj_s_out, int* status,
@@ -1205,25 +1276,26 @@ extern "C" int sa_grad_run(sa_grad* g, const double* vs3d, const double* vp3d,
     const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
     double* svel = svel_out ? svel_out : g->svel.p;
     double* adj_s = adj_s_out ? adj_s_out : g->adj_s.p;
-    // SurfGrid::fwdsurf (phase, Rayleigh, spherical earth)
-    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->periods.p, 1, 2, 0, g->lc.p, svel,
-                                    g->colst.p, st));
+    // SurfGrid::fwdsurf (Rayleigh phase or group velocities, spherical earth)
+    int rc = grad_velocities(g, vs3d, svel, st);
+    if (rc) return rc;
     SA_CUDA(cudaEventRecord(g->e_disp, st));
     // forward_for_event over every event (accumulates adj_s and the misfit)
-    int rc = sa_plan_forward_adjoint(P, svel, nullptr, nullptr, nullptr, tt_obs, weight, 1,
-                                     nullptr, adj_s, chi, nullptr, nullptr, nullptr, st);
+    rc = sa_plan_forward_adjoint(P, svel, nullptr, nullptr, nullptr, tt_obs, weight, 1, nullptr,
+                                 adj_s, chi, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
     // compute_dispersion_kernel on a second stream: it needs only vs3d and the
-    // phase velocities, so it runs while the event batch drains
+    // velocities, so it runs while the event batch drains
     SA_CUDA(cudaStreamWaitEvent(g->side, g->e_disp, 0));
-    SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p, g->sen_vs.p,
-                               g->sen_vp.p, g->sen_rho.p, g->side));
+    rc = grad_depth_kernels(g, vs3d, svel, nullptr, g->side);
+    if (rc) return rc;
     SA_CUDA(cudaEventRecord(g->e_sen, g->side));
     SA_CUDA(cudaStreamWaitEvent(st, g->e_sen, 0));
     // combine_kernels (vs-only parametrisation)
     SA_CUDA(launch_combine_vs(nx, ny, nz, nper, adj_s, vs3d, vp3d, g->sen_vs.p, g->sen_vp.p,
                               g->sen_rho.p, ker_vs, st));
-    SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
+    SA_CUDA(launch_grad_status(grad_ncolst(g), g->colst.p, P->worst.p,
+                               status ? status : g->worst.p, st));
     return SA_OK;
 }
 
@@ -1237,11 +1309,13 @@ extern "C" int sa_grad_forward(sa_grad* g, const double* vs3d, double* syn, doub
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
     double* svel = svel_out ? svel_out : g->svel.p;
-    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->periods.p, 1, 2, 0, g->lc.p, svel,
-                                    g->colst.p, st));
+    (void)nz;
+    (void)nper;
+    int rc = grad_velocities(g, vs3d, svel, st);
+    if (rc) return rc;
     // forward only: tt_obs / weight are not read (no residuals)
-    int rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, syn,
-                      nullptr, nullptr, nullptr, nullptr, nullptr, st);
+    rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, syn, nullptr,
+                  nullptr, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
     SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
     return SA_OK;
@@ -1256,23 +1330,24 @@ extern "C" int sa_grad_vjp(sa_grad* g, const double* vs3d, const double* vp3d,
     if (!vs3d || !grad || (P->npair > 0 && !source_adj))
         return fail(ctx, SA_ERR_ARG, "vs3d, source_adj and grad are required");
     if (convention != 0 && convention != 1) return fail(ctx, SA_ERR_ARG, "convention 0 or 1");
+    if (convention == 1 && g->igr != 0)
+        return fail(ctx, SA_ERR_ARG, "the derivative convention is for phase-velocity data");
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
     double* svel = svel_out ? svel_out : g->svel.p;
     double* adj_s = adj_s_out ? adj_s_out : g->adj_s.p;
     if (convention == 1) SA_CUDA(g->sen_hs.alloc((size_t)nx * ny * nper * 3));
-    SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->periods.p, 1, 2, 0, g->lc.p, svel,
-                                    g->colst.p, st));
+    int rc = grad_velocities(g, vs3d, svel, st);
+    if (rc) return rc;
     SA_CUDA(cudaEventRecord(g->e_disp, st));
     // every forward field recomputed, the adjoint driven by source_adj
-    int rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, source_adj, 1,
-                      nullptr, adj_s, nullptr, nullptr, nullptr, nullptr, st);
+    rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, source_adj, 1, nullptr,
+                  adj_s, nullptr, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
     SA_CUDA(cudaStreamWaitEvent(g->side, g->e_disp, 0));
-    SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p, g->sen_vs.p,
-                               g->sen_vp.p, g->sen_rho.p, g->side,
-                               convention == 1 ? g->sen_hs.p : nullptr));
+    rc = grad_depth_kernels(g, vs3d, svel, convention == 1 ? g->sen_hs.p : nullptr, g->side);
+    if (rc) return rc;
     SA_CUDA(cudaEventRecord(g->e_sen, g->side));
     SA_CUDA(cudaStreamWaitEvent(st, g->e_sen, 0));
     if (convention == 0)
@@ -1282,7 +1357,8 @@ extern "C" int sa_grad_vjp(sa_grad* g, const double* vs3d, const double* vp3d,
         SA_CUDA(launch_combine_vs_derivative(nx, ny, nz, nper, adj_s, vs3d, vp3d, g->sen_vs.p,
                                              g->sen_vp.p, g->sen_rho.p, g->sen_hs.p, g->area.p,
                                              g->lc.p, grad, st));
-    SA_CUDA(launch_grad_status(nx * ny, g->colst.p, P->worst.p, status ? status : g->worst.p, st));
+    SA_CUDA(launch_grad_status(grad_ncolst(g), g->colst.p, P->worst.p,
+                               status ? status : g->worst.p, st));
     return SA_OK;
 }
 

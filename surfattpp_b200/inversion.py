@@ -45,7 +45,8 @@ from .preproc import ForwardAdjointPlan, _c
 class MisfitGradient:
     """One misfit-gradient evaluation per ``run`` (sa_grad)."""
 
-    def __init__(self, plan: ForwardAdjointPlan, zgrid, periods):
+    def __init__(self, plan: ForwardAdjointPlan, zgrid, periods, data_type="ph"):
+        """data_type "ph" (Rayleigh phase velocities) or "gr" (group)."""
         self.plan = plan
         self.zgrid = _c(zgrid)
         self.periods = _c(periods)
@@ -56,6 +57,10 @@ class MisfitGradient:
         rc = _capi.lib().sa_grad_create(plan.h, self.nz, self.zgrid, self.periods, C.byref(h))
         _capi.check(plan.ctx.h, rc)
         self.h = h
+        self.data_type = data_type
+        igr = {"ph": 0, "gr": 1}[data_type]
+        if igr:
+            _capi.check(plan.ctx.h, _capi.lib().sa_grad_set_data_type(self.h, igr))
 
     def close(self):
         if getattr(self, "h", None):
@@ -243,8 +248,8 @@ def _fn():
 
 
 class Inversion:
-    """Inversion::run_inversion (reference src/inversion.cpp:106-160) for one
-    data type (Rayleigh phase), vs-only parametrisation, on the device.
+    """Inversion::run_inversion (reference src/inversion.cpp:106-160) for
+    Rayleigh phase and/or group data, vs-only parametrisation, on the device.
 
     Per iteration: the forward/adjoint gradient (``MisfitGradient``), kernel
     smoothing (PostProc::pde_smooth, smooth_method 0) giving
@@ -262,8 +267,13 @@ class Inversion:
 
     def __init__(self, grad: MisfitGradient, tt_obs, weight, smooth=None, niter=10,
                  optim="lbfgs", step_length=0.02, max_sub_niter=10, c1=0.1, c2=0.9,
-                 maxshrink=0.8, min_derr=0.0, data_weight=1.0, autograd=False):
+                 maxshrink=0.8, min_derr=0.0, data_weight=1.0, autograd=False,
+                 more_data=None):
         """smooth = dict(ygrid, zgrid, dx, dy, dz, sigma_h, sigma_v) or None.
+        more_data: further data types as (MisfitGradient, tt_obs, weight,
+        data_weight) tuples, e.g. group-velocity data next to phase data; the
+        misfit, kernel and gradient are summed over the types as
+        src/inversion.cpp:250-296 does.
         autograd: take the kernel as the torch.autograd gradient of chi built
         in torch on TravelTimes (forward: receiver times, nothing stored;
         backward: every forward field recomputed, the adjoint driven by
@@ -275,37 +285,44 @@ class Inversion:
         self.step_length, self.max_sub_niter = step_length, int(max_sub_niter)
         self.c1, self.c2, self.maxshrink, self.min_derr = c1, c2, maxshrink, min_derr
         self.w = data_weight
+        self.data = [(grad, tt_obs, weight, data_weight)] + list(more_data or [])
+        self._outs = [None] * len(self.data)
         self.autograd = bool(autograd)
         self.misfit, self.alphas, self.sub_iters, self.restarts = [], [], [], 0
         self._out = None
 
     def run_forward_adjoint(self, vs):
         """Inversion::run_forward_adjoint(true) (src/inversion.cpp:245-296):
-        returns (misfit, ker_curr, gradient)."""
+        for every data type, misfit_total += chi w, ker_curr += K w and
+        gradient += smooth(K) w / chi; returns (misfit_total, ker_curr,
+        gradient)."""
         import torch
         from . import postproc
-        if self.autograd:
-            v = vs.detach().clone().requires_grad_(True)
-            c = misfit(self.g, v, self.tt, self.wt)
-            c.backward()
-            out = {"status": self.g.last_status, "chi": c.detach().reshape(1)}
-            ker = v.grad
-        else:
-            out = self.g.run(vs, self.tt, self.wt, out=self._out)
-            self._out = out
-            ker = out["ker_vs"]
-        torch.cuda.synchronize()
-        if int(out["status"][0]) != 0:
-            raise _capi.SAError(int(out["status"][0]), "forward/adjoint evaluation failed")
-        chi = float(out["chi"][0])
-        ker_curr = ker * self.w
-        sm = ker.clone()
-        if self.smooth is not None:
-            s = self.smooth
-            postproc.pde_smooth(sm, s["ygrid"], s["zgrid"], s["dx"], s["dy"], s["dz"],
-                                s["sigma_h"], s["sigma_v"])
-        grad = sm * self.w / chi
-        return chi * self.w, ker_curr, grad
+        total, ker_curr, grad = 0.0, None, None
+        for i, (g, tt, wt, dw) in enumerate(self.data):
+            if self.autograd:
+                v = vs.detach().clone().requires_grad_(True)
+                c = misfit(g, v, tt, wt)
+                c.backward()
+                out = {"status": g.last_status, "chi": c.detach().reshape(1)}
+                ker = v.grad
+            else:
+                out = g.run(vs, tt, wt, out=self._outs[i])
+                self._outs[i] = out
+                ker = out["ker_vs"]
+            torch.cuda.synchronize()
+            if int(out["status"][0]) != 0:
+                raise _capi.SAError(int(out["status"][0]), "forward/adjoint evaluation failed")
+            chi = float(out["chi"][0])
+            sm = ker.clone()
+            if self.smooth is not None:
+                s = self.smooth
+                postproc.pde_smooth(sm, s["ygrid"], s["zgrid"], s["dx"], s["dy"], s["dz"],
+                                    s["sigma_h"], s["sigma_v"])
+            total += chi * dw
+            ker_curr = ker * dw if ker_curr is None else ker_curr + ker * dw
+            grad = sm * dw / chi if grad is None else grad + sm * dw / chi
+        return total, ker_curr, grad
 
     def _check_convergence(self, it):
         """src/inversion.cpp:212-243."""

@@ -164,3 +164,48 @@ def test_gradient_finite_differences(c2, gpu):
     assert np.all(np.sign(fd) == np.sign(kk)), np.c_[fd, kk]
     r = np.corrcoef(fd, kk)[0, 1]
     assert r >= 0.95, r
+
+
+def test_joint_phase_and_group_gradient(c2, gpu, orc):
+    """Rayleigh phase and group data together (src/inversion.cpp:250-296):
+    misfit_total = sum w_t chi_t, ker_curr = sum w_t K_t, gradient = sum
+    w_t K_t / chi_t over the two types.  Group data: group velocities from
+    fwdsurf (igr = 1) and the sregnpu kernels.  FP64 against the oracle's
+    chain: misfits 1e-12; kernels 1e-12 of max against the oracle evaluated
+    with the device's correctly rounded exp/log/sin/cos, 1e-9 against the
+    C-library oracle (group kernels carry the C library's misroundings at
+    1e-10 of a column's largest value)."""
+    import torch
+    from surfattpp_b200 import inversion
+    w, ev, vs0, ref = c2
+    m11, m12, m22 = w.media()
+    u_true, _ = orc.fwdsurf(w.zgrid, w.vs3d, w.periods, igr=1, nthreads=8)
+    ev_gr = dict(ev)
+    ev_gr["tt_obs"] = orc.forward_for_events(w.xx_deg, w.yy_deg, u_true, m11, m12, m22, ev,
+                                             calc_adj=False, nthreads=8)["syn"].copy()
+    u0, _ = orc.fwdsurf(w.zgrid, vs0, w.periods, igr=1, nthreads=8)
+    ref_gr = orc.forward_for_events(w.xx_deg, w.yy_deg, u0, m11, m12, m22, ev_gr, calc_adj=True,
+                                    nthreads=8)
+    vp0 = np.vectorize(orc.vs2vp)(vs0)
+    wph, wgr = 0.7, 0.3
+    kers = []
+    for math in ("cr", "libc"):
+        sp = orc.depthkernel_hti(w.zgrid, vs0, w.periods, nthreads=8, math=math)
+        sg = orc.depthkernel_group(w.zgrid, vs0, w.periods, nthreads=8, math=math)
+        kph = orc.combine_kernels_vs(ref["adj_s"], vs0, vp0, *sp[:3])
+        kgr = orc.combine_kernels_vs(ref_gr["adj_s"], vs0, vp0, *sg[:3])
+        kers.append((kph, kgr))
+    plan, g_ph, tt, wt, t = _grad(w, ev, "fp64")
+    g_gr = inversion.MisfitGradient(plan, w.zgrid, w.periods, data_type="gr")
+    inv = inversion.Inversion(g_ph, tt, wt, smooth=None, data_weight=wph,
+                              more_data=[(g_gr, t(ev_gr["tt_obs"]), wt, wgr)])
+    total, ker_curr, grad = inv.run_forward_adjoint(t(vs0))
+    torch.cuda.synchronize()
+    want = wph * ref["chi"] + wgr * ref_gr["chi"]
+    assert abs(total - want) <= 1e-12 * abs(want)
+    kc, gr = ker_curr.cpu().numpy(), grad.cpu().numpy()
+    for (kph, kgr), tol in zip(kers, (1e-12, 1e-9)):
+        kref = wph * kph + wgr * kgr
+        gref = wph * kph / ref["chi"] + wgr * kgr / ref_gr["chi"]
+        assert np.abs(kc - kref).max() <= tol * np.abs(kref).max()
+        assert np.abs(gr - gref).max() <= tol * np.abs(gref).max()
