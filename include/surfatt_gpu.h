@@ -434,7 +434,7 @@ int sa_grad_combine(sa_grad* grad, const double* vs3d, const double* vp3d, const
  * functions the dispersion and depth-kernel routines use in place of CUDA's
  * (and which agree with the C library the reference calls except where the C
  * library misrounds): f = 0 exp, 1 log, 2 sin, 3 cos, 4 sin and cos (y holds
- * n (sin, cos) pairs).  x [n], y [n or 2n]: device arrays; enqueued on
+ * n (sin, cos) pairs), 5 pow(x, -3) (the kernel accumulation's svel^-3).  x [n], y [n or 2n]: device arrays; enqueued on
  * `stream` (a cudaStream_t, NULL = legacy stream). */
 int sa_math_eval(int f, size_t n, const double* x, double* y, void* stream);
 

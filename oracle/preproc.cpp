@@ -1,6 +1,7 @@
 // CPU oracle: per-event forward/adjoint driver, kernel accumulation, kernel
 // combination and the Brocher relations.  TEST INFRASTRUCTURE ONLY.
 #include "oracle.h"
+#include "omath.h"
 
 #include <cmath>
 #include <thread>
@@ -74,7 +75,7 @@ double run_event(const EventRange& R, int ie, double* adj_acc) {
     if (R.adj_iters) R.adj_iters[ie] = it;
     orc_mask_uniform_grid(nx, ny, R.xx_deg, R.yy_deg, Ta.data(), R.evlo[ie], R.evla[ie]);
     double* acc = adj_acc + static_cast<size_t>(ip) * n;
-    for (int k = 0; k < n; k++) acc[k] += Ta[k] * std::pow(svel[k], -3.0);
+    for (int k = 0; k < n; k++) acc[k] += Ta[k] * om::pow_m3(svel[k]);   // pow(svel, -3)
     double s = 0.0;
     for (int i = 0; i < nr; i++) {
         const double r = ttsyn[i] - R.tt_obs[r0 + i];

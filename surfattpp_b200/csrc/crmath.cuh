@@ -294,6 +294,21 @@ CR_HD inline double cos(double x) {
     return fast_two_sum(v.hi, v.lo).hi;
 }
 
+// ---- x^-3 ------------------------------------------------------------------
+// pow(x, -3.0) correctly rounded (normal x, result normal): x^3 as an exact
+// double-double product chain, then 1 / x^3 with one Newton correction in
+// double-double.
+CR_HD inline double pow_m3(double x) {
+    const dd x2 = two_prod(x, x);
+    const dd x3 = dd_mul_d(x2, x);              // x^3 to about 2^-104 relative
+    const double q = 1.0 / x3.hi;
+    // r = 1 - q * x3 (exact pieces), y = q + q r
+    const dd p = two_prod(q, x3.hi);
+    const double r = ((1.0 - p.hi) - p.lo) - q * x3.lo;
+    const dd y = fast_two_sum(q, q * r);
+    return y.hi;
+}
+
 // sin and cos of one argument with one reduction
 CR_HD inline void sincos(double x, double* sn, double* cs) {
     const double ax = fabs(x);

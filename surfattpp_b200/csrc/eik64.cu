@@ -7,6 +7,7 @@
 #include "common.cuh"
 #include "event_common.cuh"
 #include "batch.cuh"
+#include "crmath.cuh"
 #include "launch.h"
 
 namespace sa {
@@ -27,7 +28,7 @@ __global__ void media64_kernel(int nx, int ny, int nper, const double* __restric
          i += (size_t)gridDim.x * blockDim.x) {
         const double s = svel[i];
         fun[i] = (1.0 / s) * 1.0;
-        inv3[i] = pow(s, -3.0);
+        inv3[i] = cr::pow_m3(s);   // pow(svel, -3), correctly rounded
         if (m11) {
             const int iy = (int)((i % n) / nx);
             const double cos_y = cosy[iy];

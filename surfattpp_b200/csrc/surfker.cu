@@ -59,7 +59,8 @@ surfdisp_columns_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
 }
 
 // The correctly rounded transcendentals on device arrays (sa_math_eval):
-// f = 0 exp, 1 log, 2 sin, 3 cos, 4 sincos (y holds sin, cos pairs); exp,
+// f = 0 exp, 1 log, 2 sin, 3 cos, 4 sincos (y holds sin, cos pairs), 5
+// x^-3; exp,
 // log and sincos through the same out-of-line routines the kernels call.
 __global__ void math_eval_kernel(int f, size_t n, const double* __restrict__ x,
                                  double* __restrict__ y) {
@@ -71,6 +72,7 @@ __global__ void math_eval_kernel(int f, size_t n, const double* __restrict__ x,
             case 1: y[i] = sk::sk_log(v); break;
             case 2: y[i] = cr::sin(v); break;
             case 3: y[i] = cr::cos(v); break;
+            case 5: y[i] = cr::pow_m3(v); break;
             default: sk::sk_sincos(v, &y[2 * i], &y[2 * i + 1]); break;
         }
     }
@@ -342,7 +344,7 @@ int build_layer_const(int nz, const double* zgrid, void* out) {
 }  // namespace sa
 
 extern "C" int sa_math_eval(int f, size_t n, const double* x, double* y, void* stream) {
-    if (f < 0 || f > 4 || (n > 0 && (!x || !y))) return SA_ERR_ARG;
+    if (f < 0 || f > 5 || (n > 0 && (!x || !y))) return SA_ERR_ARG;
     if (n == 0) return SA_OK;
     const int threads = 256;
     const size_t blocks = std::min<size_t>((n + threads - 1) / threads, 148 * 16);

@@ -17,6 +17,7 @@ extern "C" void cr_eval(int f, const double* x, double* y, long n) {
             case 1: y[i] = sa::cr::log(x[i]); break;
             case 2: y[i] = sa::cr::sin(x[i]); break;
             case 3: y[i] = sa::cr::cos(x[i]); break;
+            case 5: y[i] = sa::cr::pow_m3(x[i]); break;
             default: {
                 double s, c;
                 sa::cr::sincos(x[i], &s, &c);
@@ -43,7 +44,12 @@ extern "C" void cr_check(int f, double lo, double hi, int logu, long n, unsigned
             case 0: y = sa::cr::exp(x); q = (double)expq((__float128)x); l = std::exp(x); break;
             case 1: y = sa::cr::log(x); q = (double)logq((__float128)x); l = std::log(x); break;
             case 2: y = sa::cr::sin(x); q = (double)sinq((__float128)x); l = std::sin(x); break;
-            default: y = sa::cr::cos(x); q = (double)cosq((__float128)x); l = std::cos(x); break;
+            case 3: y = sa::cr::cos(x); q = (double)cosq((__float128)x); l = std::cos(x); break;
+            default:
+                y = sa::cr::pow_m3(x);
+                q = (double)powq((__float128)x, -3);
+                l = std::pow(x, -3.0);
+                break;
         }
         if (y != q) a++;
         if (y != l) b++;

@@ -19,11 +19,12 @@ OUT = os.path.join(HERE, "_build", "libcrmath_check.so")
 
 # (function, lo, hi, log-uniform): var / dltar4 / up take sin, cos of layer
 # phases (0-40 rad), exp of -2p, -exa (-60..0) and of propagator exponents;
-# normc takes log of positive maxima
+# normc takes log of positive maxima; x^-3 (f = 5) of phase velocities
 RANGES = [(0, -60.0, 30.0, 0), (0, -700.0, 700.0, 0), (0, -1e-6, 1e-6, 0),
           (1, 1e-300, 1e300, 1), (1, 0.5, 2.0, 0), (1, 0.999, 1.001, 0),
           (2, -40.0, 40.0, 0), (2, -1e5, 1e5, 0), (2, 1e-9, 1.0, 1),
-          (3, -40.0, 40.0, 0), (3, -1e5, 1e5, 0), (3, 1e-9, 1.0, 1)]
+          (3, -40.0, 40.0, 0), (3, -1e5, 1e5, 0), (3, 1e-9, 1.0, 1),
+          (5, 0.5, 10.0, 0), (5, 1e-30, 1e30, 1)]
 
 
 def _lib():
@@ -77,7 +78,7 @@ def test_special_values():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("f", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("f", [0, 1, 2, 3, 4, 5])
 def test_device_matches_host_bits(gpu, f):
     import torch
     from surfattpp_b200 import _capi
@@ -85,6 +86,8 @@ def test_device_matches_host_bits(gpu, f):
     n = 1 << 20
     if f == 1:
         x = np.exp(rng.uniform(-700, 700, n))
+    elif f == 5:
+        x = rng.uniform(0.5, 10.0, n)
     else:
         x = rng.uniform(-60, 40, n) if f == 0 else rng.uniform(-50, 50, n)
     want = host_eval(f, x)

@@ -262,14 +262,16 @@ def test_c3_full_size_fp32_against_fp64(gpu):
 def test_deterministic_adj_s_is_the_reference_sum(c1, gpu, orc, chunk_events):
     """sa_plan_set_deterministic: adj_s and chi summed in event order.  FP64:
     bit-identical to the oracle's single-thread event loop (the reference on
-    one MPI rank); a second evaluation, and a run in chunks of 37 events,
-    give the same bits."""
+    one MPI rank) evaluated with the device's correctly rounded svel^-3 (the
+    C library's pow(svel, -3) misrounds about 0.08 % of its arguments, where
+    the C-library oracle's terms differ by one ulp: 1e-12 there); a second
+    evaluation, and a run in chunks of 37 events, give the same bits."""
     import torch
     from surfattpp_b200 import preproc
     w, svel0, ev, ref = c1
     m11, m12, m22 = w.media()
     ref1 = orc.forward_for_events(w.xx_deg, w.yy_deg, svel0, m11, m12, m22, ev, calc_adj=True,
-                                  nthreads=1)
+                                  nthreads=1, math="cr")
     plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
                                       ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
                                       ev["stla"], precision="fp64")
@@ -286,6 +288,8 @@ def test_deterministic_adj_s_is_the_reference_sum(c1, gpu, orc, chunk_events):
     for adj, chi in outs:
         assert np.array_equal(adj, ref1["adj_s"])
         assert chi == ref1["chi"]
+    scale = np.abs(ref["adj_s"]).max()
+    assert np.abs(outs[0][0] - ref["adj_s"]).max() <= 1e-12 * scale
     # FP32 plan: reproducible run to run
     p32 = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
