@@ -102,6 +102,12 @@ int sa_plan_set_graph(sa_plan* plan, int enable);
  * memory). */
 int sa_plan_set_deterministic(sa_plan* plan, int enable, size_t max_bytes);
 
+/* is_kden on a plan: while kden_s (device, [nper][ny][nx]) is set, every
+ * evaluation with the adjoint also solves the kernel-density adjoint
+ * (src/preproc.cpp:128-137) and overwrites kden_s with its accumulation
+ * (accumulate_kernels, :32-34).  NULL turns it off. */
+int sa_plan_kden_output(sa_plan* plan, double* kden_s);
+
 /* One forward (+ adjoint) evaluation of every event of the plan: replaces
  * preproc::forward_for_event (reference include/preproc.h:14,
  * src/preproc.cpp:71-148) with accumulate_kernels (:19-34), isotropic
@@ -375,6 +381,25 @@ void sa_grad_destroy(sa_grad* grad);
  * weighted sums over one handle per data type (weights of the reference's
  * data section). */
 int sa_grad_set_data_type(sa_grad* grad, int igr);
+
+/* Kernel-density preconditioning (the reference's is_kden, postproc
+ * kdensity_coe != 0).  Enabled, every sa_grad_run also solves, per event, the
+ * kernel-density adjoint (src/preproc.cpp:128-137: source -w at every
+ * receiver; the reference masks adj_field a second time rather than this
+ * field, so it is accumulated unmasked) into kden_s; sa_grad_ker_den
+ * combines it with the run's depth kernels into ker_den (nx, ny, nz)
+ * (src/preproc.cpp:294-300), and sa_kernel_precondition applies
+ * postproc::kernel_precondition (src/postproc.cpp:487-517) to a kernel.
+ * The plan accumulates into this handle's buffer while enabled
+ * (sa_plan_kden_output); one handle per plan may enable it. */
+int sa_grad_set_kden(sa_grad* grad, int enable);
+int sa_grad_ker_den(sa_grad* grad, const double* vs3d, const double* vp3d, double* ker_den,
+                    void* stream);
+/* ker[n] *= 1 / (ker_den / max|ker_den|) where that ratio exceeds 1e-12
+ * (VERYTINY), unchanged elsewhere; nothing if max|ker_den| < 1e-12.  Device
+ * arrays, enqueued on `stream` (NULL = the context's stream). */
+int sa_kernel_precondition(sa_ctx* ctx, size_t n, const double* ker_den, double* ker,
+                           void* stream);
 
 /* Device arrays: vs3d, vp3d (NULL = Brocher vs2vp(vs3d), as the model keeps it
  * for vs-only inversions), ker_vs: (nx, ny, nz) row-major; tt_obs, weight:

@@ -60,7 +60,9 @@ void orc_interp2d(int nx, int ny, const double* xgrid, const double* ygrid,
  * is ACCUMULATED (caller zeroes it) and the misfit is returned in *chi.
  * fwd_iters/adj_iters (may be NULL) receive per-event iteration counts.
  * nthreads > 1 deals events round-robin over threads (reference
- * include/parallel.h:39-41) and sums per-thread accumulators in thread order. */
+ * include/parallel.h:39-41) and sums per-thread accumulators in thread order.
+ * kden_s (may be NULL; is_kden) [nper][ny][nx] ACCUMULATES the
+ * kernel-density adjoint (src/preproc.cpp:128-137). */
 int orc_forward_for_events(int nx, int ny, int nper, const double* xx_deg,
                            const double* yy_deg, const double* svel,
                            const double* m11, const double* m12, const double* m22,
@@ -69,7 +71,10 @@ int orc_forward_for_events(int nx, int ny, int nper, const double* xx_deg,
                            const double* stlo, const double* stla,
                            const double* tt_obs, const double* weight,
                            int calc_adj, double* syn, double* adj_s, double* chi,
-                           int* fwd_iters, int* adj_iters, int nthreads);
+                           int* fwd_iters, int* adj_iters, int nthreads, double* kden_s);
+
+/* postproc::kernel_precondition (src/postproc.cpp:487-517), in place on ker[n]. */
+void orc_kernel_precondition(size_t n, const double* ker_den, double* ker);
 
 /* preproc::combine_kernels, vs-only branch (src/preproc.cpp:276-304).
  *   adj_s [nper][ny][nx]; vs3d, vp3d (nx, ny, nz) row-major;

@@ -61,9 +61,8 @@ def lib(math: str = "libc"):
     if math == "native":
         if _lib_native is None:
             path = _native_path()
-            if not os.path.exists(path):
-                subprocess.run(["make", "-s", "-C", _HERE, "native", f"NATIVE_OUT={path}"],
-                               check=True)
+            # make rebuilds it when a source is newer
+            subprocess.run(["make", "-s", "-C", _HERE, f"NATIVE_OUT={path}", path], check=True)
             _lib_native = _declare(C.CDLL(path))
         return _lib_native
     if math == "cr":
@@ -91,7 +90,8 @@ def _declare(L):
     L.orc_interp2d.argtypes = [i, i, _dp, _dp, _dp, i, _dp, _dp, _dp]
     L.orc_forward_for_events.argtypes = [i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _dp, _dp,
                                          _ip, _ip, _ip, _dp, _dp, _dp, _dp, i, _dp, _dp,
-                                         C.POINTER(d), _ip, _ip, i]
+                                         C.POINTER(d), _ip, _ip, i, C.c_void_p]
+    L.orc_kernel_precondition.argtypes = [C.c_size_t, _dp, _dp]
     L.orc_combine_kernels_vs.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
     for f in ("orc_vs2vp", "orc_vp2rho", "orc_dalpha_dbeta", "orc_drho_dalpha"):
         getattr(L, f).argtypes = [d]
@@ -171,13 +171,14 @@ def interp2d(xgrid, ygrid, z, xq, yq):
 
 
 def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, nthreads=1,
-                       math="libc"):
+                       math="libc", kden=False):
     """preproc::forward_for_event over an event set.
 
     svel/m11/m12/m22: (nper, ny, nx).  ``ev`` is a dict with evlo, evla, iper,
     rec_ptr, rec_idx, stlo, stla, tt_obs, weight (see tests/workloads.py).
-    math: which build runs it (see lib()).
-    Returns dict(syn, adj_s, chi, fwd_iters, adj_iters).
+    math: which build runs it (see lib()).  kden: also the kernel-density
+    adjoint (is_kden, src/preproc.cpp:128-137), returned as kden_s.
+    Returns dict(syn, adj_s, chi, fwd_iters, adj_iters[, kden_s]).
     """
     xx, yy = _c(xx_deg), _c(yy_deg)
     nper, ny, nx = svel.shape
@@ -185,6 +186,7 @@ def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, n
     nrec = int(ev["rec_ptr"][-1])
     syn = np.zeros(max(nrec, 1))
     adj_s = np.zeros((nper, ny, nx))
+    kden_s = np.zeros((nper, ny, nx)) if kden else None
     chi = C.c_double(0.0)
     fi = np.zeros(max(ne, 1), np.int32)
     ai = np.zeros(max(ne, 1), np.int32)
@@ -192,8 +194,19 @@ def forward_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, calc_adj=True, n
         nx, ny, nper, xx, yy, _c(svel), _c(m11), _c(m12), _c(m22), ne,
         _c(ev["evlo"]), _c(ev["evla"]), _c(ev["iper"], np.int32), _c(ev["rec_ptr"], np.int32),
         _c(ev["rec_idx"], np.int32), _c(ev["stlo"]), _c(ev["stla"]), _c(ev["tt_obs"]),
-        _c(ev["weight"]), int(calc_adj), syn, adj_s, C.byref(chi), fi, ai, int(nthreads))
-    return dict(syn=syn[:nrec], adj_s=adj_s, chi=chi.value, fwd_iters=fi[:ne], adj_iters=ai[:ne])
+        _c(ev["weight"]), int(calc_adj), syn, adj_s, C.byref(chi), fi, ai, int(nthreads),
+        kden_s.ctypes.data if kden_s is not None else None)
+    out = dict(syn=syn[:nrec], adj_s=adj_s, chi=chi.value, fwd_iters=fi[:ne], adj_iters=ai[:ne])
+    if kden_s is not None:
+        out["kden_s"] = kden_s
+    return out
+
+
+def kernel_precondition(ker_den, ker):
+    """postproc::kernel_precondition: a preconditioned copy of ker."""
+    out = _c(ker).copy()
+    lib().orc_kernel_precondition(out.size, _c(ker_den), out)
+    return out
 
 
 def combine_kernels_vs(adj_s, vs3d, vp3d, sen_vs, sen_vp, sen_rho):

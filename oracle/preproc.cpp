@@ -3,6 +3,7 @@
 #include "oracle.h"
 #include "omath.h"
 
+#include <algorithm>
 #include <cmath>
 #include <thread>
 #include <vector>
@@ -37,11 +38,15 @@ struct EventRange {
     int calc_adj;
     double* syn;
     int *fwd_iters, *adj_iters;
+    bool kden;    // is_kden: the kernel-density adjoint as well
 };
 
 // One event of preproc::forward_for_event (src/preproc.cpp:79-143) plus
 // accumulate_kernels (src/preproc.cpp:19-34).  Returns 0.5*sum(w r^2).
-double run_event(const EventRange& R, int ie, double* adj_acc) {
+// With R.kden, the kernel-density adjoint (:128-137): source -w at every
+// receiver, the field NOT masked (the reference masks adj_field a second
+// time instead), accumulated into kden_acc with svel^-3.
+double run_event(const EventRange& R, int ie, double* adj_acc, double* kden_acc) {
     const int nx = R.nx, ny = R.ny, n = nx * ny;
     const int ip = R.iper[ie];
     const double* svel = R.svel + static_cast<size_t>(ip) * n;
@@ -76,6 +81,14 @@ double run_event(const EventRange& R, int ie, double* adj_acc) {
     orc_mask_uniform_grid(nx, ny, R.xx_deg, R.yy_deg, Ta.data(), R.evlo[ie], R.evla[ie]);
     double* acc = adj_acc + static_cast<size_t>(ip) * n;
     for (int k = 0; k < n; k++) acc[k] += Ta[k] * om::pow_m3(svel[k]);   // pow(svel, -3)
+    if (R.kden && kden_acc) {
+        std::vector<double> sk(nr), Tk(n);
+        for (int i = 0; i < nr; i++) sk[i] = -R.weight[r0 + i] * 1.0;
+        orc_eik_adj(nx, ny, R.xx_deg, R.yy_deg, m11, m22, sphc.data(), T.data(), nr, xr.data(),
+                    yr.data(), sk.data(), Tk.data(), &it);
+        double* kacc = kden_acc + static_cast<size_t>(ip) * n;
+        for (int k = 0; k < n; k++) kacc[k] += Tk[k] * om::pow_m3(svel[k]);
+    }
     double s = 0.0;
     for (int i = 0; i < nr; i++) {
         const double r = ttsyn[i] - R.tt_obs[r0 + i];
@@ -94,28 +107,31 @@ extern "C" int orc_forward_for_events(int nx, int ny, int nper, const double* xx
                                       const double* stlo, const double* stla,
                                       const double* tt_obs, const double* weight,
                                       int calc_adj, double* syn, double* adj_s, double* chi,
-                                      int* fwd_iters, int* adj_iters, int nthreads) {
+                                      int* fwd_iters, int* adj_iters, int nthreads,
+                                      double* kden_s) {
     EventRange R{nx, ny, nper, xx_deg, yy_deg, svel, m11, m12, m22, evlo, evla, iper,
                  rec_ptr, rec_idx, stlo, stla, tt_obs, weight, calc_adj, syn,
-                 fwd_iters, adj_iters};
+                 fwd_iters, adj_iters, kden_s != nullptr};
     const size_t plane = static_cast<size_t>(nx) * ny * nper;
     if (nthreads <= 1) {
         double c = 0.0;
-        for (int ie = 0; ie < ne; ie++) c += run_event(R, ie, adj_s);
+        for (int ie = 0; ie < ne; ie++) c += run_event(R, ie, adj_s, kden_s);
         if (chi) *chi = c;
         return 0;
     }
     // Round-robin event ownership, one private accumulator per worker, summed
     // in worker order afterwards (the allreduce of src/preproc.cpp:146, :238).
-    std::vector<std::vector<double>> acc(nthreads);
+    std::vector<std::vector<double>> acc(nthreads), kacc(nthreads);
     std::vector<double> chis(nthreads, 0.0);
     std::vector<std::thread> pool;
     for (int t = 0; t < nthreads; t++) {
         pool.emplace_back([&, t]() {
             if (calc_adj) acc[t].assign(plane, 0.0);
+            if (calc_adj && kden_s) kacc[t].assign(plane, 0.0);
             double c = 0.0;
             for (int ie = t; ie < ne; ie += nthreads)
-                c += run_event(R, ie, calc_adj ? acc[t].data() : nullptr);
+                c += run_event(R, ie, calc_adj ? acc[t].data() : nullptr,
+                               calc_adj && kden_s ? kacc[t].data() : nullptr);
             chis[t] = c;
         });
     }
@@ -125,9 +141,26 @@ extern "C" int orc_forward_for_events(int nx, int ny, int nper, const double* xx
         c += chis[t];
         if (calc_adj)
             for (size_t k = 0; k < plane; k++) adj_s[k] += acc[t][k];
+        if (calc_adj && kden_s)
+            for (size_t k = 0; k < plane; k++) kden_s[k] += kacc[t][k];
     }
     if (chi) *chi = c;
     return 0;
+}
+
+// postproc::kernel_precondition (src/postproc.cpp:487-517): with the kernel
+// density normalised by its largest magnitude, ker *= 1/norm where norm >
+// VERYTINY (1e-12, include/config.h:71), unchanged elsewhere; nothing when
+// the density itself is below VERYTINY.
+extern "C" void orc_kernel_precondition(size_t n, const double* ker_den, double* ker) {
+    double L_inf = 0.0;
+    for (size_t i = 0; i < n; i++) L_inf = std::max(L_inf, std::abs(ker_den[i]));
+    if (L_inf < 1e-12) return;
+    for (size_t i = 0; i < n; i++) {
+        const double norm = ker_den[i] / L_inf;
+        const double h = norm > 1e-12 ? 1.0 / norm : 1.0;
+        ker[i] = ker[i] * h;
+    }
 }
 
 // src/preproc.cpp:276-304 (vs-only parametrisation, is_kden = false).

@@ -270,7 +270,17 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
             __syncwarp();
         }
 
-        if (B.mode != MODE_FWD) {
+        // pass 0: the adjoint of the residuals (or the given source); pass 1
+        // (is_kden): the kernel-density adjoint, source -w at every receiver,
+        // not masked and accumulated into kden_s (src/preproc.cpp:128-137)
+        const int npass = (B.mode == MODE_FWD) ? 0
+                          : (B.mode == MODE_FWD_ADJ && B.out.kden_s && !B.ev.sadj) ? 2
+                                                                                   : 1;
+        for (int pass = 0; pass < npass; pass++) {
+            if (pass == 1) {
+                for (int ir = lane; ir < nr; ir += 32) P_sadj[ir] = -B.ev.weight[r0 + ir] * 1.0;
+                __syncwarp();
+            }
             // adjoint source (src/eikonal_solver.cpp:354-375), receivers in order
             if (lane == 0) spread_delta(g, B.ev, r0, nr, P_sadj, P_delta, false);
             __syncwarp();
@@ -434,11 +444,20 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
                         if (Linf <= 4.0 * 5.960464477539063e-08 * vmax) break;
                     }
             }
-            if (lane == 0 && B.out.adj_iters) B.out.adj_iters[e] = iters;
+            if (lane == 0 && B.out.adj_iters && pass == 0) B.out.adj_iters[e] = iters;
             if (lane == 0) spread_delta(g, B.ev, r0, nr, P_sadj, P_delta, true);
             bool finite = true;
             const S* TaS = reinterpret_cast<const S*>(base + L.Ta);
-            if (B.mode == MODE_ADJ_ONLY) {
+            if (pass == 1) {
+                const double* inv3 = B.inv3 + (size_t)ip * n;
+                double* acc = B.out.kden_s + (size_t)ip * n;
+                for (size_t k = lane; k < n; k += 32) {
+                    const double v = (double)TaS[k];
+                    if (!isfinite(v)) finite = false;
+                    const double c = v * inv3[k];
+                    if (c != 0.0) atomicAdd(acc + k, c);
+                }
+            } else if (B.mode == MODE_ADJ_ONLY) {
                 for (size_t k = lane; k < n; k += 32) {
                     const double v = (double)TaS[k];
                     if (!isfinite(v)) finite = false;
@@ -464,6 +483,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
                 }
             }
             if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;
+            __syncwarp();
         }
         if (lane == 0 && B.out.status) B.out.status[e] = status;
         __syncwarp();

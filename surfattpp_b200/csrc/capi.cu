@@ -142,6 +142,7 @@ struct sa_plan {
     DArr<int> iota, per_ptr, per_ev;
     double* dbg_T = nullptr;
     double* dbg_Ta = nullptr;
+    double* kden_out = nullptr;   // is_kden accumulation target (sa_plan_kden_output)
     bool use_graph = true;
     bool have_graph = false;
     GraphKey key{};
@@ -494,10 +495,14 @@ int plan_enqueue(sa_plan* P, const double* svel, const double* m11, const double
     d.out.status = status ? status : P->status_tmp.p;
     d.out.T_out = P->dbg_T;
     d.out.Ta_out = P->dbg_Ta;
+    d.out.kden_s = (calc_adj && !sadj) ? P->kden_out : nullptr;
     d.mode = calc_adj ? MODE_FWD_ADJ : MODE_FWD;
     SA_CUDA(cudaMemsetAsync(P->queue.p, 0, sizeof(unsigned int), st));
     if (calc_adj && adj_s)
         SA_CUDA(cudaMemsetAsync(adj_s, 0, (size_t)P->nx * P->ny * P->nper * sizeof(double), st));
+    if (d.out.kden_s)
+        SA_CUDA(cudaMemsetAsync(d.out.kden_s, 0,
+                                (size_t)P->nx * P->ny * P->nper * sizeof(double), st));
     const bool determ = P->determ && calc_adj && adj_s && P->ne > 0;
     if (P->ne > 0) {
         if (P->timing) SA_CUDA(cudaEventRecord(P->tk0, st));
@@ -663,6 +668,12 @@ extern "C" int sa_plan_get_tune(sa_plan* P, int* variant, int* active_slots, int
     return SA_OK;
 }
 
+extern "C" int sa_plan_kden_output(sa_plan* P, double* kden_s) {
+    if (!P) return SA_ERR_ARG;
+    P->kden_out = kden_s;
+    return SA_OK;
+}
+
 extern "C" int sa_plan_set_deterministic(sa_plan* P, int enable, size_t max_bytes) {
     if (!P) return SA_ERR_ARG;
     sa_ctx* ctx = P->ctx;
@@ -760,7 +771,7 @@ int plan_run(sa_plan* P, const double* svel, const double* m11, const double* m1
                             fwd_iters, adj_iters, status, st, sadj);
     GraphKey k{};
     const void* ptrs[17] = {svel, m11, m12, m22, tt_obs, weight, syn, adj_s, chi, fwd_iters,
-                            adj_iters, status, P->dbg_T, P->dbg_Ta, sadj, nullptr, nullptr};
+                            adj_iters, status, P->dbg_T, P->dbg_Ta, sadj, P->kden_out, nullptr};
     std::memcpy(k.ptr, ptrs, sizeof(ptrs));
     k.calc_adj = calc_adj;
     if (!(P->have_graph && P->key == k)) {
@@ -1138,6 +1149,8 @@ struct sa_grad {
     // sregnpu; colst then holds 4 status planes (group, 3 phase runs)
     int igr = 0;
     DArr<double> per3, cps3;
+    bool kden = false;       // is_kden (sa_grad_set_kden): kden_s accumulated per run
+    DArr<double> kden_s;
     cudaStream_t side = nullptr;
     cudaEvent_t e_disp = nullptr, e_sen = nullptr;
     ~sa_grad() {
@@ -1260,6 +1273,32 @@ extern "C" int sa_grad_set_data_type(sa_grad* g, int igr) {
         SA_CUDA(cudaStreamSynchronize(ctx->stream));
     }
     g->igr = igr;
+    return SA_OK;
+}
+
+extern "C" int sa_grad_set_kden(sa_grad* g, int enable) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    if (enable) SA_CUDA(g->kden_s.alloc((size_t)P->nx * P->ny * P->nper));
+    g->kden = enable != 0;
+    return sa_plan_kden_output(P, g->kden ? g->kden_s.p : nullptr);
+}
+
+extern "C" int sa_grad_ker_den(sa_grad* g, const double* vs3d, const double* vp3d,
+                               double* ker_den, void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (!g->kden) return fail(ctx, SA_ERR_ARG, "kernel density not enabled (sa_grad_set_kden)");
+    if (!vs3d || !ker_den) return fail(ctx, SA_ERR_ARG, "vs3d and ker_den are required");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    SA_CUDA(cudaStreamWaitEvent(st, g->e_sen, 0));
+    // preproc::combine_kernels' ker_den (src/preproc.cpp:294-300)
+    SA_CUDA(launch_combine_vs(P->nx, P->ny, g->nz, P->nper, g->kden_s.p, vs3d, vp3d,
+                              g->sen_vs.p, g->sen_vp.p, g->sen_rho.p, ker_den, st));
     return SA_OK;
 }
 
@@ -1613,6 +1652,18 @@ extern "C" int sa_dot(sa_ctx* ctx, size_t n, const double* a, const double* b, d
     double* red = ctx_red(ctx, &rc);
     if (rc) return rc;
     return reduce_to_host(ctx, launch_dot(n, a, b, red, ctx->stream), red, out, ctx->stream);
+}
+
+extern "C" int sa_kernel_precondition(sa_ctx* ctx, size_t n, const double* ker_den, double* ker,
+                                      void* stream) {
+    if (!ctx || !ker_den || !ker) return SA_ERR_ARG;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    double* red = ctx_red(ctx, &rc);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    SA_CUDA(launch_kernel_precondition(n, ker_den, red, ker, st));
+    return SA_OK;
 }
 
 extern "C" int sa_grad_normalization(sa_ctx* ctx, size_t n, double* g, double* max_out) {

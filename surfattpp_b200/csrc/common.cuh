@@ -93,6 +93,8 @@ struct Outputs {
     // and an ordered reduction sums them in event order (may be null)
     double* contrib;
     int contrib_e0;
+    // is_kden: [nper][ny][nx] accumulated kernel-density adjoint (may be null)
+    double* kden_s;
 };
 
 enum Mode : int { MODE_FWD = 0, MODE_FWD_ADJ = 1, MODE_ADJ_ONLY = 2 };

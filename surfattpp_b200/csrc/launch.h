@@ -105,6 +105,9 @@ size_t reduce_scratch_doubles();
 cudaError_t launch_dot(size_t n, const double* a, const double* b, double* scratch,
                        cudaStream_t st);
 cudaError_t launch_absmax(size_t n, const double* a, double* scratch, cudaStream_t st);
+// postproc::kernel_precondition of ker by ker_den (scratch: reduction scratch)
+cudaError_t launch_kernel_precondition(size_t n, const double* ker_den, double* scratch,
+                                       double* ker, cudaStream_t st);
 cudaError_t launch_lbfgs_pair(size_t n, const double* m0, const double* m1, const double* g0,
                               const double* g1, double* s, double* y, cudaStream_t st);
 cudaError_t launch_axpy(size_t n, int kind, double c, const double* x, double* y,

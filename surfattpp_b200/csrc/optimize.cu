@@ -97,8 +97,32 @@ __global__ void model_update_kernel(size_t n, const double* __restrict__ vs,
     }
 }
 
+// postproc::kernel_precondition (src/postproc.cpp:487-517): with L = max
+// |ker_den| (linf[0], from launch_absmax), ker *= 1 / (ker_den / L) where
+// ker_den / L > VERYTINY (include/config.h:71), and nothing when L < VERYTINY.
+__global__ void precondition_kernel(size_t n, const double* __restrict__ ker_den,
+                                    const double* __restrict__ linf, double* ker) {
+    const double L = *linf;
+    if (L < 1e-12) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double norm = ker_den[i] / L;
+        const double h = norm > 1e-12 ? 1.0 / norm : 1.0;
+        ker[i] = ker[i] * h;
+    }
+}
+
 unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
 }  // namespace
+
+cudaError_t launch_kernel_precondition(size_t n, const double* ker_den, double* scratch,
+                                       double* ker, cudaStream_t st) {
+    cudaError_t e = launch_absmax(n, ker_den, scratch, st);
+    if (e != cudaSuccess) return e;
+    precondition_kernel<<<grid_for(n), 256, 0, st>>>(n, ker_den,
+                                                    scratch + reduce_scratch_doubles() - 1, ker);
+    return cudaGetLastError();
+}
 
 size_t reduce_scratch_doubles() { return RED_BLOCKS + 1; }
 

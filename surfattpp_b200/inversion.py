@@ -62,6 +62,12 @@ class MisfitGradient:
         if igr:
             _capi.check(plan.ctx.h, _capi.lib().sa_grad_set_data_type(self.h, igr))
 
+    def set_kden(self, enable=True):
+        """is_kden: every run also returns ker_den, the kernel density
+        (sa_grad_set_kden / sa_grad_ker_den)."""
+        _capi.check(self.plan.ctx.h, _capi.lib().sa_grad_set_kden(self.h, int(bool(enable))))
+        self.kden = bool(enable)
+
     def close(self):
         if getattr(self, "h", None):
             _capi.lib().sa_grad_destroy(self.h)
@@ -108,6 +114,13 @@ class MisfitGradient:
         if multi:
             distributed.reduce_gradient(out["adj_s"], out["chi"], out["status"], group)
             self.combine(vs3d, out["adj_s"], vp3d, out["ker_vs"], stream)
+        if getattr(self, "kden", False):
+            if multi:
+                raise NotImplementedError("kernel density with more than one rank")
+            out.setdefault("ker_den", torch.empty((p.nx, p.ny, self.nz), **f64))
+            rc = _capi.lib().sa_grad_ker_den(self.h, ptr(vs3d), ptr(vp3d), ptr(out["ker_den"]),
+                                             stream)
+            _capi.check(p.ctx.h, rc)
         return out
 
     def combine(self, vs3d, adj_s, vp3d=None, ker_vs=None, stream=None):
@@ -258,8 +271,8 @@ class Inversion:
     and restarts (src/inversion.cpp:396-463, src/optimize.cpp), and the
     multiplicative model update vs *= (1 - alpha*dir) with Brocher vp, rho.
     The model and gradient history the reference writes to HDF5 stays on the
-    device (optimize.LBFGS).  Kernel-density preconditioning (is_kden) is not
-    applied.
+    device (optimize.LBFGS).  Kernel-density preconditioning (is_kden) is
+    applied when asked for.
     """
 
     BREAK_ITER = 5          # include/config.h:94
@@ -268,12 +281,15 @@ class Inversion:
     def __init__(self, grad: MisfitGradient, tt_obs, weight, smooth=None, niter=10,
                  optim="lbfgs", step_length=0.02, max_sub_niter=10, c1=0.1, c2=0.9,
                  maxshrink=0.8, min_derr=0.0, data_weight=1.0, autograd=False,
-                 more_data=None):
+                 more_data=None, kden=False):
         """smooth = dict(ygrid, zgrid, dx, dy, dz, sigma_h, sigma_v) or None.
         more_data: further data types as (MisfitGradient, tt_obs, weight,
         data_weight) tuples, e.g. group-velocity data next to phase data; the
         misfit, kernel and gradient are summed over the types as
         src/inversion.cpp:250-296 does.
+        kden: kernel-density preconditioning of every type's kernel before
+        the smoothing (postproc::kernel_precondition, src/postproc.cpp:
+        487-517; the reference's is_kden).
         autograd: take the kernel as the torch.autograd gradient of chi built
         in torch on TravelTimes (forward: receiver times, nothing stored;
         backward: every forward field recomputed, the adjoint driven by
@@ -288,6 +304,12 @@ class Inversion:
         self.data = [(grad, tt_obs, weight, data_weight)] + list(more_data or [])
         self._outs = [None] * len(self.data)
         self.autograd = bool(autograd)
+        self.kden = bool(kden)
+        if self.kden:
+            if self.autograd:
+                raise ValueError("kden preconditioning runs on the fused evaluation")
+            for g, *_ in self.data:
+                g.set_kden(True)
         self.misfit, self.alphas, self.sub_iters, self.restarts = [], [], [], 0
         self._out = None
 
@@ -315,6 +337,8 @@ class Inversion:
                 raise _capi.SAError(int(out["status"][0]), "forward/adjoint evaluation failed")
             chi = float(out["chi"][0])
             sm = ker.clone()
+            if self.kden:
+                postproc.kernel_precondition(out["ker_den"], sm)
             if self.smooth is not None:
                 s = self.smooth
                 postproc.pde_smooth(sm, s["ygrid"], s["zgrid"], s["dx"], s["dy"], s["dz"],

@@ -4,7 +4,8 @@
 rank: nstep explicit Euler steps of the spherical 7-point Laplacian with
 Neumann boundary copies, over a (nx, ny, nz) row-major field (depth fastest,
 as Tensor3r).  ``kernel_smooth`` applies it to each kernel of a list
-(postproc::kernel_smooth, :519-534).  Device memory is held in torch tensors;
+(postproc::kernel_smooth, :519-534); ``kernel_precondition`` the kernel-density
+preconditioning (:487-517).  Device memory is held in torch tensors;
 the arithmetic runs in libsurfatt_gpu.so.
 """
 from __future__ import annotations
@@ -59,3 +60,14 @@ def kernel_smooth(kernels, ygrid, zgrid, dx_deg, dy_deg, dz_km, sigma_h, sigma_v
         pde_smooth(s, ygrid, zgrid, dx_deg, dy_deg, dz_km, sigma_h, sigma_v, work=work, ctx=ctx)
         out.append(s)
     return out
+
+
+def kernel_precondition(ker_den, ker, ctx=None, stream=None):
+    """postproc::kernel_precondition (src/postproc.cpp:487-517), in place on
+    the device tensor ker: ker *= 1 / (ker_den / max|ker_den|) where that
+    ratio exceeds 1e-12, unchanged elsewhere, nothing if max|ker_den| <
+    1e-12 (sa_kernel_precondition)."""
+    ctx = ctx or default_context()
+    rc = _capi.lib().sa_kernel_precondition(ctx.h, ker.numel(), ptr(ker_den), ptr(ker), stream)
+    _capi.check(ctx.h, rc)
+    return ker

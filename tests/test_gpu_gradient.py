@@ -209,3 +209,45 @@ def test_joint_phase_and_group_gradient(c2, gpu, orc):
         gref = wph * kph / ref["chi"] + wgr * kgr / ref_gr["chi"]
         assert np.abs(kc - kref).max() <= tol * np.abs(kref).max()
         assert np.abs(gr - gref).max() <= tol * np.abs(gref).max()
+
+
+def test_kernel_density_preconditioning(c2, gpu, orc):
+    """is_kden (src/preproc.cpp:128-137, :294-300; src/postproc.cpp:487-517):
+    the kernel-density adjoint (source -w, accumulated unmasked), its
+    combination into ker_den and the preconditioning, FP64, against the
+    oracle: kden_s and ker_den 1e-11 of their maxima (FP64 atomics in
+    completion order), the preconditioning of identical inputs bit for bit,
+    and the preconditioned gradient of one inversion step 1e-9 of its
+    maximum."""
+    import torch
+    from surfattpp_b200 import inversion, postproc
+    w, ev, vs0, ref = c2
+    m11, m12, m22 = w.media()
+    sv0 = ref["svel"]
+    rk = orc.forward_for_events(w.xx_deg, w.yy_deg, sv0, m11, m12, m22, ev, calc_adj=True,
+                                nthreads=8, kden=True)
+    assert np.array_equal(rk["adj_s"], ref["adj_s"])   # the kden pass leaves adj_s alone
+    sen = orc.depthkernel_hti(w.zgrid, vs0, w.periods, nthreads=8)
+    vp0 = np.vectorize(orc.vs2vp)(vs0)
+    kden_ref = orc.combine_kernels_vs(rk["kden_s"], vs0, vp0, *sen[:3])
+    plan, g, tt, wt, t = _grad(w, ev, "fp64")
+    g.set_kden(True)
+    out = g.run(t(vs0), tt, wt)
+    torch.cuda.synchronize()
+    kd = out["ker_den"].cpu().numpy()
+    assert np.abs(kd - kden_ref).max() <= 1e-11 * np.abs(kden_ref).max()
+    # the preconditioning itself, on identical inputs (with tiny and negative
+    # densities): bit for bit
+    rng = np.random.default_rng(8)
+    dens = rng.standard_normal(5000) * np.where(rng.random(5000) < 0.1, 1e-14, 1.0)
+    ker = rng.standard_normal(5000)
+    got = postproc.kernel_precondition(t(dens), t(ker).clone())
+    torch.cuda.synchronize()
+    assert np.array_equal(got.cpu().numpy(), orc.kernel_precondition(dens, ker))
+    # one inversion step with is_kden (no smoothing)
+    inv = inversion.Inversion(g, tt, wt, smooth=None, kden=True)
+    total, ker_curr, grad = inv.run_forward_adjoint(t(vs0))
+    torch.cuda.synchronize()
+    gref = orc.kernel_precondition(kden_ref, ref["ker"]) / ref["chi"]
+    assert np.abs(grad.cpu().numpy() - gref).max() <= 1e-9 * np.abs(gref).max()
+    assert np.abs(ker_curr.cpu().numpy() - ref["ker"]).max() <= 1e-12 * np.abs(ref["ker"]).max()
