@@ -188,6 +188,35 @@ int sa_plan_kernel_ms(sa_plan* plan, float* ms);
 int sa_plan_debug_fields(sa_plan* plan, double* T_out, double* Ta_out);
 
 
+/* ---- one launch over several grids ---------------------------------------- */
+
+/* No counterpart in the reference, which solves each grid's events in its
+ * own loop.  Binds plans of one context and precision -- e.g. the levels of
+ * a multi-grid topography batch, 101^2, 201^2 and 401^2 -- so that one
+ * persistent launch solves every plan's events: each queue entry names its
+ * plan (grid, media, geometry, outputs), scratch slots are sized for the
+ * largest grid, and the queue is ordered by the previous evaluation's work
+ * (sweeps x cells) across plans, longest first.  Results equal each plan's
+ * own sa_plan_forward_adjoint (adj_s to the order of its FP64 atomics). */
+typedef struct sa_multi sa_multi;
+int sa_multi_create(sa_plan* const* plans, int nplans, sa_multi** out);
+void sa_multi_destroy(sa_multi* multi);
+
+/* One evaluation of every plan's events in one launch: the arguments of
+ * sa_plan_forward_adjoint, one pointer per plan (m11/m12/m22 NULL or set for
+ * every plan; syn, adj_s, chi, status may be NULL or hold NULL entries).
+ * The first plan's FP32 launch variant applies to all.  Enqueued on
+ * `stream` (NULL = the context's stream). */
+int sa_multi_forward_adjoint(sa_multi* multi, const double* const* svel, const double* const* m11,
+                             const double* const* m12, const double* const* m22,
+                             const double* const* tt_obs, const double* const* weight,
+                             int calc_adj, double* const* syn, double* const* adj_s,
+                             double* const* chi, int* const* status, void* stream);
+/* Device time of the last evaluation's batch launch (waits for it). */
+int sa_multi_kernel_ms(sa_multi* multi, float* ms);
+/* The worst event status of the last evaluation over all plans (synchronous). */
+int sa_multi_status(sa_multi* multi, int* worst);
+
 /* ---- surfker:: and preproc::combine_kernels (device arrays) --------------- */
 
 /* Replaces the column loop of SurfGrid::fwdsurf (reference

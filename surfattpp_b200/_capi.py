@@ -31,7 +31,8 @@ EXPORTED = (
     "sa_eik_fwd_field_noalloc", "sa_math_eval", "sa_plan_adjoint_source",
     "sa_grad_forward", "sa_grad_vjp", "sa_plan_set_deterministic",
     "sa_grad_set_data_type", "sa_plan_kden_output", "sa_grad_set_kden", "sa_grad_ker_den",
-    "sa_kernel_precondition",
+    "sa_kernel_precondition", "sa_multi_create", "sa_multi_destroy",
+    "sa_multi_forward_adjoint", "sa_multi_kernel_ms", "sa_multi_status",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen", "sa_grad_combine",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
@@ -109,6 +110,12 @@ def lib():
     L.sa_grad_set_kden.argtypes = [_vp, i]
     L.sa_grad_ker_den.argtypes = [_vp] * 4 + [_vp]
     L.sa_kernel_precondition.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
+    L.sa_multi_create.argtypes = [C.POINTER(_vp), i, C.POINTER(_vp)]
+    L.sa_multi_destroy.argtypes = [_vp]
+    L.sa_multi_forward_adjoint.argtypes = [_vp] + [C.POINTER(_vp)] * 6 + [i] + \
+        [C.POINTER(_vp)] * 4 + [_vp]
+    L.sa_multi_kernel_ms.argtypes = [_vp, C.POINTER(C.c_float)]
+    L.sa_multi_status.argtypes = [_vp, C.POINTER(i)]
     L.sa_grad_create.argtypes = [_vp, i, _dp, _dp, C.POINTER(_vp)]
     L.sa_grad_destroy.argtypes = [_vp]
     L.sa_grad_run.argtypes = [_vp] + [_vp] * 9 + [_vp]

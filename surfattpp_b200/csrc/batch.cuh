@@ -200,18 +200,20 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     return fun0_64;
 }
 
-// Body of the persistent batch kernel (below), shared with the FP64 variant
-// that reads the grid spacing from device memory (eik64.cu).
+// One event of the batch on the warp's scratch slot `base` (laid out for
+// this event's grid).  Shared by the single-grid persistent kernel and the
+// multi-grid one (one launch over plans of different grid sizes).
+// `clear_delta`: the slot last held an event of another grid size, whose
+// planes overlap this grid's adjoint-source plane, so it is zeroed first (in
+// a single-grid launch it is zero between events by construction).
 template <class S, bool ISO, int VAR>
-__device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
+__device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int e,
+                                            unsigned char* base, bool clear_delta = false) {
     const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (slot >= B.sc.nslots) return;
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
     const size_t n = (size_t)nx * ny;
     const SlotLayout L = slot_layout<S>(nx, ny, B.maxr);
-    unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
     S* P_tau = reinterpret_cast<S*>(base + L.tau);
     S* P_tst = reinterpret_cast<S*>(base + L.tst);
     double* P_T = reinterpret_cast<double*>(base + L.T);
@@ -221,11 +223,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
     Q4<S>* P_pk = reinterpret_cast<Q4<S>*>(base + L.PK);
     unsigned char* P_fl = base + L.flags;
     int2* P_rng = reinterpret_cast<int2*>(base + L.rng);
-
-    for (;;) {
-        const unsigned int qi = warp_next_event(B.sc.queue);
-        if (qi >= (unsigned)B.ev.ne) break;
-        const unsigned int e = B.sc.order ? (unsigned)B.sc.order[qi] : qi;
+    {
         const int ip = B.ev.iper[e];
         const int r0 = B.ev.rec_ptr[e];
         const int nr = B.ev.rec_ptr[e + 1] - r0;
@@ -276,6 +274,10 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
         const int npass = (B.mode == MODE_FWD) ? 0
                           : (B.mode == MODE_FWD_ADJ && B.out.kden_s && !B.ev.sadj) ? 2
                                                                                    : 1;
+        if (clear_delta && npass > 0) {
+            for (size_t k = lane; k < n; k += 32) P_delta[k] = 0.0;
+            __syncwarp();
+        }
         for (int pass = 0; pass < npass; pass++) {
             if (pass == 1) {
                 for (int ir = lane; ir < nr; ir += 32) P_sadj[ir] = -B.ev.weight[r0 + ir] * 1.0;
@@ -490,10 +492,46 @@ __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
     }
 }
 
+// Body of the persistent batch kernel (below), shared with the FP64 variant
+// that reads the grid spacing from device memory (eik64.cu): one warp per
+// scratch slot pulls events from the queue until it is empty.
+template <class S, bool ISO, int VAR>
+__device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= B.sc.nslots) return;
+    unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
+    for (;;) {
+        const unsigned int qi = warp_next_event(B.sc.queue);
+        if (qi >= (unsigned)B.ev.ne) break;
+        const unsigned int e = B.sc.order ? (unsigned)B.sc.order[qi] : qi;
+        batch_event<S, ISO, VAR>(B, e, base);
+    }
+}
+
 template <class S, bool ISO, int VAR>
 __global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? SA_MINB64 : SA_MINB32)
 batch_kernel(BatchArgs<S> B) {
     batch_body<S, ISO, VAR>(B);
+}
+
+// One persistent launch over the events of several plans (grid levels of
+// different size): queue position qi -> code[qi] = level << 24 | event, each
+// level's arguments in device memory, scratch slots sized for the largest
+// level.  `code` is ordered by work across levels, so the long solves of the
+// fine grids start first and the short ones fill the tail.
+template <class S, bool ISO, int VAR>
+__global__ void __launch_bounds__(128, sizeof(S) == sizeof(double) ? SA_MINB64 : SA_MINB32)
+batch_multi_kernel(const BatchArgs<S>* __restrict__ levels, unsigned int ntotal,
+                   const unsigned int* __restrict__ code, Scratch sc) {
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= sc.nslots) return;
+    unsigned char* base = sc.base + (size_t)slot * sc.slot_bytes;
+    for (;;) {
+        const unsigned int qi = warp_next_event(sc.queue);
+        if (qi >= ntotal) break;
+        const unsigned int c = code[qi];
+        batch_event<S, ISO, VAR>(levels[c >> 24], c & 0xffffffu, base, true);
+    }
 }
 
 template <class S>

@@ -827,6 +827,180 @@ extern "C" int sa_plan_adjoint_source(sa_plan* P, const double* svel, const doub
                     nullptr, nullptr, nullptr, status, stream);
 }
 
+// ---- one launch over several plans (grid levels) ----------------------------
+
+struct sa_multi {
+    sa_ctx* ctx = nullptr;
+    std::vector<sa_plan*> plans;
+    std::vector<int> off;          // first queue entry of each level
+    int prec = SA_FP32, ntotal = 0, nslots = 0;
+    size_t slot_bytes = 0;
+    DArr<unsigned char> args, scratch, sort_tmp;
+    DArr<unsigned int> queue, key_a, key_b;
+    DArr<int> code_in, code;
+    size_t sort_bytes = 0;
+    cudaEvent_t tk0 = nullptr, tk1 = nullptr;
+    ~sa_multi() {
+        if (tk0) cudaEventDestroy(tk0);
+        if (tk1) cudaEventDestroy(tk1);
+    }
+};
+
+extern "C" int sa_multi_create(sa_plan* const* plans, int nplans, sa_multi** out) {
+    if (!plans || nplans < 1 || nplans > 127 || !out || !plans[0]) return SA_ERR_ARG;
+    *out = nullptr;
+    sa_ctx* ctx = plans[0]->ctx;
+    SA_CUDA(cudaSetDevice(ctx->device));
+    sa_multi* M = new sa_multi();
+    M->ctx = ctx;
+    M->prec = plans[0]->prec;
+    const int maxs =
+        M->prec == SA_FP64 ? batch64_max_slots(ctx->device) : batch32_max_slots(ctx->device);
+    for (int i = 0; i < nplans; i++) {
+        sa_plan* P = plans[i];
+        if (!P || P->ctx != ctx || P->prec != M->prec || P->ne >= (1 << 24)) {
+            delete M;
+            return fail(ctx, SA_ERR_ARG, "sa_multi_create: plans of one context and precision, "
+                                         "fewer than 2^24 events each");
+        }
+        M->plans.push_back(P);
+        M->off.push_back(M->ntotal);
+        M->ntotal += P->ne;
+        M->slot_bytes = std::max(M->slot_bytes, P->slot_bytes);
+    }
+    const size_t nt = (size_t)std::max(M->ntotal, 1);
+    size_t fr = 0, tot = 0;
+    cudaError_t e = cudaMemGetInfo(&fr, &tot);
+    int ns = std::min(maxs, std::max(M->ntotal, 1));
+    while (ns > 1 && (size_t)ns * M->slot_bytes > fr / 10 * 7) ns--;
+    M->nslots = ns;
+    std::vector<int> code(nt, 0);
+    for (int i = 0; i < nplans; i++)
+        for (int k = 0; k < plans[i]->ne; k++) code[M->off[i] + k] = (i << 24) | k;
+    const size_t argb = M->prec == SA_FP64 ? batch64_args_bytes() : batch32_args_bytes();
+    M->sort_bytes = sort_events_temp_bytes((int)nt);
+    if (e == cudaSuccess) e = M->args.alloc(argb * nplans);
+    if (e == cudaSuccess) e = M->scratch.alloc((size_t)ns * M->slot_bytes);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(M->scratch.p, 0, (size_t)ns * M->slot_bytes, ctx->stream);
+    if (e == cudaSuccess) e = M->queue.alloc(1);
+    if (e == cudaSuccess) e = M->key_a.alloc(nt);
+    if (e == cudaSuccess) e = M->key_b.alloc(nt);
+    if (e == cudaSuccess) e = M->code_in.alloc(nt);
+    if (e == cudaSuccess) e = M->code.upload(code.data(), nt, ctx->stream);
+    if (e == cudaSuccess) e = M->sort_tmp.alloc(std::max<size_t>(M->sort_bytes, 1));
+    if (e == cudaSuccess) e = cudaEventCreate(&M->tk0);
+    if (e == cudaSuccess) e = cudaEventCreate(&M->tk1);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete M;
+        return fail(ctx, e == cudaErrorMemoryAllocation ? SA_ERR_NOMEM : SA_ERR_CUDA,
+                    std::string("sa_multi_create: ") + cudaGetErrorString(e));
+    }
+    *out = M;
+    return SA_OK;
+}
+
+extern "C" void sa_multi_destroy(sa_multi* M) {
+    if (!M) return;
+    cudaSetDevice(M->ctx->device);
+    delete M;
+}
+
+extern "C" int sa_multi_forward_adjoint(sa_multi* M, const double* const* svel,
+                                        const double* const* m11, const double* const* m12,
+                                        const double* const* m22, const double* const* tt_obs,
+                                        const double* const* weight, int calc_adj,
+                                        double* const* syn, double* const* adj_s,
+                                        double* const* chi, int* const* status, void* stream) {
+    if (!M || !svel || !tt_obs || !weight) return SA_ERR_ARG;
+    sa_ctx* ctx = M->ctx;
+    const int nlev = (int)M->plans.size();
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const bool general = m11 && m11[0];
+    std::vector<BatchDesc> d(nlev);
+    for (int i = 0; i < nlev; i++) {
+        sa_plan* P = M->plans[i];
+        const bool gi = m11 && m11[i];
+        if (gi != general || (gi && (!m12 || !m22 || !m12[i] || !m22[i])))
+            return fail(ctx, SA_ERR_ARG, "sa_multi: media for every plan or for none");
+        if (!svel[i] || (P->npair > 0 && (!tt_obs[i] || !weight[i])))
+            return fail(ctx, SA_ERR_ARG, "sa_multi: svel, tt_obs and weight for every plan");
+        int rc = plan_media(P, svel[i], gi ? m11[i] : nullptr, gi ? m12[i] : nullptr,
+                            gi ? m22[i] : nullptr, gi, st);
+        if (rc) return rc;
+        BatchDesc& b = d[i];
+        b = plan_desc(P, gi);
+        b.ev.tt_obs = tt_obs[i];
+        b.ev.weight = weight[i];
+        b.out.syn = syn ? syn[i] : nullptr;
+        double* as = (calc_adj && adj_s) ? adj_s[i] : nullptr;
+        b.out.adj_s = as;
+        b.out.chi_ev = (calc_adj && chi && chi[i]) ? P->chi_ev.p : nullptr;
+        b.out.fwd_iters = P->fit.p;
+        b.out.adj_iters = P->ait.p;
+        b.out.status = (status && status[i]) ? status[i] : P->status_tmp.p;
+        b.mode = calc_adj ? MODE_FWD_ADJ : MODE_FWD;
+        b.variant = M->prec == SA_FP32 ? M->plans[0]->variant : 0;
+        if (as)
+            SA_CUDA(cudaMemsetAsync(as, 0, (size_t)P->nx * P->ny * P->nper * sizeof(double), st));
+    }
+    Scratch sc{};
+    sc.nslots = M->nslots;
+    sc.slot_bytes = M->slot_bytes;
+    sc.base = M->scratch.p;
+    sc.queue = M->queue.p;
+    sc.order = nullptr;
+    SA_CUDA(cudaMemsetAsync(M->queue.p, 0, sizeof(unsigned int), st));
+    SA_CUDA(cudaEventRecord(M->tk0, st));
+    if (M->ntotal > 0) {
+        const unsigned* code = reinterpret_cast<const unsigned*>(M->code.p);
+        SA_CUDA(M->prec == SA_FP64
+                    ? launch_batch64_multi(d.data(), nlev, M->args.p, M->ntotal, code, sc, st)
+                    : launch_batch32_multi(d.data(), nlev, M->args.p, M->ntotal, code, sc, st));
+    }
+    SA_CUDA(cudaEventRecord(M->tk1, st));
+    for (int i = 0; i < nlev; i++) {
+        sa_plan* P = M->plans[i];
+        if (P->ne == 0) {
+            if (calc_adj && chi && chi[i]) SA_CUDA(cudaMemsetAsync(chi[i], 0, sizeof(double), st));
+            SA_CUDA(cudaMemsetAsync(P->worst.p, 0, sizeof(int), st));
+            continue;
+        }
+        if (calc_adj && chi && chi[i]) SA_CUDA(launch_sum_events(P->ne, P->chi_ev.p, chi[i], st));
+        SA_CUDA(launch_fold_status(P->ne, d[i].out.status, P->worst.p, st));
+        const unsigned scale = (unsigned)std::max<size_t>(1, (size_t)P->nx * P->ny / 256);
+        SA_CUDA(launch_multi_cost(P->ne, P->fit.p, P->ait.p, scale, i, M->key_a.p + M->off[i],
+                                  M->code_in.p + M->off[i], st));
+    }
+    // the next evaluation's queue: every plan's events by work, longest first
+    if (M->ntotal > 0)
+        SA_CUDA(launch_sort_events(M->ntotal, M->key_a.p, M->key_b.p, M->code_in.p, M->code.p,
+                                   M->sort_tmp.p, M->sort_bytes, st));
+    return SA_OK;
+}
+
+extern "C" int sa_multi_kernel_ms(sa_multi* M, float* ms) {
+    if (!M || !ms) return SA_ERR_ARG;
+    sa_ctx* ctx = M->ctx;
+    SA_CUDA(cudaEventSynchronize(M->tk1));
+    SA_CUDA(cudaEventElapsedTime(ms, M->tk0, M->tk1));
+    return SA_OK;
+}
+
+extern "C" int sa_multi_status(sa_multi* M, int* worst) {
+    if (!M || !worst) return SA_ERR_ARG;
+    sa_ctx* ctx = M->ctx;
+    *worst = 0;
+    for (sa_plan* P : M->plans) {
+        int w = 0;
+        SA_CUDA(cudaMemcpy(&w, P->worst.p, sizeof(int), cudaMemcpyDeviceToHost));
+        *worst = std::max(*worst, w);
+    }
+    return SA_OK;
+}
+
 namespace {
 int plan_worst_status(sa_plan* P, cudaStream_t st) {
     sa_ctx* ctx = P->ctx;

@@ -2,6 +2,8 @@
 // kernel.  Sweeps run in FP32 (fast division and square root); T0 and T,
 // residuals, adjoint coefficients, convergence sums and the kernel
 // accumulation stay FP64 (see batch.cuh).
+#include <vector>
+
 #include "batch.cuh"
 #include "launch.h"
 
@@ -57,5 +59,39 @@ cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st) {
     }
     return cudaGetLastError();
 }
+
+// One launch over several plans' events (batch_multi_kernel): the levels'
+// arguments are copied to `dev_args` (nlev BatchArgs<float>), `code` lists
+// level << 24 | event in queue order.  One variant and one metric kind (iso
+// or general) for all levels.
+namespace {
+template <int VAR>
+void launch_multi_variant(bool iso, const BatchArgs<float>* args, unsigned ntotal,
+                          const unsigned* code, const Scratch& sc, int blocks, cudaStream_t st) {
+    if (iso) batch_multi_kernel<float, true, VAR><<<blocks, 128, 0, st>>>(args, ntotal, code, sc);
+    else batch_multi_kernel<float, false, VAR><<<blocks, 128, 0, st>>>(args, ntotal, code, sc);
+}
+}  // namespace
+
+cudaError_t launch_batch32_multi(const BatchDesc* d, int nlev, void* dev_args, unsigned ntotal,
+                                 const unsigned* code, const Scratch& sc, cudaStream_t st) {
+    std::vector<BatchArgs<float>> h(nlev);
+    for (int i = 0; i < nlev; i++) h[i] = make_batch_args<float>(d[i]);
+    cudaError_t e = cudaMemcpyAsync(dev_args, h.data(), nlev * sizeof(BatchArgs<float>),
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    const auto* args = static_cast<const BatchArgs<float>*>(dev_args);
+    const int blocks = (sc.nslots + 3) / 4;
+    const bool iso = d[0].iso != 0;
+    switch (d[0].variant) {
+        case 1: launch_multi_variant<1>(iso, args, ntotal, code, sc, blocks, st); break;
+        case 2: launch_multi_variant<2>(iso, args, ntotal, code, sc, blocks, st); break;
+        case 3: launch_multi_variant<3>(iso, args, ntotal, code, sc, blocks, st); break;
+        default: launch_multi_variant<0>(iso, args, ntotal, code, sc, blocks, st); break;
+    }
+    return cudaGetLastError();
+}
+
+size_t batch32_args_bytes() { return sizeof(BatchArgs<float>); }
 
 }  // namespace sa

@@ -4,6 +4,8 @@
 //
 // Compiled with -fmad=false: every multiply and add rounds separately, as in
 // the reference's FP64 source.  The FP64 path is the parity path.
+#include <vector>
+
 #include "common.cuh"
 #include "event_common.cuh"
 #include "batch.cuh"
@@ -164,5 +166,22 @@ cudaError_t launch_batch64_dev_spacing(const BatchDesc& d, const double* dxdy,
     else batch_kernel_dev_spacing<false><<<blocks, 128, 0, st>>>(B, dxdy);
     return cudaGetLastError();
 }
+
+// One launch over several plans' events (FP64; see launch_batch32_multi).
+cudaError_t launch_batch64_multi(const BatchDesc* d, int nlev, void* dev_args, unsigned ntotal,
+                                 const unsigned* code, const Scratch& sc, cudaStream_t st) {
+    std::vector<BatchArgs<double>> h(nlev);
+    for (int i = 0; i < nlev; i++) h[i] = make_batch_args<double>(d[i]);
+    cudaError_t e = cudaMemcpyAsync(dev_args, h.data(), nlev * sizeof(BatchArgs<double>),
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    const auto* args = static_cast<const BatchArgs<double>*>(dev_args);
+    const int blocks = (sc.nslots + 3) / 4;
+    if (d[0].iso) batch_multi_kernel<double, true, 0><<<blocks, 128, 0, st>>>(args, ntotal, code, sc);
+    else batch_multi_kernel<double, false, 0><<<blocks, 128, 0, st>>>(args, ntotal, code, sc);
+    return cudaGetLastError();
+}
+
+size_t batch64_args_bytes() { return sizeof(BatchArgs<double>); }
 
 }  // namespace sa

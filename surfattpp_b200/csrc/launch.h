@@ -62,6 +62,14 @@ cudaError_t launch_geometry(int nx, int ny, int nsrc, const double* siny, const 
                             const double* sdl, T* G, T* Gx, T* Gy, double* G64,
                             cudaStream_t st);
 cudaError_t launch_batch64(const BatchDesc& d, cudaStream_t st);
+// one launch over nlev plans' events (code[qi] = level << 24 | event); the
+// levels' arguments are copied to dev_args (nlev x batch{32,64}_args_bytes())
+cudaError_t launch_batch32_multi(const BatchDesc* d, int nlev, void* dev_args, unsigned ntotal,
+                                 const unsigned* code, const Scratch& sc, cudaStream_t st);
+cudaError_t launch_batch64_multi(const BatchDesc* d, int nlev, void* dev_args, unsigned ntotal,
+                                 const unsigned* code, const Scratch& sc, cudaStream_t st);
+size_t batch32_args_bytes();
+size_t batch64_args_bytes();
 // launch_batch64 with the grid spacing read on the device from dxdy[0..1]
 cudaError_t launch_batch64_dev_spacing(const BatchDesc& d, const double* dxdy, cudaStream_t st);
 cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st);
@@ -94,6 +102,9 @@ cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int n
                                double* sen_hs = nullptr);
 cudaError_t launch_event_cost(int ne, const int* fwd_it, const int* adj_it, unsigned int* key,
                               int* idx, cudaStream_t st);
+// multi-grid queue keys of one level (work = sweeps x cells) and codes
+cudaError_t launch_multi_cost(int ne, const int* fwd_it, const int* adj_it, unsigned int scale,
+                              int lev, unsigned int* key, int* code, cudaStream_t st);
 size_t sort_events_temp_bytes(int ne);
 cudaError_t launch_sort_events(int ne, const unsigned int* key_in, unsigned int* key_out,
                                const int* idx_in, int* order, void* temp, size_t temp_bytes,

@@ -70,6 +70,26 @@ cudaError_t launch_event_cost(int ne, const int* fwd_it, const int* adj_it, unsi
     return cudaGetLastError();
 }
 
+// Sort keys of one level's events in a multi-grid launch: the previous
+// evaluation's sweep counts times the level's cell count (in units of 256
+// cells), so solves of different grid sizes compare by work; code = level
+// << 24 | event.
+__global__ void multi_cost_kernel(int ne, const int* __restrict__ fwd_it,
+                                  const int* __restrict__ adj_it, unsigned int scale, int lev,
+                                  unsigned int* key, int* code) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ne) return;
+    key[i] = (3u * (unsigned)fwd_it[i] + (unsigned)adj_it[i] + 1u) * scale;
+    code[i] = (lev << 24) | i;
+}
+
+cudaError_t launch_multi_cost(int ne, const int* fwd_it, const int* adj_it, unsigned int scale,
+                              int lev, unsigned int* key, int* code, cudaStream_t st) {
+    if (ne <= 0) return cudaSuccess;
+    multi_cost_kernel<<<(ne + 255) / 256, 256, 0, st>>>(ne, fwd_it, adj_it, scale, lev, key, code);
+    return cudaGetLastError();
+}
+
 // Deterministic accumulation (src/preproc.cpp:28-31 in event order): for one
 // chunk of events [e0, e0 + nchunk), adj_s[ip][k] += contrib[e - e0][k] over
 // the chunk's events of period ip in event order (per_ptr / per_ev: the

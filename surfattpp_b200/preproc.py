@@ -162,3 +162,64 @@ def forward_for_event(xx_deg, yy_deg, svel, events, calc_adj=True, m11=None, m12
     _capi.check(ctx.h, rc)
     return dict(syn=syn[:npair], adj_s=adj_s, chi=chi.value, fwd_iters=fi[:ne],
                 adj_iters=ai[:ne])
+
+
+class MultiPlan:
+    """One persistent launch over the events of several plans -- grid levels
+    of different size (sa_multi): each queue entry names its plan, scratch
+    slots hold the largest grid, and the queue is ordered by work across the
+    plans.  ``run`` takes per-plan lists and returns per-plan output dicts
+    (syn, adj_s, chi, status) equal to each plan's own ``run``."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        self.ctx = self.plans[0].ctx
+        n = len(self.plans)
+        arr = (C.c_void_p * n)(*[p.h for p in self.plans])
+        h = C.c_void_p()
+        rc = _capi.lib().sa_multi_create(arr, n, C.byref(h))
+        _capi.check(self.ctx.h, rc)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().sa_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, svel, tt_obs, weight, calc_adj=True, m11=None, m12=None, m22=None, outs=None,
+            stream=None):
+        import torch
+        n = len(self.plans)
+        outs = [{} for _ in range(n)] if outs is None else outs
+        for p, o, sv in zip(self.plans, outs, svel):
+            f64 = dict(dtype=torch.float64, device=sv.device)
+            o.setdefault("syn", torch.empty(max(p.npair, 1), **f64))
+            o.setdefault("adj_s", torch.empty((p.nper, p.ny, p.nx), **f64))
+            o.setdefault("chi", torch.zeros(1, **f64))
+            o.setdefault("status", torch.zeros(max(p.ne, 1), dtype=torch.int32, device=sv.device))
+        arr = lambda xs: (C.c_void_p * n)(*[ptr(x) for x in xs])
+        none = [None] * n
+        rc = _capi.lib().sa_multi_forward_adjoint(
+            self.h, arr(svel), arr(m11 or none), arr(m12 or none), arr(m22 or none), arr(tt_obs),
+            arr(weight), int(bool(calc_adj)), arr([o["syn"] for o in outs]),
+            arr([o["adj_s"] for o in outs]), arr([o["chi"] for o in outs]),
+            arr([o["status"] for o in outs]), stream)
+        _capi.check(self.ctx.h, rc)
+        return outs
+
+    def kernel_ms(self):
+        """Device time of the last evaluation's batch launch."""
+        ms = C.c_float(0.0)
+        _capi.check(self.ctx.h, _capi.lib().sa_multi_kernel_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def worst_status(self):
+        w = C.c_int(0)
+        _capi.check(self.ctx.h, _capi.lib().sa_multi_status(self.h, C.byref(w)))
+        return w.value
