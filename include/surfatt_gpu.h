@@ -256,6 +256,18 @@ int sa_depthkernel_columns_group(sa_ctx* ctx, int nx, int ny, int nz, const doub
                                  double* sen_vs, double* sen_vp, double* sen_rho, int* status,
                                  void* stream);
 
+/* Replaces the column loop of SurfGrid::compute_dispersion_kernel for Love
+ * waves: surfker::depthkernel_love_phase (igr 0, src/surfdisp.cpp:295-349,
+ * slegn96 src/surfker/slegn96.f90:672-783) and depthkernel_love_group
+ * (igr 1, src/surfdisp.cpp:351-426, slegnpu :785-919): Love phase velocities
+ * (surfdisp96, iwave 1) at t (and t(1 +- 0.005)) per column, then per
+ * (column, period) sen_vs = dc/db (du/db) and sen_rho = dc/drho (du/drho)
+ * (device, (nx, ny, nz, nper)); Love waves have no vp kernel.  status (HOST,
+ * ny*nx, may be NULL) as sa_depthkernel_columns_group.  Synchronous. */
+int sa_depthkernel_columns_love(sa_ctx* ctx, int nx, int ny, int nz, const double* zgrid,
+                                const double* vs3d, int nper, const double* periods, int igr,
+                                double* sen_vs, double* sen_rho, int* status, void* stream);
+
 /* Replaces preproc::combine_kernels, vs-only parametrisation
  * (src/preproc.cpp:276-304): ker_vs(ix,iy,k) = -sum_iper adj_s(iper,ix,iy) *
  * (sen_vs + sen_vp*dVp/dVs + sen_rho*drho/dVp*dVp/dVs), periods in order.
@@ -410,6 +422,12 @@ void sa_grad_destroy(sa_grad* grad);
  * weighted sums over one handle per data type (weights of the reference's
  * data section). */
 int sa_grad_set_data_type(sa_grad* grad, int igr);
+/* The wave type (the reference's data iwave): 2 Rayleigh (default), 1 Love.
+ * Love data: fwdsurf with iwave 1 for the travel times; as in the reference,
+ * depth kernels exist for Love group data only (depthkernel_love_group via
+ * depthkernel1d, src/surf_grid.cpp:282-286), so a Love phase-data run returns
+ * SA_ERR_ARG where the reference's depthkernelHTI1d throws. */
+int sa_grad_set_wave_type(sa_grad* grad, int iwave);
 
 /* Kernel-density preconditioning (the reference's is_kden, postproc
  * kdensity_coe != 0).  Enabled, every sa_grad_run also solves, per event, the

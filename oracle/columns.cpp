@@ -150,3 +150,52 @@ extern "C" int orc_depthkernel_group(int nx, int ny, int nz, const double* zgrid
     });
     return 0;
 }
+
+// surfker::depthkernel_love_phase (src/surfdisp.cpp:295-349, igr 0) and
+// depthkernel_love_group (:351-426, igr 1) per column: Love phase
+// velocities (surfdisp96, iwave 1) at t (and t(1 +- 0.005)), then slegn96 /
+// slegnpu; sen_vs, sen_rho (nx, ny, nz, nper) the first nz layers.
+extern "C" int orc_depthkernel_love(int nx, int ny, int nz, const double* zgrid,
+                                    const double* vs3d, int nper, const double* periods,
+                                    int igr, double* sen_vs, double* sen_rho, int* status,
+                                    int nthreads) {
+    const int ncol = nx * ny;
+    const int mmax = nz + 1;
+    const double dt = 0.01;
+    std::vector<double> t1(nper), t2(nper);
+    for (int i = 0; i < nper; ++i) {
+        t1[i] = periods[i] * (1.0 + 0.5 * dt);
+        t2[i] = periods[i] * (1.0 - 0.5 * dt);
+    }
+    for_columns(ncol, nthreads, [&](int col) {
+        const int ix = col / ny, iy = col % ny;
+        std::vector<float> thk, vp, vs, rho;
+        build_layers(nz, zgrid, vs3d + static_cast<size_t>(col) * nz, thk, vp, vs, rho);
+        std::vector<double> cp(nper, 0.0), cp1(nper, 0.0), cp2(nper, 0.0);
+        int st = orc_surfdisp96(thk.data(), vp.data(), vs.data(), rho.data(), mmax, 1, 1, 1, 0,
+                                nper, periods, cp.data());
+        if (igr) {
+            st |= orc_surfdisp96(thk.data(), vp.data(), vs.data(), rho.data(), mmax, 1, 1, 1, 0,
+                                 nper, t1.data(), cp1.data());
+            st |= orc_surfdisp96(thk.data(), vp.data(), vs.data(), rho.data(), mmax, 1, 1, 1, 0,
+                                 nper, t2.data(), cp2.data());
+        }
+        if (status) status[ix + nx * iy] = st;
+        std::vector<double> kb(mmax), kr(mmax);
+        for (int ip = 0; ip < nper; ip++) {
+            double cg = 0.0;
+            if (igr)
+                orc_slegnpu(thk.data(), vs.data(), rho.data(), mmax, periods[ip], cp[ip], t1[ip],
+                            cp1[ip], t2[ip], cp2[ip], &cg, kb.data(), kr.data(), 1);
+            else
+                orc_slegn96(thk.data(), vs.data(), rho.data(), mmax, periods[ip], cp[ip], &cg,
+                            kb.data(), kr.data(), 1);
+            for (int k = 0; k < nz; k++) {
+                const size_t i4 = ((static_cast<size_t>(col)) * nz + k) * nper + ip;
+                sen_vs[i4] = kb[k];
+                sen_rho[i4] = kr[k];
+            }
+        }
+    });
+    return 0;
+}

@@ -178,6 +178,20 @@ int orc_depthkernel_group(int nx, int ny, int nz, const double* zgrid, const dou
                           int nper, const double* periods, double* sen_vs, double* sen_vp,
                           double* sen_rho, int* status, int nthreads);
 
+/* slegn96 / slegnpu (src/surfker/slegn96.f90:672-919): Love phase kernels
+ * dc2db = b dc/db, dc2dr at cp; group kernels du2db, du2dr from the phase
+ * velocities at t, t1, t2.  Arrays of length nlayer; cg (may be NULL). */
+void orc_slegn96(const float* thk, const float* vs, const float* rhom, int nlayer, double t,
+                 double cp, double* cg, double* dc2db, double* dc2dr, int iflsph);
+void orc_slegnpu(const float* thk, const float* vs, const float* rhom, int nlayer, double t,
+                 double cp, double t1, double cp1, double t2, double cp2, double* cg,
+                 double* du2db, double* du2dr, int iflsph);
+/* Per-column Love depth kernels (surfker::depthkernel_love_phase / _group,
+ * src/surfdisp.cpp:295-426): sen_vs, sen_rho (nx, ny, nz, nper). */
+int orc_depthkernel_love(int nx, int ny, int nz, const double* zgrid, const double* vs3d,
+                         int nper, const double* periods, int igr, double* sen_vs,
+                         double* sen_rho, int* status, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,9 @@ def _declare(L):
                                          _ip, _ip, _ip, _dp, _dp, _dp, _dp, i, _dp, _dp,
                                          C.POINTER(d), _ip, _ip, i, C.c_void_p]
     L.orc_kernel_precondition.argtypes = [C.c_size_t, _dp, _dp]
+    L.orc_slegn96.argtypes = [_fp, _fp, _fp, i, d, d, C.POINTER(d), _dp, _dp, i]
+    L.orc_slegnpu.argtypes = [_fp, _fp, _fp, i, d, d, d, d, d, d, C.POINTER(d), _dp, _dp, i]
+    L.orc_depthkernel_love.argtypes = [i, i, i, _dp, _dp, i, _dp, i, _dp, _dp, _ip, i]
     L.orc_combine_kernels_vs.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
     for f in ("orc_vs2vp", "orc_vp2rho", "orc_dalpha_dbeta", "orc_drho_dalpha"):
         getattr(L, f).argtypes = [d]
@@ -384,3 +387,26 @@ def depthkernel_group(zgrid, vs3d, periods, nthreads=1, math="libc"):
     lib(math).orc_depthkernel_group(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, sv, sp, sr, st,
                                 int(nthreads))
     return sv, sp, sr, st
+
+
+def depthkernel_love(zgrid, vs3d, periods, igr=0, nthreads=1, math="libc"):
+    """Love-wave depth kernels (depthkernel_love_phase / _group): sen_vs,
+    sen_rho (nx, ny, nz, nper), status (ny, nx)."""
+    nx, ny, nz = vs3d.shape
+    p = _c(periods)
+    shp = (nx, ny, nz, p.size)
+    sv, sr = np.zeros(shp), np.zeros(shp)
+    st = np.zeros((ny, nx), np.int32)
+    lib(math).orc_depthkernel_love(nx, ny, nz, _c(zgrid), _c(vs3d), p.size, p, int(igr), sv, sr,
+                                   st, int(nthreads))
+    return sv, sr, st
+
+
+def slegn96(thk, vs, rho, t, cp, iflsph=1):
+    """One slegn96 call: dict(dc2db, dc2dr, cg)."""
+    n = len(thk)
+    kb, kr, cg = np.zeros(n), np.zeros(n), C.c_double()
+    f = lambda a: _c(a, np.float32)
+    lib().orc_slegn96(f(thk), f(vs), f(rho), n, float(t), float(cp), C.byref(cg), kb, kr,
+                      int(iflsph))
+    return dict(dc2db=kb, dc2dr=kr, cg=cg.value)

@@ -33,6 +33,7 @@ EXPORTED = (
     "sa_grad_set_data_type", "sa_plan_kden_output", "sa_grad_set_kden", "sa_grad_ker_den",
     "sa_kernel_precondition", "sa_multi_create", "sa_multi_destroy",
     "sa_multi_forward_adjoint", "sa_multi_kernel_ms", "sa_multi_status",
+    "sa_depthkernel_columns_love", "sa_grad_set_wave_type",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen", "sa_grad_combine",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
@@ -106,6 +107,7 @@ def lib():
     L.sa_grad_vjp.argtypes = [_vp] * 4 + [i] + [_vp] * 4 + [_vp]
     L.sa_plan_set_deterministic.argtypes = [_vp, i, C.c_size_t]
     L.sa_grad_set_data_type.argtypes = [_vp, i]
+    L.sa_grad_set_wave_type.argtypes = [_vp, i]
     L.sa_plan_kden_output.argtypes = [_vp, _vp]
     L.sa_grad_set_kden.argtypes = [_vp, i]
     L.sa_grad_ker_den.argtypes = [_vp] * 4 + [_vp]
@@ -116,6 +118,8 @@ def lib():
         [C.POINTER(_vp)] * 4 + [_vp]
     L.sa_multi_kernel_ms.argtypes = [_vp, C.POINTER(C.c_float)]
     L.sa_multi_status.argtypes = [_vp, C.POINTER(i)]
+    L.sa_depthkernel_columns_love.argtypes = [_vp, i, i, i, _dp, _vp, i, _dp, i, _vp, _vp, _vp,
+                                              _vp]
     L.sa_grad_create.argtypes = [_vp, i, _dp, _dp, C.POINTER(_vp)]
     L.sa_grad_destroy.argtypes = [_vp]
     L.sa_grad_run.argtypes = [_vp] + [_vp] * 9 + [_vp]

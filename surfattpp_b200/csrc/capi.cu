@@ -1293,6 +1293,54 @@ extern "C" int sa_depthkernel_columns_group(sa_ctx* ctx, int nx, int ny, int nz,
     return SA_OK;
 }
 
+extern "C" int sa_depthkernel_columns_love(sa_ctx* ctx, int nx, int ny, int nz,
+                                           const double* zgrid, const double* vs3d, int nper,
+                                           const double* periods, int igr, double* sen_vs,
+                                           double* sen_rho, int* status, void* stream) {
+    if (!ctx) return SA_ERR_ARG;
+    if (nx < 1 || ny < 1 || nz < 2 || nper < 1 || nper > 64 || !zgrid || !periods || !vs3d ||
+        !sen_vs || !sen_rho || (igr != 0 && igr != 1))
+        return fail(ctx, SA_ERR_ARG, "sa_depthkernel_columns_love: bad sizes, igr or pointers");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    int rc = SA_OK;
+    const void* L = layer_const_dev(ctx, nz, zgrid, &rc);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    // periods t(1 +- 0.5*0.01) (src/surfdisp.cpp:361-366)
+    const double dt = 0.01;
+    std::vector<double> t3(3 * (size_t)nper);
+    for (int i = 0; i < nper; ++i) {
+        t3[i] = periods[i];
+        t3[nper + i] = periods[i] * (1.0 + 0.5 * dt);
+        t3[2 * nper + i] = periods[i] * (1.0 - 0.5 * dt);
+    }
+    const int nrun = igr ? 3 : 1;
+    const size_t plane = (size_t)nx * ny * nper, ncol = (size_t)nx * ny;
+    DArr<double> dper, cps;
+    DArr<int> st3;
+    SA_CUDA(dper.upload(t3.data(), t3.size(), st));
+    SA_CUDA(cps.alloc(3 * plane));
+    SA_CUDA(st3.alloc(3 * ncol));
+    SA_CUDA(cudaMemsetAsync(st3.p, 0, 3 * ncol * sizeof(int), st));
+    for (int k = 0; k < nrun; k++)   // Love phase velocities (iwave 1)
+        SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, dper.p + k * nper, 1, 1, 0, L,
+                                        cps.p + k * plane, st3.p + k * ncol, st));
+    SA_CUDA(launch_depthkernel_love(nx, ny, nz, vs3d, nper, dper.p, dper.p + nper,
+                                    dper.p + 2 * nper, cps.p, cps.p + plane, cps.p + 2 * plane,
+                                    igr, L, sen_vs, sen_rho, st));
+    std::vector<int> hs(3 * ncol);
+    SA_CUDA(cudaMemcpyAsync(hs.data(), st3.p, hs.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    SA_CUDA(cudaStreamSynchronize(st));
+    int bad = 0;
+    for (size_t c = 0; c < ncol; c++) {
+        const int v = hs[c] | hs[ncol + c] | hs[2 * ncol + c];
+        if (status) status[c] = v;
+        bad |= v;
+    }
+    if (bad) return fail(ctx, SA_ERR_NOROOT, "Dispersion calculation failed");
+    return SA_OK;
+}
+
 extern "C" int sa_combine_kernels_vs(sa_ctx* ctx, int nx, int ny, int nz, int nper,
                                      const double* adj_s, const double* vs3d, const double* vp3d,
                                      const double* sen_vs, const double* sen_vp,
@@ -1322,6 +1370,7 @@ struct sa_grad {
     // phase velocities at t, t(1 + 0.005), t(1 - 0.005) (per3, cps3) and
     // sregnpu; colst then holds 4 status planes (group, 3 phase runs)
     int igr = 0;
+    int iwave = 2;           // 2 Rayleigh, 1 Love (sa_grad_set_wave_type)
     DArr<double> per3, cps3;
     bool kden = false;       // is_kden (sa_grad_set_kden): kden_s accumulated per run
     DArr<double> kden_s;
@@ -1391,8 +1440,8 @@ namespace {
 int grad_velocities(sa_grad* g, const double* vs3d, double* svel, cudaStream_t st) {
     sa_plan* P = g->plan;
     sa_ctx* ctx = P->ctx;
-    SA_CUDA(launch_surfdisp_columns(P->nx, P->ny, g->nz, vs3d, P->nper, g->periods.p, 1, 2,
-                                    g->igr, g->lc.p, svel, g->colst.p, st));
+    SA_CUDA(launch_surfdisp_columns(P->nx, P->ny, g->nz, vs3d, P->nper, g->periods.p, 1,
+                                    g->iwave, g->igr, g->lc.p, svel, g->colst.p, st));
     return SA_OK;
 }
 // The data type's depth kernels on `st` (phase: sregn96_hti at svel; group:
@@ -1403,15 +1452,27 @@ int grad_depth_kernels(sa_grad* g, const double* vs3d, const double* svel, doubl
     sa_ctx* ctx = P->ctx;
     const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
     if (g->igr == 0) {
+        if (g->iwave == 1)   // SurfGrid::compute_dispersion_kernel sends phase data to
+            return fail(ctx, SA_ERR_ARG,   // depthkernelHTI1d, which takes Rayleigh only
+                        "Love phase-velocity data: the reference's kernels are Rayleigh only "
+                        "(src/surf_grid.cpp:282-286, src/surfdisp.cpp:484-487)");
         SA_CUDA(launch_depthkernel(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p,
                                    g->sen_vs.p, g->sen_vp.p, g->sen_rho.p, st, sen_hs));
         return SA_OK;
     }
     const size_t plane = (size_t)nx * ny * nper, ncol = (size_t)nx * ny;
     for (int k = 0; k < 3; k++)
-        SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->per3.p + k * nper, 1, 2, 0,
-                                        g->lc.p, g->cps3.p + k * plane,
+        SA_CUDA(launch_surfdisp_columns(nx, ny, nz, vs3d, nper, g->per3.p + k * nper, 1,
+                                        g->iwave, 0, g->lc.p, g->cps3.p + k * plane,
                                         g->colst.p + (k + 1) * ncol, st));
+    if (g->iwave == 1) {   // Love group kernels (no vp kernel)
+        SA_CUDA(launch_depthkernel_love(nx, ny, nz, vs3d, nper, g->per3.p, g->per3.p + nper,
+                                        g->per3.p + 2 * nper, g->cps3.p, g->cps3.p + plane,
+                                        g->cps3.p + 2 * plane, 1, g->lc.p, g->sen_vs.p,
+                                        g->sen_rho.p, st));
+        SA_CUDA(cudaMemsetAsync(g->sen_vp.p, 0, plane * nz * sizeof(double), st));
+        return SA_OK;
+    }
     SA_CUDA(launch_depthkernel_group(nx, ny, nz, vs3d, nper, g->per3.p, g->per3.p + nper,
                                      g->per3.p + 2 * nper, g->cps3.p, g->cps3.p + plane,
                                      g->cps3.p + 2 * plane, g->lc.p, g->sen_vs.p, g->sen_vp.p,
@@ -1422,6 +1483,14 @@ int grad_ncolst(const sa_grad* g) {
     return (g->igr ? 4 : 1) * g->plan->nx * g->plan->ny;
 }
 }  // namespace
+
+extern "C" int sa_grad_set_wave_type(sa_grad* g, int iwave) {
+    if (!g) return SA_ERR_ARG;
+    sa_ctx* ctx = g->plan->ctx;
+    if (iwave != 1 && iwave != 2) return fail(ctx, SA_ERR_ARG, "wave type: 1 Love, 2 Rayleigh");
+    g->iwave = iwave;
+    return SA_OK;
+}
 
 extern "C" int sa_grad_set_data_type(sa_grad* g, int igr) {
     if (!g) return SA_ERR_ARG;
@@ -1543,8 +1612,8 @@ extern "C" int sa_grad_vjp(sa_grad* g, const double* vs3d, const double* vp3d,
     if (!vs3d || !grad || (P->npair > 0 && !source_adj))
         return fail(ctx, SA_ERR_ARG, "vs3d, source_adj and grad are required");
     if (convention != 0 && convention != 1) return fail(ctx, SA_ERR_ARG, "convention 0 or 1");
-    if (convention == 1 && g->igr != 0)
-        return fail(ctx, SA_ERR_ARG, "the derivative convention is for phase-velocity data");
+    if (convention == 1 && (g->igr != 0 || g->iwave != 2))
+        return fail(ctx, SA_ERR_ARG, "the derivative convention is for Rayleigh phase data");
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;

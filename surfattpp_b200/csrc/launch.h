@@ -142,6 +142,12 @@ cudaError_t launch_grid_topo(int nxr, int nyr, const double* xr, const double* y
 cudaError_t launch_pde_smooth(int nx, int ny, int nz, double B, double D, const double* rowX,
                               const double* rowY, const double* depE, int nstep, double* field,
                               double* work, cudaStream_t st);
+// Love depth kernels (igr 0 phase at cp; 1 group from cp, cp1, cp2)
+cudaError_t launch_depthkernel_love(int nx, int ny, int nz, const double* vs3d, int nper,
+                                    const double* periods, const double* p1, const double* p2,
+                                    const double* cp, const double* cp1, const double* cp2,
+                                    int igr, const void* layer_const, double* sen_vs,
+                                    double* sen_rho, cudaStream_t st);
 cudaError_t launch_depthkernel_group(int nx, int ny, int nz, const double* vs3d, int nper,
                                      const double* periods, const double* p1, const double* p2,
                                      const double* cp, const double* cp1, const double* cp2,

@@ -152,6 +152,94 @@ depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int 
     }
 }
 
+// Love-wave depth kernels, one thread per (column, period):
+// surfker::depthkernel_love_phase (src/surfdisp.cpp:295-349) through slegn96
+// (src/surfker/slegn96.f90:672-783) when igr = 0, depthkernel_love_group
+// (:351-426) through slegnpu (:785-919) when igr = 1 (phase velocities at t,
+// t1 = t(1 + 0.005), t2 = t(1 - 0.005) from cp, cp1, cp2).  sen_vs = dc/db
+// (du/db), sen_rho = dc/drho (du/drho) of the first nz layers,
+// earth-flattening corrected (splove, :631-670).  Models without water.
+__global__ void __launch_bounds__(64, SK_DEPTH_MINB)
+depthkernel_love_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
+                        const double* __restrict__ periods, const double* __restrict__ p1,
+                        const double* __restrict__ p2, const double* __restrict__ cp_plane,
+                        const double* __restrict__ cp1_plane,
+                        const double* __restrict__ cp2_plane, int igr,
+                        const LayerConst* __restrict__ Lp, double* sen_vs, double* sen_rho) {
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= (long long)nx * ny * nper) return;
+    const int ip = (int)(gid % nper);
+    const int col = (int)(gid / nper);
+    const int ix = col / ny, iy = col % ny;
+    const LayerConst& L = *Lp;
+    float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];
+    sk::column_model(vs3d + (size_t)col * nz, nz, L, vp, vs, rho);
+    sk::LW W;
+    sk::lv_model(W, vs, rho, L);
+    const double twopi = 2.0 * sk::kLovePiF;
+    const double ar = 6371.0;
+    const size_t pix = (size_t)ip * nx * ny + ix + (size_t)nx * iy;
+    const double t = periods[ip], cp = cp_plane[pix];
+    double omega = twopi / t;
+    sk::lv_shfunc(W, omega, omega / cp);
+    sk::lv_energy(W, omega, omega / cp);
+    if (!igr) {
+        const double x = (3.0 * cp) / ((2.0 * ar) * omega);
+        const double tm = sqrt(1.0 + x * x);
+        const double tm3 = tm * tm * tm;
+        for (int k = 0; k < nz; k++) {
+            const size_t i4 = ((size_t)col * nz + k) * nper + ip;
+            sen_vs[i4] = W.dcdb[k] * L.rg_vtp[k] / tm3;
+            sen_rho[i4] = W.dcdr[k] * L.lv_rtp[k] / tm3;
+        }
+        return;
+    }
+    const double cg = W.ugr;
+    double b0[sk::MMAX], r0[sk::MMAX], b1[sk::MMAX], r1[sk::MMAX];
+    for (int k = 0; k < nz; k++) {
+        b0[k] = W.dcdb[k];
+        r0[k] = W.dcdr[k];
+    }
+    const double t1 = p1[ip], t2 = p2[ip];
+    omega = twopi / t1;
+    const double c1 = cp1_plane[pix];
+    sk::lv_shfunc(W, omega, omega / c1);
+    sk::lv_energy(W, omega, omega / c1);
+    for (int k = 0; k < nz; k++) {
+        b1[k] = W.dcdb[k];
+        r1[k] = W.dcdr[k];
+    }
+    omega = twopi / t2;
+    const double c2 = cp2_plane[pix];
+    sk::lv_shfunc(W, omega, omega / c2);
+    sk::lv_energy(W, omega, omega / c2);   // W.dc* now hold this evaluation
+    const double uc1 = cg / cp;
+    omega = twopi / t;
+    const double x = (3.0 * cp) / ((2.0 * ar) * omega);
+    const double tm = sqrt(1.0 + x * x);
+    const double y = 1.5 / (ar * omega);
+    const double tm1 = (y * y) / tm;
+    for (int k = 0; k < nz; k++) {
+        const double dub = uc1 * (2.0 - uc1) * W.dcdb[k] - uc1 * uc1 * t * (W.dcdb[k] - b1[k]) / (t2 - t1);
+        const double dur = uc1 * (2.0 - uc1) * W.dcdr[k] - uc1 * uc1 * t * (W.dcdr[k] - r1[k]) / (t2 - t1);
+        const size_t i4 = ((size_t)col * nz + k) * nper + ip;
+        sen_vs[i4] = (tm * dub + cg * cp * b0[k] * tm1) * L.rg_vtp[k];
+        sen_rho[i4] = (tm * dur + cg * cp * r0[k] * tm1) * L.lv_rtp[k];
+    }
+}
+
+cudaError_t launch_depthkernel_love(int nx, int ny, int nz, const double* vs3d, int nper,
+                                    const double* periods, const double* p1, const double* p2,
+                                    const double* cp, const double* cp1, const double* cp2,
+                                    int igr, const void* layer_const, double* sen_vs,
+                                    double* sen_rho, cudaStream_t st) {
+    const long long n = (long long)nx * ny * nper;
+    depthkernel_love_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
+        nx, ny, nz, vs3d, nper, periods, p1, p2, cp, cp1, cp2, igr,
+        reinterpret_cast<const LayerConst*>(layer_const), sen_vs, sen_rho);
+    return cudaGetLastError();
+}
+
 // preproc::combine_kernels, vs-only branch (src/preproc.cpp:276-304): one
 // thread per (ix, iy, k), periods accumulated in order from zero.
 __global__ void combine_vs_kernel(int nx, int ny, int nz, int nper, const double* __restrict__ adj_s,
@@ -332,6 +420,9 @@ int build_layer_const(int nz, const double* zgrid, void* out) {
             const double tmp = (2.0 * ar) / (r0 + r1);
             L.rg_vtp[i - 1] = tmp;
             L.rg_rtp[i - 1] = std::pow(tmp, expo);
+            // slegn96 bldsph: tmp**(-5) as gfortran expands it (x^3 x^2, inverse)
+            const double x2 = tmp * tmp, x3 = x2 * tmp, x5 = x3 * x2;
+            L.lv_rtp[i - 1] = 1.0 / x5;
             L.rg_dtp[i - 1] = ar / r0;
             L.rg_zd[i - 1] = z1 - z0;
             r0 = r1;

@@ -39,6 +39,7 @@ struct LayerConst {
     double rg_zd[MMAX];      // flattened thickness (zd(mmax) = 0)
     double rg_vtp[MMAX];
     double rg_rtp[MMAX];     // tmp**(-2.275), FP64 power
+    double lv_rtp[MMAX];     // tmp**(-5) of slegn96's bldsph (Love density factor)
     double rg_dtp[MMAX];
     float thk[MMAX];         // unflattened float thickness (build_disp_req)
 };
@@ -1275,6 +1276,167 @@ __device__ inline double energy(RW& W, double om, double wvno, double& ugr, doub
         W.dcdgc[m] = W.dcdgc[m] / (ugr * sumi0);
     }
     return sumi0;
+}
+
+// ---------------------------------------------------------------------------
+// slegn96 / slegnpu: Love-wave eigenfunctions and depth kernels
+// (src/surfker/slegn96.f90, modules LoveWaveModel / LoveWaveKernel)
+// ---------------------------------------------------------------------------
+struct LW {
+    int mmax;
+    double zd[MMAX], zb[MMAX], zrho[MMAX], xmu[MMAX], uu[MMAX], tt[MMAX], exl[MMAX];
+    double dcdb[MMAX], dcdr[MMAX];
+    double cosq, sinq, yl, zl, mu;
+    double sumi0, sumi1, sumi2, ugr;
+};
+
+// pi of both Love drivers: a REAL*4 value (slegn96.f90:689, :808)
+constexpr double kLovePiF = (double)3.1415926535898f;
+
+// The model (slegn96.f90:697-716, :834-852) with bldsph (:107-167) from the
+// per-layer constants; group: iwat from zb > 0, phase: from zb == 0 (the
+// same for the models here, which have no water).
+__device__ inline void lv_model(LW& W, const float* vs, const float* rho, const LayerConst& L) {
+    W.mmax = L.mmax;
+    for (int i = 0; i < L.mmax; i++) {
+        W.zb[i] = (double)vs[i] * L.rg_vtp[i];
+        W.zrho[i] = (double)rho[i] * L.lv_rtp[i];
+        W.zd[i] = L.rg_zd[i];
+        W.xmu[i] = W.zrho[i] * (W.zb[i] * W.zb[i]);
+    }
+}
+
+// varl (:248-328)
+__device__ inline void lv_varl(LW& W, int m, double& rb, double omega, double wvno, double& xkb,
+                               double dpth, double& eexl) {
+    xkb = omega / W.zb[m];
+    const double wvnop = wvno + xkb;
+    const double wvnom = fabs(wvno - xkb);
+    rb = sqrt(wvnop * wvnom);
+    const double q = rb * dpth;
+    W.mu = W.zrho[m] * W.zb[m] * W.zb[m];
+    eexl = 0.0;
+    if (wvno < xkb) {
+        sk_sincos(q, &W.sinq, &W.cosq);
+        W.yl = W.sinq / rb;
+        W.zl = -(rb * W.sinq);
+    } else if (wvno == xkb) {
+        W.cosq = 1.0;
+        W.yl = dpth;
+        W.zl = 0.0;
+    } else if (wvno > xkb) {
+        eexl = q;
+        double fac = 0.0;
+        if (q < 18.0) fac = sk_exp(-2.0 * q);
+        W.cosq = (1.0 + fac) * 0.5;
+        W.sinq = (1.0 - fac) * 0.5;
+        W.yl = W.sinq / rb;
+        W.zl = rb * W.sinq;
+    }
+}
+
+// shfunc (:179-246) with up (:372-445) and hskl (:330-351)
+static __device__ SK_NOINLINE_EIG void lv_shfunc(LW& W, double omega, double wvno) {
+    const int mmax = W.mmax;
+    double rb = 0, xkb = 0, eexl = 0;
+    if (W.zb[mmax - 1] > (double)0.01f) {
+        lv_varl(W, mmax - 1, rb, omega, wvno, xkb, 0.0, eexl);
+        W.uu[mmax - 1] = 1.0;
+        W.tt[mmax - 1] = -(W.xmu[mmax - 1] * rb);
+    } else {
+        W.uu[mmax - 1] = 1.0;
+        W.tt[mmax - 1] = 0.0;
+    }
+    W.exl[mmax - 1] = 0.0;
+    for (int k = mmax - 2; k >= 0; k--) {
+        lv_varl(W, k, rb, omega, wvno, xkb, W.zd[k], eexl);
+        const double a11 = W.cosq, a22 = W.cosq, a12 = -(W.yl / W.mu), a21 = -(W.zl * W.mu);
+        const double amp0 = a11 * W.uu[k + 1] + a12 * W.tt[k + 1];
+        const double str0 = a21 * W.uu[k + 1] + a22 * W.tt[k + 1];
+        double rr = fabs(amp0);
+        const double ss = fabs(str0);
+        if (ss > rr) rr = ss;
+        if (rr < 1.e-30) rr = 1.0;
+        W.exl[k] = sk_log(rr) + eexl;
+        W.uu[k] = amp0 / rr;
+        W.tt[k] = str0 / rr;
+    }
+    double ext = 0.0;
+    double umax = W.uu[0];
+    W.tt[0] = 0.0;
+    for (int k = 1; k < mmax; k++) {
+        ext = ext + W.exl[k - 1];
+        double fact = 0.0;
+        if (ext < 80.0) fact = 1.0 / sk_exp(ext);
+        W.uu[k] = W.uu[k] * fact;
+        W.tt[k] = W.tt[k] * fact;
+        if (fabs(W.uu[k]) > fabs(umax)) umax = W.uu[k];
+    }
+    if (W.uu[0] != 0.0) umax = W.uu[0];
+    if (fabs(umax) > 0.0)
+        for (int k = 0; k < mmax; k++) {
+            W.uu[k] = W.uu[k] / umax;
+            W.tt[k] = W.tt[k] / umax;
+        }
+}
+
+// energy (:447-629): velocity and density kernels (dc/db, dc/drho) and the
+// energy integrals
+static __device__ SK_NOINLINE_EIG void lv_energy(LW& W, double omega, double wvno) {
+    const int mmax = W.mmax;
+    const double c = omega / wvno;
+    const double wvno2 = wvno * wvno;
+    W.sumi0 = W.sumi1 = W.sumi2 = 0.0;
+    for (int k = 0; k < mmax; k++) {
+        const double TN = W.zrho[k] * W.zb[k] * W.zb[k];
+        const double TL = W.zrho[k] * W.zb[k] * W.zb[k];
+        const double VSHH = W.zb[k], VSHV = W.zb[k];
+        const double drho = W.zrho[k];
+        const double dpth = W.zd[k];
+        double rb = 0, xkb = 0, eexl = 0;
+        lv_varl(W, k, rb, omega, wvno, xkb, dpth, eexl);
+        const double dmu = W.xmu[k];
+        if (rb < 1.0e-10) rb = 1.0e-10;
+        double upup, dupdup;
+        if (k == mmax - 1) {
+            upup = (0.5 / rb) * W.uu[mmax - 1] * W.uu[mmax - 1];
+            dupdup = (0.5 * rb) * W.uu[mmax - 1] * W.uu[mmax - 1];
+        } else {
+            cx nub = C(rb, 0.0);
+            if (wvno < xkb) nub = C(0.0, rb);
+            const cx xnub = dmu * nub;
+            // emat (:353-370)
+            const cx wx = wvno * xnub;
+            const cx ei11 = C(0.5 / wvno), ei12 = C(0.5) / wx, ei21 = C(0.5 / wvno),
+                     ei22 = -(C(0.5) / wx);
+            const cx el11 = C(wvno), el12 = C(wvno);
+            const cx km1dn = ei21 * W.uu[k] + ei22 * W.tt[k];
+            const cx kmup = ei11 * W.uu[k + 1] + ei12 * W.tt[k + 1];
+            const cx f3 = nub * dpth;
+            cx exqq = C(0.0);
+            if (f3.re < 40.0) exqq = cexp_(-2.0 * f3);
+            const cx f = (1.0 - exqq) / (2.0 * nub);
+            exqq = C(0.0);
+            if (f3.re < 75.0) exqq = cexp_(-f3);
+            const cx g = dpth * exqq;
+            const cx f1 = f * (el11 * el11 * kmup * kmup + el12 * el12 * km1dn * km1dn);
+            const cx f2 = g * (el11 * el12 + el11 * el12) * kmup * km1dn;
+            upup = (f1 + f2).re;
+            dupdup = (nub * nub * (f1 - f2)).re;
+        }
+        W.sumi0 = W.sumi0 + drho * upup;
+        W.sumi1 = W.sumi1 + TN * upup;
+        W.sumi2 = W.sumi2 + TL * dupdup;
+        const double DCDBH = c * drho * VSHH * upup;
+        const double DCDBV = c * drho * VSHV * dupdup / wvno2;
+        W.dcdb[k] = DCDBH + DCDBV;
+        W.dcdr[k] = 0.5 * c * (-(c * c * upup) + VSHH * VSHH * upup + VSHV * VSHV * dupdup / wvno2);
+    }
+    for (int k = 0; k < mmax; k++) {
+        W.dcdb[k] = W.dcdb[k] / W.sumi1;
+        W.dcdr[k] = W.dcdr[k] / W.sumi1;
+    }
+    W.ugr = W.sumi1 / (c * W.sumi0);
 }
 
 }  // namespace sk

@@ -45,8 +45,11 @@ from .preproc import ForwardAdjointPlan, _c
 class MisfitGradient:
     """One misfit-gradient evaluation per ``run`` (sa_grad)."""
 
-    def __init__(self, plan: ForwardAdjointPlan, zgrid, periods, data_type="ph"):
-        """data_type "ph" (Rayleigh phase velocities) or "gr" (group)."""
+    def __init__(self, plan: ForwardAdjointPlan, zgrid, periods, data_type="ph",
+                 wave="rayleigh"):
+        """data_type "ph" (phase velocities) or "gr" (group); wave "rayleigh"
+        or "love" (Love kernels exist for group data only, as in the
+        reference)."""
         self.plan = plan
         self.zgrid = _c(zgrid)
         self.periods = _c(periods)
@@ -61,6 +64,10 @@ class MisfitGradient:
         igr = {"ph": 0, "gr": 1}[data_type]
         if igr:
             _capi.check(plan.ctx.h, _capi.lib().sa_grad_set_data_type(self.h, igr))
+        self.wave = wave
+        iwave = {"rayleigh": 2, "love": 1}[wave]
+        if iwave != 2:
+            _capi.check(plan.ctx.h, _capi.lib().sa_grad_set_wave_type(self.h, iwave))
 
     def set_kden(self, enable=True):
         """is_kden: every run also returns ker_den, the kernel density
@@ -137,10 +144,13 @@ class MisfitGradient:
         return ker_vs
 
     def forward_times(self, vs3d, syn=None, svel=None, stream=None):
-        """Receiver travel times T_rec [npair] of vs3d (sa_grad_forward)."""
+        """Receiver travel times T_rec [npair] of vs3d (sa_grad_forward), on
+        torch's current stream unless `stream` is given."""
         import torch
         p = self.plan
         dev = vs3d.device
+        if stream is None:
+            stream = torch.cuda.current_stream(dev).cuda_stream
         if syn is None:
             syn = torch.empty(max(p.npair, 1), dtype=torch.float64, device=dev)
         st = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -151,10 +161,13 @@ class MisfitGradient:
 
     def vjp(self, vs3d, source_adj, convention="reference", vp3d=None, grad=None,
             adj_s=None, stream=None):
-        """The vs gradient of sum(source_adj * T_rec) (sa_grad_vjp); see the
-        module docstring for the conventions."""
+        """The vs gradient of sum(source_adj * T_rec) (sa_grad_vjp), on
+        torch's current stream unless `stream` is given; see the module
+        docstring for the conventions."""
         import torch
         p = self.plan
+        if stream is None:
+            stream = torch.cuda.current_stream(vs3d.device).cuda_stream
         conv = {"reference": 0, "derivative": 1}[convention]
         if grad is None:
             grad = torch.empty((p.nx, p.ny, self.nz), dtype=torch.float64, device=vs3d.device)

@@ -87,3 +87,25 @@ def depthkernel_group(zgrid, vs3d, periods, ctx=None, stream=None):
         raise DispersionError(f"Dispersion calculation failed in {int((status != 0).sum())} columns")
     _capi.check(ctx.h, rc)
     return tuple(out)
+
+
+def depthkernel_love(zgrid, vs3d, periods, igr=0, ctx=None, stream=None):
+    """Love-wave depth kernels (surfker::depthkernel_love_phase for igr 0,
+    depthkernel_love_group for igr 1): (sen_vs, sen_rho) each (nx, ny, nz,
+    nper) -- dc/db, dc/drho (du/db, du/drho); raises DispersionError where a
+    root search fails."""
+    import torch
+    ctx = ctx or default_context()
+    nx, ny, nz = vs3d.shape
+    p = np.ascontiguousarray(periods, dtype=np.float64)
+    z = np.ascontiguousarray(zgrid, dtype=np.float64)
+    out = [torch.empty((nx, ny, nz, p.size), dtype=torch.float64, device=vs3d.device)
+           for _ in range(2)]
+    status = np.zeros(nx * ny, np.int32)
+    rc = _capi.lib().sa_depthkernel_columns_love(ctx.h, nx, ny, nz, z, ptr(vs3d), p.size, p,
+                                                 int(igr), ptr(out[0]), ptr(out[1]),
+                                                 status.ctypes.data, stream)
+    if rc == _capi.SA_ERR_NOROOT:
+        raise DispersionError(f"Dispersion calculation failed in {int((status != 0).sum())} columns")
+    _capi.check(ctx.h, rc)
+    return tuple(out)

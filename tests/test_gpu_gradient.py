@@ -251,3 +251,38 @@ def test_kernel_density_preconditioning(c2, gpu, orc):
     gref = orc.kernel_precondition(kden_ref, ref["ker"]) / ref["chi"]
     assert np.abs(grad.cpu().numpy() - gref).max() <= 1e-9 * np.abs(gref).max()
     assert np.abs(ker_curr.cpu().numpy() - ref["ker"]).max() <= 1e-12 * np.abs(ref["ker"]).max()
+
+
+def test_love_group_gradient(c2, gpu, orc):
+    """Love group-velocity data (the reference's only Love path in an
+    inversion: depthkernel1d for group data, src/surf_grid.cpp:282-286):
+    group velocities from fwdsurf (iwave 1, igr 1), the slegnpu kernels, no
+    vp kernel.  FP64 against the oracle's chain: misfit 1e-12, ker_vs 1e-12
+    of max.  Love phase data are rejected, as the reference's
+    depthkernelHTI1d does."""
+    import torch
+    from surfattpp_b200 import _capi, inversion
+    w, ev, vs0, ref = c2
+    m11, m12, m22 = w.media()
+    u_true, _ = orc.fwdsurf(w.zgrid, w.vs3d, w.periods, iwave=1, igr=1, nthreads=8)
+    ev_l = dict(ev)
+    ev_l["tt_obs"] = orc.forward_for_events(w.xx_deg, w.yy_deg, u_true, m11, m12, m22, ev,
+                                            calc_adj=False, nthreads=8)["syn"].copy()
+    u0, _ = orc.fwdsurf(w.zgrid, vs0, w.periods, iwave=1, igr=1, nthreads=8)
+    rl = orc.forward_for_events(w.xx_deg, w.yy_deg, u0, m11, m12, m22, ev_l, calc_adj=True,
+                                nthreads=8)
+    sv, sr, st = orc.depthkernel_love(w.zgrid, vs0, w.periods, igr=1, nthreads=8)
+    assert st.sum() == 0
+    vp0 = np.vectorize(orc.vs2vp)(vs0)
+    kref = orc.combine_kernels_vs(rl["adj_s"], vs0, vp0, sv, np.zeros_like(sv), sr)
+    plan, g, tt, wt, t = _grad(w, ev_l, "fp64")
+    g_love = inversion.MisfitGradient(plan, w.zgrid, w.periods, data_type="gr", wave="love")
+    out = g_love.run(t(vs0), tt, wt)
+    torch.cuda.synchronize()
+    assert int(out["status"][0]) == 0
+    assert abs(float(out["chi"][0]) - rl["chi"]) <= 1e-12 * abs(rl["chi"])
+    ker = out["ker_vs"].cpu().numpy()
+    assert np.abs(ker - kref).max() <= 1e-12 * np.abs(kref).max()
+    g_ph = inversion.MisfitGradient(plan, w.zgrid, w.periods, data_type="ph", wave="love")
+    with pytest.raises(_capi.SAError):
+        g_ph.run(t(vs0), tt, wt)

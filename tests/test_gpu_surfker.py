@@ -117,3 +117,22 @@ def test_group_depthkernel_matches_oracle(orc, gpu, c1):
         g = g.cpu().numpy()
         assert np.array_equal(g, rc)
         assert np.max(_column_err(g, r)) <= 2e-10
+
+
+@pytest.mark.parametrize("igr", [0, 1])
+def test_love_depthkernel_matches_oracle(orc, gpu, c1, igr):
+    """Love-wave kernels (depthkernel_love_phase / _group through slegn96 /
+    slegnpu): bit-identical to the correctly-rounded-math oracle, within
+    1e-12 of each column's largest kernel of the C-library oracle (whose
+    own floor here is 2e-13)."""
+    from surfattpp_b200 import surfker
+    w = c1
+    vs = w.vs3d[::4, ::4].copy()
+    ref = orc.depthkernel_love(w.zgrid, vs, w.periods, igr=igr, nthreads=8)
+    ref_cr = orc.depthkernel_love(w.zgrid, vs, w.periods, igr=igr, nthreads=8, math="cr")
+    assert ref[2].sum() == 0
+    got = surfker.depthkernel_love(w.zgrid, _dev(vs), w.periods, igr=igr)
+    for g, r, rc in zip(got, ref[:2], ref_cr[:2]):
+        g = g.cpu().numpy()
+        assert np.array_equal(g, rc)
+        assert np.max(_column_err(g, r)) <= 1e-12

@@ -268,3 +268,59 @@ def test_sregnpu_group_velocity_and_homogeneity(orc):
         assert abs(cg - u[k]) / u[k] < 2e-4
         s = ua.sum() + ub.sum() + (h * uh).sum()
         assert abs(s - cg) / cg < 5e-3   # the kernels difference t(1 +- 0.005): 0.3 % observed
+
+
+def _love_fd(orc, model, T, igr, which, h, iflsph):
+    thk, vp, vs, rho = model
+    out = []
+    for layer in range(4):
+        vals = []
+        for s in (1.0, -1.0):
+            b, r = vs.copy(), rho.copy()
+            (b if which == "b" else r)[layer] += s * h
+            v, _ = orc.surfdisp96(thk, vp, b, r, np.array([T]), iflsph=iflsph, iwave=1, igr=igr)
+            vals.append(v[0])
+        out.append((vals[0] - vals[1]) / (2 * h))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("iflsph", [0, 1])
+def test_slegn96_love_kernels_match_fd(orc, iflsph):
+    """slegn96 (src/surfker/slegn96.f90:672-783): its energy-integral group
+    velocity equals surfdisp96's Love group velocity (2e-4), and its kernels
+    are plain derivatives dc/db, dc/drho (unlike sregn96's dimensionless
+    ones): central differences of surfdisp96's Love phase velocity agree to
+    1e-2 of the largest layer value (the REAL*4 model and root limit the
+    differences)."""
+    model = _surfdisp_test_model()
+    thk, vp, vs, rho = model
+    c, _ = orc.surfdisp96(thk, vp, vs, rho, PERIODS, iflsph=iflsph, iwave=1)
+    u, _ = orc.surfdisp96(thk, vp, vs, rho, PERIODS, iflsph=iflsph, iwave=1, igr=1)
+    for k, T in enumerate(PERIODS):
+        assert abs(orc.slegn96(thk, vs, rho, T, c[k], iflsph=iflsph)["cg"] - u[k]) < 2e-4 * u[k]
+    T = 20.0
+    o = orc.slegn96(thk, vs, rho, T, c[2], iflsph=iflsph)
+    for which, key in (("b", "dc2db"), ("r", "dc2dr")):
+        fd = _love_fd(orc, model, T, 0, which, 1e-3, iflsph)
+        assert np.max(np.abs(fd - o[key][:4])) <= 1e-2 * np.max(np.abs(fd))
+
+
+@pytest.mark.parametrize("iflsph", [0, 1])
+def test_slegnpu_love_group_kernels_match_fd(orc, iflsph):
+    """slegnpu (src/surfker/slegn96.f90:785-919): du/db, du/drho against
+    central differences of surfdisp96's Love group velocity (itself a
+    difference in period), 3e-2 of the largest layer value."""
+    import ctypes as C
+    model = _surfdisp_test_model()
+    thk, vp, vs, rho = model
+    T = 20.0
+    Ts = np.array([T, T * 1.005, T * 0.995])
+    c3, _ = orc.surfdisp96(thk, vp, vs, rho, Ts, iflsph=iflsph, iwave=1)
+    n = len(thk)
+    kb, kr, cg = np.zeros(n), np.zeros(n), C.c_double()
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    orc.lib().orc_slegnpu(f(thk), f(vs), f(rho), n, Ts[0], c3[0], Ts[1], c3[1], Ts[2], c3[2],
+                          C.byref(cg), kb, kr, iflsph)
+    for which, k in (("b", kb), ("r", kr)):
+        fd = _love_fd(orc, model, T, 1, which, 1e-2, iflsph)
+        assert np.max(np.abs(fd - k[:4])) <= 3e-2 * np.max(np.abs(fd))
