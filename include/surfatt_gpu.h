@@ -300,6 +300,22 @@ int sa_pde_smooth(sa_ctx* ctx, int nx, int ny, int nz, double dx_deg, double dy_
                   double dz_km, const double* ygrid, const double* zgrid, double sigma_h,
                   double sigma_v, double* field, double* work, int* nstep_out, void* stream);
 
+/* Multigrid smoothing, the reference's smooth_method 1
+ * (PostProc::InvGrid::init / fwd2inv / inv2fwd, src/postproc.cpp:160-386;
+ * PostProc::smooth, :465-480): nset staggered coarse grids of n_inv[0..2] +
+ * 2 nodes over the model grid x[nx] (deg), y[ny] (deg), z[nz] (km) (host
+ * arrays); sa_multigrid_smooth projects a (nx, ny, nz) row-major device field
+ * onto them and interpolates back, averaged over the sets, into out (device,
+ * not aliasing field).  As the reference computes it: the projection adds
+ * each fine node to a single corner, and the coarse index uses the inner
+ * counts as strides.  Equal bit for bit to a CPU evaluation.  SA_ERR_ARG when
+ * a node lies outside a coarse grid (the reference aborts). */
+typedef struct sa_multigrid sa_multigrid;
+int sa_multigrid_create(int device, int nx, int ny, int nz, const double* x, const double* y,
+                        const double* z, const int* n_inv, int nset, sa_multigrid** out);
+void sa_multigrid_destroy(sa_multigrid* mg);
+int sa_multigrid_smooth(sa_multigrid* mg, const double* field, double* out, void* stream);
+
 /* ---- observation table and event builder (host only) ----------------------- */
 
 /* SrcRec::load with get_periods and get_events (reference src/src_rec.cpp:20-228,

@@ -192,6 +192,12 @@ int orc_depthkernel_love(int nx, int ny, int nz, const double* zgrid, const doub
                          int nper, const double* periods, int igr, double* sen_vs,
                          double* sen_rho, int* status, int nthreads);
 
+/* PostProc::smooth, smooth_method 1 (src/postproc.cpp:160-386, :465-480):
+ * buf, out (nx, ny, nz) row-major; -1 when a node lies outside. */
+int orc_multigrid_smooth(int nx, int ny, int nz, const double* x, const double* y,
+                         const double* z, const int* n_inv, int nset, const double* buf,
+                         double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,8 @@ def _declare(L):
     L.orc_slegn96.argtypes = [_fp, _fp, _fp, i, d, d, C.POINTER(d), _dp, _dp, i]
     L.orc_slegnpu.argtypes = [_fp, _fp, _fp, i, d, d, d, d, d, d, C.POINTER(d), _dp, _dp, i]
     L.orc_depthkernel_love.argtypes = [i, i, i, _dp, _dp, i, _dp, i, _dp, _dp, _ip, i]
+    L.orc_multigrid_smooth.argtypes = [i, i, i, _dp, _dp, _dp, _ip, i, _dp, _dp]
+    L.orc_multigrid_smooth.restype = i
     L.orc_combine_kernels_vs.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
     for f in ("orc_vs2vp", "orc_vp2rho", "orc_dalpha_dbeta", "orc_drho_dalpha"):
         getattr(L, f).argtypes = [d]
@@ -410,3 +412,14 @@ def slegn96(thk, vs, rho, t, cp, iflsph=1):
     lib().orc_slegn96(f(thk), f(vs), f(rho), n, float(t), float(cp), C.byref(cg), kb, kr,
                       int(iflsph))
     return dict(dc2db=kb, dc2dr=kr, cg=cg.value)
+
+
+def multigrid_smooth(field, x, y, z, n_inv, nset):
+    """PostProc::smooth with smooth_method 1 on a (nx, ny, nz) field."""
+    f = _c(field)
+    out = np.zeros_like(f)
+    rc = lib().orc_multigrid_smooth(f.shape[0], f.shape[1], f.shape[2], _c(x), _c(y), _c(z),
+                                    _c(n_inv, np.int32), int(nset), f, out)
+    if rc != 0:
+        raise ValueError("a node lies outside a coarse grid")
+    return out

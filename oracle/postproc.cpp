@@ -111,3 +111,127 @@ extern "C" int orc_pde_smooth(int nx, int ny, int nz, double dx, double dy, doub
     std::copy(u.begin(), u.end(), field);
     return 0;
 }
+
+// ---- multigrid smoothing (smooth_method 1) --------------------------------
+// PostProc::InvGrid::init / fwd2inv / inv2fwd (src/postproc.cpp:160-386) and
+// PostProc::smooth (:465-480): nset staggered coarse grids of
+// (n_inv + 2) nodes per axis; the field is projected onto them and
+// interpolated back, averaged over the sets.  Kept as the reference has it:
+// fwd2inv adds each fine node to one corner only (the one of n = 7: its
+// accumulation sits after the corner loop), and the coarse index uses the
+// inner counts n_inv_J, n_inv_K as strides (I2V_INV_GRIDS,
+// include/postproc.h:53-55).
+namespace {
+int locate_bissection(const double* v, int n, double x) {   // include/utils.h:39-60
+    int low = 0, high = n - 1;
+    if (x < v[0] || x > v[n - 1]) return -1;
+    while (high - low > 1) {
+        const int mid = (high + low) / 2;
+        if (v[mid] > x) high = mid;
+        else low = mid;
+    }
+    if (x == v[0]) return 0;
+    if (x == v[n - 1]) return n - 2;
+    return low;
+}
+
+struct InvGrid {
+    int nI, nJ, nK, nset;
+    std::vector<double> xinv, yinv, zinv;   // [set][node]
+    int idx(int A, int B, int C, int D) const { return A * nK * nJ * nset + B * nK * nset + C * nset + D; }
+};
+
+InvGrid inv_grid_init(const double* x, int nx, const double* y, int ny, const double* z, int nz,
+                      const int* n_inv, int nset) {
+    InvGrid G{n_inv[0], n_inv[1], n_inv[2], nset, {}, {}, {}};
+    auto axis = [&](const double* g, int n, int ninner, std::vector<double>& out) {
+        const int m = ninner + 2;
+        const double g0 = g[0], g1 = g[n - 1];
+        const double d = (g1 - g0) / ninner;
+        const double add = d / nset;
+        const double beg = g0 - add, end = g1 + add;
+        out.assign((size_t)m * nset, 0.0);
+        for (int is = 0; is < nset; ++is) {
+            double* o = out.data() + (size_t)is * m;
+            o[0] = beg;
+            o[m - 1] = end;
+            for (int j = 1; j < m - 1; ++j) o[j] = (g0 + (j - 1) * d) + is * add;
+        }
+    };
+    axis(x, nx, G.nI, G.xinv);
+    axis(y, ny, G.nJ, G.yinv);
+    axis(z, nz, G.nK, G.zinv);
+    return G;
+}
+}  // namespace
+
+// buf, out: (nx, ny, nz) row-major.  Returns -1 when a node lies outside a
+// coarse grid (the reference aborts).
+extern "C" int orc_multigrid_smooth(int nx, int ny, int nz, const double* x, const double* y,
+                                    const double* z, const int* n_inv, int nset,
+                                    const double* buf, double* out) {
+    const InvGrid G = inv_grid_init(x, nx, y, ny, z, nz, n_inv, nset);
+    const int mx = G.nI + 2, my = G.nJ + 2, mz = G.nK + 2;
+    const size_t ngrid = (size_t)mx * my * mz * nset;
+    std::vector<double> tmp(ngrid, 0.0), weight(ngrid, 0.0), arr(ngrid, 0.0);
+    for (int ig = 0; ig < nset; ++ig) {
+        const double* xi = G.xinv.data() + (size_t)ig * mx;
+        const double* yi = G.yinv.data() + (size_t)ig * my;
+        const double* zi = G.zinv.data() + (size_t)ig * mz;
+        for (int i = 0; i < nx; ++i) {
+            const int ix = locate_bissection(xi, mx, x[i]);
+            if (ix < 0) return -1;
+            const double wx = (x[i] - xi[ix]) / (xi[ix + 1] - xi[ix]);
+            for (int j = 0; j < ny; ++j) {
+                const int iy = locate_bissection(yi, my, y[j]);
+                if (iy < 0) return -1;
+                const double wy = (y[j] - yi[iy]) / (yi[iy + 1] - yi[iy]);
+                for (int k = 0; k < nz; ++k) {
+                    const int iz = locate_bissection(zi, mz, z[k]);
+                    if (iz < 0) return -1;
+                    const double wz = (z[k] - zi[iz]) / (zi[iz + 1] - zi[iz]);
+                    const int m = G.idx(ix + 1, iy, iz + 1, ig);   // the n = 7 corner
+                    const double wt = wx * (1.0 - wy) * wz;
+                    weight[m] += wt;
+                    tmp[m] += wt * buf[((size_t)i * ny + j) * nz + k];
+                }
+            }
+        }
+    }
+    for (size_t i = 0; i < ngrid; ++i) arr[i] = weight[i] > 0.0 ? tmp[i] / weight[i] : 0.0;
+    for (size_t i = 0; i < (size_t)nx * ny * nz; ++i) out[i] = 0.0;
+    for (int ig = 0; ig < nset; ++ig) {
+        const double* xi = G.xinv.data() + (size_t)ig * mx;
+        const double* yi = G.yinv.data() + (size_t)ig * my;
+        const double* zi = G.zinv.data() + (size_t)ig * mz;
+        for (int i = 0; i < nx; ++i) {
+            const int ix = locate_bissection(xi, mx, x[i]);
+            const double wx = (x[i] - xi[ix]) / (xi[ix + 1] - xi[ix]);
+            for (int j = 0; j < ny; ++j) {
+                const int iy = locate_bissection(yi, my, y[j]);
+                const double wy = (y[j] - yi[iy]) / (yi[iy + 1] - yi[iy]);
+                for (int k = 0; k < nz; ++k) {
+                    const int iz = locate_bissection(zi, mz, z[k]);
+                    const double wz = (z[k] - zi[iz]) / (zi[iz + 1] - zi[iz]);
+                    const int c[8][3] = {{ix, iy, iz},         {ix, iy + 1, iz},
+                                         {ix + 1, iy + 1, iz}, {ix + 1, iy, iz},
+                                         {ix, iy, iz + 1},     {ix, iy + 1, iz + 1},
+                                         {ix + 1, iy + 1, iz + 1}, {ix + 1, iy, iz + 1}};
+                    const double w[8] = {(1.0 - wx) * (1.0 - wy) * (1.0 - wz),
+                                         (1.0 - wx) * wy * (1.0 - wz),
+                                         wx * wy * (1.0 - wz),
+                                         wx * (1.0 - wy) * (1.0 - wz),
+                                         (1.0 - wx) * (1.0 - wy) * wz,
+                                         (1.0 - wx) * wy * wz,
+                                         wx * wy * wz,
+                                         wx * (1.0 - wy) * wz};
+                    double val = 0.0;
+                    for (int n = 0; n < 8; ++n) val += w[n] * arr[G.idx(c[n][0], c[n][1], c[n][2], ig)];
+                    out[((size_t)i * ny + j) * nz + k] += val;
+                }
+            }
+        }
+    }
+    for (size_t i = 0; i < (size_t)nx * ny * nz; ++i) out[i] = out[i] / static_cast<double>(nset);
+    return 0;
+}

@@ -33,7 +33,8 @@ EXPORTED = (
     "sa_grad_set_data_type", "sa_plan_kden_output", "sa_grad_set_kden", "sa_grad_ker_den",
     "sa_kernel_precondition", "sa_multi_create", "sa_multi_destroy",
     "sa_multi_forward_adjoint", "sa_multi_kernel_ms", "sa_multi_status",
-    "sa_depthkernel_columns_love", "sa_grad_set_wave_type",
+    "sa_depthkernel_columns_love", "sa_grad_set_wave_type", "sa_multigrid_create",
+    "sa_multigrid_destroy", "sa_multigrid_smooth",
     "sa_grad_create", "sa_grad_destroy", "sa_grad_run", "sa_grad_sen", "sa_grad_combine",
     "sa_pde_smooth_nstep", "sa_pde_smooth",
     "sa_lbfgs_create", "sa_lbfgs_destroy", "sa_lbfgs_store", "sa_lbfgs_direction", "sa_dot",
@@ -108,6 +109,9 @@ def lib():
     L.sa_plan_set_deterministic.argtypes = [_vp, i, C.c_size_t]
     L.sa_grad_set_data_type.argtypes = [_vp, i]
     L.sa_grad_set_wave_type.argtypes = [_vp, i]
+    L.sa_multigrid_create.argtypes = [i, i, i, i, _dp, _dp, _dp, _ip, i, C.POINTER(_vp)]
+    L.sa_multigrid_destroy.argtypes = [_vp]
+    L.sa_multigrid_smooth.argtypes = [_vp, _vp, _vp, _vp]
     L.sa_plan_kden_output.argtypes = [_vp, _vp]
     L.sa_grad_set_kden.argtypes = [_vp, i]
     L.sa_grad_ker_den.argtypes = [_vp] * 4 + [_vp]

@@ -6,6 +6,7 @@ Each translation unit gets the flags its arithmetic contract needs:
   eik32.cu   fast FP32 division/sqrt, FTZ: the FP32 sweep path
   surfker*.cu -fmad=false: surfdisp96 / sregn96 operation for operation
   postproc.cu -fmad=false: PDE smoothing rounds as the reference's FP64
+  multigrid.cu -fmad=false: multigrid smoothing, likewise
   others     default IEEE flags
 """
 from __future__ import annotations
@@ -32,6 +33,7 @@ UNITS = {
     "capi.cu": ["-Xcompiler", "-ffp-contract=off"],
     "noalloc.cu": ["-fmad=false"],
     "postproc.cu": ["-fmad=false"],
+    "multigrid.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
     "optimize.cu": ["-fmad=false"],
     "topo.cu": ["-fmad=false"],
     "srcrec.cpp": ["-Xcompiler", "-ffp-contract=off"],

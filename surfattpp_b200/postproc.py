@@ -71,3 +71,44 @@ def kernel_precondition(ker_den, ker, ctx=None, stream=None):
     rc = _capi.lib().sa_kernel_precondition(ctx.h, ker.numel(), ptr(ker_den), ptr(ker), stream)
     _capi.check(ctx.h, rc)
     return ker
+
+
+class MultigridSmoother:
+    """The reference's multigrid smoothing (smooth_method 1,
+    PostProc::InvGrid, src/postproc.cpp:160-386): nset staggered coarse grids
+    of n_inv + 2 nodes per axis over the model grid; ``smooth`` projects a
+    (nx, ny, nz) device field onto them and interpolates back
+    (sa_multigrid_*)."""
+
+    def __init__(self, xgrid, ygrid, zgrid, n_inv, nset, device=0):
+        x = np.ascontiguousarray(xgrid, np.float64)
+        y = np.ascontiguousarray(ygrid, np.float64)
+        z = np.ascontiguousarray(zgrid, np.float64)
+        ni = np.ascontiguousarray(n_inv, np.int32)
+        h = C.c_void_p()
+        rc = _capi.lib().sa_multigrid_create(int(device), x.size, y.size, z.size, x, y, z, ni,
+                                             int(nset), C.byref(h))
+        if rc != _capi.SA_OK:
+            raise _capi.SAError(rc, "sa_multigrid_create")
+        self.h = h
+        self.shape = (x.size, y.size, z.size)
+
+    def smooth(self, field, out=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty_like(field)
+        rc = _capi.lib().sa_multigrid_smooth(self.h, ptr(field), ptr(out), stream)
+        if rc != _capi.SA_OK:
+            raise _capi.SAError(rc, "sa_multigrid_smooth")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().sa_multigrid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
