@@ -303,10 +303,14 @@ class Inversion:
         kden: kernel-density preconditioning of every type's kernel before
         the smoothing (postproc::kernel_precondition, src/postproc.cpp:
         487-517; the reference's is_kden).
-        autograd: take the kernel as the torch.autograd gradient of chi built
-        in torch on TravelTimes (forward: receiver times, nothing stored;
-        backward: every forward field recomputed, the adjoint driven by
-        w (T - Tobs)) -- the reference's kernel, one extra forward pass."""
+        autograd: take the kernel as a torch.autograd gradient.  True: chi
+        built in torch on TravelTimes (forward: receiver times, nothing
+        stored; backward: every forward field recomputed, the adjoint driven
+        by w (T - Tobs)) -- the reference's kernel, one extra forward pass.
+        "fused": chi from TravelTimeMisfit, whose forward is the one fused
+        forward-residual-adjoint pass of the reference and whose backward
+        scales the stored kernel -- the same kernel at the cost of the
+        plain evaluation."""
         self.g = grad
         self.tt, self.wt = tt_obs, weight
         self.smooth = smooth
@@ -316,7 +320,9 @@ class Inversion:
         self.w = data_weight
         self.data = [(grad, tt_obs, weight, data_weight)] + list(more_data or [])
         self._outs = [None] * len(self.data)
-        self.autograd = bool(autograd)
+        if autograd not in (False, True, "fused"):
+            raise ValueError("autograd must be False, True or 'fused'")
+        self.autograd = autograd
         self.kden = bool(kden)
         if self.kden:
             if self.autograd:
@@ -335,7 +341,13 @@ class Inversion:
         from . import postproc
         total, ker_curr, grad = 0.0, None, None
         for i, (g, tt, wt, dw) in enumerate(self.data):
-            if self.autograd:
+            if self.autograd == "fused":
+                v = vs.detach().clone().requires_grad_(True)
+                c = TravelTimeMisfit.apply(g, v, tt, wt)
+                c.backward()
+                out = g.last
+                ker = v.grad
+            elif self.autograd:
                 v = vs.detach().clone().requires_grad_(True)
                 c = misfit(g, v, tt, wt)
                 c.backward()

@@ -131,7 +131,7 @@ def _oracle_inversion(orc, w, ev, vs0, smooth, niter, step=0.02, max_sub=10):
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("autograd", [False, True])
+@pytest.mark.parametrize("autograd", [False, True, "fused"])
 def test_lbfgs_inversion_follows_oracle(gpu, orc, autograd):
     import torch
     from surfattpp_b200 import inversion, preproc
@@ -151,7 +151,8 @@ def test_lbfgs_inversion_follows_oracle(gpu, orc, autograd):
                                       ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
                                       ev["stla"], precision="fp64")
     g = inversion.MisfitGradient(plan, w.zgrid, w.periods)
-    # autograd: the kernel as the backward of TravelTimeMisfit (same evaluation)
+    # autograd True: the kernel as the backward of chi built in torch on
+    # TravelTimes; "fused": the backward of TravelTimeMisfit (same evaluation)
     inv = inversion.Inversion(g, _t(ev["tt_obs"]), _t(ev["weight"]), smooth=smooth, niter=niter,
                               autograd=autograd)
     vs = inv.run(_t(vs0))
