@@ -38,16 +38,21 @@ def fwdsurf(zgrid, vs3d, periods, iwave=2, igr=0, ctx=None, stream=None, check=T
     return svel, status
 
 
-def depthkernel_hti(zgrid, vs3d, periods, cp, ctx=None, stream=None):
+def depthkernel_hti(zgrid, vs3d, periods, cp, ctx=None, stream=None, out=None):
     """Rayleigh phase-velocity depth kernels (nx, ny, nz, nper) x 3 at the
-    phase velocities cp (nper, ny, nx) from fwdsurf(igr=0)."""
+    phase velocities cp (nper, ny, nx) from fwdsurf(igr=0); `out` (three
+    such float64 device tensors) is reused when given."""
     import torch
     ctx = ctx or default_context()
     nx, ny, nz = vs3d.shape
     p = np.ascontiguousarray(periods, dtype=np.float64)
     z = np.ascontiguousarray(zgrid, dtype=np.float64)
     shp = (nx, ny, nz, p.size)
-    out = [torch.empty(shp, dtype=torch.float64, device=vs3d.device) for _ in range(3)]
+    if out is None:
+        out = [torch.empty(shp, dtype=torch.float64, device=vs3d.device) for _ in range(3)]
+    elif any(tuple(o.shape) != shp or o.dtype != torch.float64 or not o.is_contiguous()
+             for o in out):
+        raise ValueError("out: three contiguous float64 tensors of shape (nx, ny, nz, nper)")
     rc = _capi.lib().sa_depthkernel_columns(ctx.h, nx, ny, nz, z, ptr(vs3d), p.size, p, ptr(cp),
                                             ptr(out[0]), ptr(out[1]), ptr(out[2]), stream)
     _capi.check(ctx.h, rc)
