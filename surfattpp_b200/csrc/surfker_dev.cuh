@@ -48,9 +48,10 @@ struct LayerConst {
 // includes this header picks per group: surfker.cu takes the transcendentals,
 // dltar4, the eigenfunction routines and the complex division out of line
 // (smaller instruction footprint, bit-identical results); surfker_group.cu
-// keeps everything inline, because the group-velocity kernel returned wrong
-// dU/dvp values with out-of-line routines (dU/dvs, dU/drho right; cause not
-// found).  SK_NOINLINE marks the routines that stay inline everywhere
+// keeps everything inline, because with layer_integrals out of line the
+// group-velocity kernel's saved first-evaluation kernels come back
+// overwritten on the device (see surfker_group.cu).  SK_NOINLINE marks the
+// routines that stay inline everywhere
 // (dltar1, nevill, getsol: out of line they cost more than they save).
 #ifndef SK_NOINLINE
 #define SK_NOINLINE inline

@@ -1,8 +1,13 @@
 // Group-velocity depth kernels (sregnpu), in a translation unit of their
-// own: here the FP64 transcendentals stay inline.  With the out-of-line copies
-// the other column kernels use, this kernel returned wrong dU/dvp values
-// (dU/dvs, dU/drho and the phase kernels right; cause not found), so it keeps
-// the inline form, which matches the oracle.  Compiled with -fmad=false.
+// own where every shared routine stays inline.  With layer_integrals out of
+// line (as the other column kernels have it), the kernels of the first
+// evaluation, held in local arrays while the two later evaluations run, come
+// back overwritten on the device (dU/dvp wrong by 1e-8 of the column
+// maximum, by 1e4 with all eigenfunction routines out of line; dU/dvs and
+// dU/drho exact).  The same source built for the host, inline or out of
+// line, is exact, and neither the stack limit, the callee's spills nor FMA
+// contraction change it.  The inline form matches the oracle bit for bit.
+// Compiled with -fmad=false.
 #define SK_MATH_NOINLINE 0
 #include "surfker_dev.cuh"
 
