@@ -5,6 +5,7 @@
 // -ffp-contract=off, each intermediate rounds exactly as the reference source
 // reads.  Citations are to the reference project.
 #include "oracle.h"
+#include "eik_state.h"
 
 #include <algorithm>
 #include <cmath>
@@ -28,14 +29,16 @@ inline double bilinear(const double* M, int nx, int idx0, int idy0, double r1, d
 
 }  // namespace
 
-// src/eikonal_solver.cpp:22-318
-extern "C" int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* yy_deg,
-                           const double* spha, const double* sphb, const double* sphc,
-                           const double* fun, double x0_deg, double y0_deg,
-                           double* T_out, int* niter) {
+// src/eikonal_solver.cpp:22-318, with the stopping rule as a parameter:
+// tol > 0 stops as the reference (L1 and Linf of the change below tol,
+// reference value 1e-4); tol == 0 iterates to a fixed point (an iteration
+// that changes no cell).  `st` (optional) receives the converged state for
+// the discrete adjoint (eikonal_discrete.cpp).
+int eik_fwd_core(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                 const double* spha, const double* sphb, const double* sphc, const double* fun,
+                 double x0_deg, double y0_deg, double TOL, int MAXITER, double* T_out,
+                 int* niter, EikState* st) {
     if (nx < 3 || ny < 3) return -1;
-    const int MAXITER = 2000;
-    const double TOL = 1e-4;
     const int n = nx * ny;
 
     std::vector<double> xx(nx), yy(ny);
@@ -70,7 +73,7 @@ extern "C" int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* y
     const double fun0 = bilinear(fun, nx, idx0, idy0, r1, r2);
 
     // :91-131
-    std::vector<double> T0(n), T0x(n), T0y(n), tau(n);
+    std::vector<double> T0(n), T0x(n), T0y(n), tau(n), G(n), Gx(n), Gy(n);
     std::vector<unsigned char> ischange(n, 1);
     for (int ix = 0; ix < nx; ix++) {
         for (int iy = 0; iy < ny; iy++) {
@@ -79,16 +82,23 @@ extern "C" int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* y
             const double tmp = std::sin(yy[iy]) * std::sin(y0)
                              + std::cos(yy[iy]) * std::cos(y0) * std::cos(dlon);
             const double tmp_c = std::max(-1.0, std::min(1.0, tmp));
-            T0[k] = std::acos(tmp_c) * R_EARTH * fun0;
+            // T0 = G fun0 etc., the products associated as the reference
+            // writes them (fun0 multiplies last)
+            G[k] = std::acos(tmp_c) * R_EARTH;
+            T0[k] = G[k] * fun0;
             const double sin_d = std::sqrt(std::max(0.0, 1.0 - tmp_c * tmp_c));
             if (sin_d < 1e-14) {
+                Gx[k] = 0.0;
+                Gy[k] = 0.0;
                 T0x[k] = 0.0;
                 T0y[k] = 0.0;
             } else {
-                T0x[k] = std::cos(yy[iy]) * std::cos(y0) * std::sin(dlon) / sin_d * R_EARTH * fun0;
-                T0y[k] = -(std::cos(yy[iy]) * std::sin(y0)
-                           - std::sin(yy[iy]) * std::cos(y0) * std::cos(dlon))
-                         / sin_d * R_EARTH * fun0;
+                Gx[k] = std::cos(yy[iy]) * std::cos(y0) * std::sin(dlon) / sin_d * R_EARTH;
+                Gy[k] = -(std::cos(yy[iy]) * std::sin(y0)
+                          - std::sin(yy[iy]) * std::cos(y0) * std::cos(dlon))
+                        / sin_d * R_EARTH;
+                T0x[k] = Gx[k] * fun0;
+                T0y[k] = Gy[k] * fun0;
             }
             if (std::abs((xx[ix] - x0) / dx) <= 1.0 && std::abs((yy[iy] - y0) / dy) <= 1.0) {
                 tau[k] = 1.0;
@@ -224,11 +234,49 @@ extern "C" int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* y
                 Linf_dif = std::max(Linf_dif, d);
             }
         L1_dif /= static_cast<double>(nx * ny);
-        if (L1_dif < TOL && Linf_dif < TOL) break;
+        if (TOL > 0.0 ? (L1_dif < TOL && Linf_dif < TOL) : (tau == tau_old)) break;
     }
     if (niter) *niter = iters_run;
     for (int k = 0; k < n; k++) T_out[k] = tau[k] * T0[k];
+    if (st) {
+        st->nx = nx;
+        st->ny = ny;
+        st->dx = dx;
+        st->dy = dy;
+        st->fun0 = fun0;
+        st->idx0 = idx0;
+        st->idy0 = idy0;
+        st->r1 = r1;
+        st->r2 = r2;
+        st->a = std::move(a);
+        st->b = std::move(b);
+        st->c = std::move(c);
+        st->T0 = std::move(T0);
+        st->T0x = std::move(T0x);
+        st->T0y = std::move(T0y);
+        st->G = std::move(G);
+        st->Gx = std::move(Gx);
+        st->Gy = std::move(Gy);
+        st->tau = std::move(tau);
+        st->ischange = std::move(ischange);
+    }
     return 0;
+}
+
+extern "C" int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                           const double* spha, const double* sphb, const double* sphc,
+                           const double* fun, double x0_deg, double y0_deg,
+                           double* T_out, int* niter) {
+    return eik_fwd_core(nx, ny, xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg, y0_deg, 1e-4,
+                        2000, T_out, niter, nullptr);
+}
+
+extern "C" int orc_eik_fwd_tol(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                               const double* spha, const double* sphb, const double* sphc,
+                               const double* fun, double x0_deg, double y0_deg, double tol,
+                               int maxiter, double* T_out, int* niter) {
+    return eik_fwd_core(nx, ny, xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg, y0_deg, tol,
+                        maxiter, T_out, niter, nullptr);
 }
 
 // src/eikonal_solver.cpp:323-511

@@ -32,6 +32,34 @@ int orc_eik_fwd(int nx, int ny, const double* xx_deg, const double* yy_deg,
                 const double* spha, const double* sphb, const double* sphc,
                 const double* fun, double x0_deg, double y0_deg,
                 double* T_out, int* niter);
+/* The forward solve with the stopping rule as a parameter: tol > 0 as the
+ * reference (1e-4), tol == 0 to a fixed point (no cell changes). */
+/* Derivatives of surfdisp96's Rayleigh phase velocities c[kmax] with
+ * respect to each layer's vs, vp, rho ([k * nlayer + layer]). */
+int orc_dispersion_dcdm(const float* thkm, const float* vpm, const float* vsm, const float* rhom,
+                        int nlayer, int kmax, const double* t, const double* c, double* dcdb,
+                        double* dcda, double* dcdr);
+int orc_eik_fwd_tol(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                    const double* spha, const double* sphb, const double* sphc, const double* fun,
+                    double x0_deg, double y0_deg, double tol, int maxiter, double* T_out,
+                    int* niter);
+/* Exact discrete adjoint of the forward solve (eikonal_discrete.cpp):
+ * receiver times syn[nr] and, with dchi_dT[nr], grad_fun = dchi/dfun. */
+int orc_eik_discrete_grad(int nx, int ny, const double* xx_deg, const double* yy_deg,
+                          const double* spha, const double* sphb, const double* sphc,
+                          const double* fun, double x0_deg, double y0_deg, double tol,
+                          int maxiter, int nr, const double* xrec_deg, const double* yrec_deg,
+                          const double* dchi_dT, double* syn, double* grad_fun, int* niter);
+/* All events with the discrete gradient: grad_svel [nper][ny][nx] +=
+ * dchi/dsvel, chi, syn (sadj: a vector-Jacobian product instead). */
+int orc_discrete_for_events(int nx, int ny, int nper, const double* xx_deg, const double* yy_deg,
+                            const double* svel, const double* m11, const double* m12,
+                            const double* m22, int ne, const double* evlo, const double* evla,
+                            const int* iper, const int* rec_ptr, const int* rec_idx,
+                            const double* stlo, const double* stla, const double* tt_obs,
+                            const double* weight, const double* sadj, double tol, int maxiter,
+                            double* syn, double* grad_svel, double* chi, int* fwd_iters,
+                            int nthreads);
 
 /* eikonal::FSM_O1_JSE_lonlat_2d (src/eikonal_solver.cpp:323-511). */
 int orc_eik_adj(int nx, int ny, const double* xx_deg, const double* yy_deg,

@@ -86,6 +86,18 @@ def _declare(L):
     L.orc_eik_adj.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp,
                               C.POINTER(i)]
     L.orc_eik_adj.restype = i
+    L.orc_eik_fwd_tol.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, d, i, _dp,
+                                  C.POINTER(i)]
+    L.orc_eik_fwd_tol.restype = i
+    L.orc_eik_discrete_grad.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, d, i, i, _dp,
+                                        _dp, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(i)]
+    L.orc_eik_discrete_grad.restype = i
+    L.orc_discrete_for_events.argtypes = [i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _dp, _dp,
+                                          _ip, _ip, _ip, _dp, _dp, C.c_void_p, _dp, C.c_void_p,
+                                          d, i, _dp, C.c_void_p, C.POINTER(d), _ip, i]
+    L.orc_discrete_for_events.restype = i
+    L.orc_dispersion_dcdm.argtypes = [_fp, _fp, _fp, _fp, i, i, _dp, _dp, _dp, _dp, _dp]
+    L.orc_dispersion_dcdm.restype = i
     L.orc_mask_uniform_grid.argtypes = [i, i, _dp, _dp, _dp, d, d]
     L.orc_interp2d.argtypes = [i, i, _dp, _dp, _dp, i, _dp, _dp, _dp]
     L.orc_forward_for_events.argtypes = [i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, i, _dp, _dp,
@@ -145,6 +157,72 @@ def eik_fwd(xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg, y0_deg):
     if rc != 0:
         raise ValueError("Grid must be at least 3x3")
     return T, it.value
+
+
+def eik_fwd_tol(xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg, y0_deg, tol=0.0,
+                maxiter=5000):
+    """The forward solve with its stopping rule as a parameter (tol 0: to a
+    fixed point).  Returns (T, niter)."""
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    nx, ny = xx.size, yy.size
+    T = np.zeros((ny, nx))
+    it = C.c_int(0)
+    rc = lib().orc_eik_fwd_tol(nx, ny, xx, yy, _c(spha), _c(sphb), _c(sphc), _c(fun),
+                               float(x0_deg), float(y0_deg), float(tol), int(maxiter), T,
+                               C.byref(it))
+    if rc != 0:
+        raise ValueError("Grid must be at least 3x3")
+    return T, it.value
+
+
+def eik_discrete_grad(xx_deg, yy_deg, spha, sphb, sphc, fun, x0_deg, y0_deg, xrec, yrec,
+                      dchi_dT, tol=0.0, maxiter=5000):
+    """Exact discrete adjoint of the forward solve: (syn [nr], dchi/dfun
+    (ny, nx), niter) for the receiver-time sensitivities dchi_dT [nr]."""
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    nx, ny = xx.size, yy.size
+    xr, yr, dd = _c(xrec).ravel(), _c(yrec).ravel(), _c(dchi_dT).ravel()
+    syn = np.zeros(max(xr.size, 1))
+    g = np.zeros((ny, nx))
+    it = C.c_int(0)
+    rc = lib().orc_eik_discrete_grad(nx, ny, xx, yy, _c(spha), _c(sphb), _c(sphc), _c(fun),
+                                     float(x0_deg), float(y0_deg), float(tol), int(maxiter),
+                                     xr.size, xr if xr.size else np.zeros(1),
+                                     yr if yr.size else np.zeros(1),
+                                     dd.ctypes.data if dd.size else None, syn.ctypes.data,
+                                     g.ctypes.data, C.byref(it))
+    if rc == -1:
+        raise ValueError("Grid must be at least 3x3")
+    if rc == -2:
+        raise RuntimeError("forward solve did not reach its stopping rule")
+    return syn[:xr.size], g, it.value
+
+
+def discrete_for_events(xx_deg, yy_deg, svel, m11, m12, m22, ev, tol=0.0, maxiter=5000,
+                        grad=True, sadj=None, nthreads=1):
+    """The event batch with the exact discrete gradient: dict(syn, chi,
+    grad_svel (nper, ny, nx) = dchi/dsvel, fwd_iters).  With sadj [npair],
+    grad_svel is the vector-Jacobian product of the receiver times with it."""
+    xx, yy = _c(xx_deg), _c(yy_deg)
+    nper, ny, nx = svel.shape
+    ne = len(ev["evlo"])
+    nrec = int(ev["rec_ptr"][-1])
+    syn = np.zeros(max(nrec, 1))
+    g = np.zeros((nper, ny, nx)) if grad else None
+    chi = C.c_double(0.0)
+    fi = np.zeros(max(ne, 1), np.int32)
+    tt = _c(ev["tt_obs"]) if ev.get("tt_obs") is not None else None
+    sa = _c(sadj) if sadj is not None else None
+    rc = lib().orc_discrete_for_events(
+        nx, ny, nper, xx, yy, _c(svel), _c(m11), _c(m12), _c(m22), ne, _c(ev["evlo"]),
+        _c(ev["evla"]), _c(ev["iper"], np.int32), _c(ev["rec_ptr"], np.int32),
+        _c(ev["rec_idx"], np.int32), _c(ev["stlo"]), _c(ev["stla"]),
+        tt.ctypes.data if tt is not None else None, _c(ev["weight"]),
+        sa.ctypes.data if sa is not None else None, float(tol), int(maxiter), syn,
+        g.ctypes.data if g is not None else None, C.byref(chi), fi, int(nthreads))
+    if rc == -2:
+        raise RuntimeError("forward solve did not reach its stopping rule")
+    return dict(syn=syn[:nrec], chi=chi.value, grad_svel=g, fwd_iters=fi[:ne])
 
 
 def eik_adj(xx_deg, yy_deg, spha, sphb, sphc, T, xrec, yrec, sadj):
@@ -247,6 +325,19 @@ def surfdisp96(thk, vp, vs, rho, periods, iflsph=1, iwave=2, mode=1, igr=0):
                               _c(rho, np.float32), len(thk), iflsph, iwave, mode, igr, t.size,
                               t, cg)
     return cg, st
+
+
+def dispersion_dcdm(thk, vp, vs, rho, periods, c):
+    """dc/d(vs, vp, rho) of surfdisp96's Rayleigh phase velocities c at
+    `periods` for every layer: three arrays (nper, nlayer)."""
+    t, cc = _c(periods), _c(c)
+    n = len(thk)
+    out = [np.zeros((t.size, n)) for _ in range(3)]
+    rc = lib().orc_dispersion_dcdm(_c(thk, np.float32), _c(vp, np.float32), _c(vs, np.float32),
+                                   _c(rho, np.float32), n, t.size, t, cc, *out)
+    if rc:
+        raise ValueError("water layers are not supported")
+    return tuple(out)
 
 
 def sregn96_hti(thk, vp, vs, rho, t, cp, iflsph=1):

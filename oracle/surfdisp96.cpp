@@ -451,6 +451,179 @@ int getsol(Model& M, double t1, double& c1, double clow, double dc, double cm, f
 }  // namespace
 
 // surfdisp96.f:57-373
+// ---------------------------------------------------------------------------
+// Derivatives of the phase-velocity root (no reference counterpart: the
+// reference's kernels come from sregn96's energy integrals, which agree
+// with differences of surfdisp96's phase velocities only to about 1e-3).
+// The Rayleigh secular function of dltar4 is F = e_hs CA_{n} ... CA_0 u / N,
+// e_hs the half-space row vector, CA_m the 5x5 compound layer matrix
+// (dnka), u the first unit vector, N the product of the normc scalings.  At
+// the root F = 0, so with B_m = CA_{m-1} ... CA_0 u and e_{m+1} the
+// normalised row vector entering layer m,
+//   dF/dp_m = e_{m+1} (dCA_m/dp_m) B_m / (n_m ... n_0),
+//   dc/dp = -(dF/dp) / (dF/dc),
+// dCA_m/dp_m and de_hs/dp by central differences of the single layer's
+// matrix (relative step 1e-6), dF/dc by central differences of dltar4.
+// ---------------------------------------------------------------------------
+namespace {
+
+// the layer matrix of dltar4's loop (surfdisp96.f:840-889) from double
+// parameters
+void layer_ca(double a, double b, double rho, double d, double wvno, double omega,
+              double ca[5][5]) {
+    const double wvno2 = wvno * wvno;
+    const double xka = omega / a, xkb = omega / b;
+    const double t = b / omega;
+    const double gammk = 2.0 * t * t;
+    const double gam = gammk * wvno2;
+    const double ra = std::sqrt((wvno + xka) * std::abs(wvno - xka));
+    const double rb = std::sqrt((wvno + xkb) * std::abs(wvno - xkb));
+    const VarOut v = var(ra * d, rb * d, ra, rb, wvno, xka, xkb, d);
+    dnka(ca, wvno2, gam, gammk, rho, v);
+}
+
+// the half-space vector of dltar4 (surfdisp96.f:811-830)
+void halfspace_e(double a, double b, double rho, double wvno, double omega, double e[5]) {
+    const double wvno2 = wvno * wvno;
+    const double xka = omega / a, xkb = omega / b;
+    const double ra = std::sqrt((wvno + xka) * std::abs(wvno - xka));
+    const double rb = std::sqrt((wvno + xkb) * std::abs(wvno - xkb));
+    const double t = b / omega;
+    const double gammk = 2.0 * t * t;
+    const double gam = gammk * wvno2;
+    const double gamm1 = gam - 1.0;
+    e[0] = rho * rho * (gamm1 * gamm1 - gam * gammk * ra * rb);
+    e[1] = -(rho * ra);
+    e[2] = rho * (gamm1 - gammk * ra * rb);
+    e[3] = rho * rb;
+    e[4] = wvno2 - ra * rb;
+}
+
+}  // namespace
+
+// Rayleigh phase velocities c[kmax] (surfdisp96's roots for the unflattened
+// float layer model, iflsph 1) -> dc/d(vs, vp, rho) of every layer,
+// [k * nlayer + layer].  Returns 0, or 1 for a model with a water layer.
+extern "C" int orc_dispersion_dcdm(const float* thkm, const float* vpm, const float* vsm,
+                                   const float* rhom, int nlayer, int kmax, const double* t,
+                                   const double* c, double* dcdb, double* dcda, double* dcdr) {
+    Model M;
+    const int mmax = nlayer;
+    M.mmax = mmax;
+    M.d.assign(thkm, thkm + mmax);
+    M.a.assign(vpm, vpm + mmax);
+    M.b.assign(vsm, vsm + mmax);
+    M.rho.assign(rhom, rhom + mmax);
+    M.rtp.assign(mmax, 0.0f);
+    M.dtp.assign(mmax, 0.0f);
+    M.btp.assign(mmax, 0.0f);
+    M.dhalf = 0.0f;
+    M.llw = (M.b[0] <= 0.0f) ? 2 : 1;
+    if (M.llw != 1) return 1;
+    sphere(M, 0, 0);
+    sphere(M, 2, 1);
+    const double twopi = 2.0 * 3.141592653589793;
+    std::vector<double> ein(5 * static_cast<size_t>(mmax)), logn(mmax, 0.0);
+    for (int k = 0; k < kmax; k++) {
+        const double omega = std::max(twopi / t[k], 1.0e-4);
+        const double wvno = omega / c[k];
+        // forward pass of dltar4 keeping each layer's input vector and scale
+        double e[5], ee[5], ca[5][5];
+        halfspace_e(M.a[mmax - 1], M.b[mmax - 1], M.rho[mmax - 1], wvno, omega, e);
+        for (int m = mmax - 2; m >= 0; m--) {
+            for (int i = 0; i < 5; i++) ein[5 * m + i] = e[i];
+            layer_ca(M.a[m], M.b[m], M.rho[m], M.d[m], wvno, omega, ca);
+            double t1 = 0.0;
+            for (int i = 0; i < 5; i++) {
+                double cr = 0.0;
+                for (int j = 0; j < 5; j++) cr += e[j] * ca[j][i];
+                ee[i] = cr;
+                t1 = std::max(t1, std::abs(cr));
+            }
+            if (t1 < 1.e-40) t1 = 1.0;
+            for (int i = 0; i < 5; i++) e[i] = ee[i] / t1;
+            logn[m] = std::log(t1);
+        }
+        // dF/dc by central differences of the secular function
+        const double hc = 1e-7 * c[k];
+        const double Fc = (dltar4(M, omega / (c[k] + hc), omega)
+                           - dltar4(M, omega / (c[k] - hc), omega)) / (2.0 * hc);
+        // top-down vectors B_m (normalised, log scale LB) and the layer terms
+        double B[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
+        double LB = 0.0, LN = 0.0;   // log |B| scale, log (n_m ... n_0)
+        auto dF = [&](const double* row, const double dca[5][5]) {
+            double s = 0.0;
+            for (int i = 0; i < 5; i++) {
+                double r = 0.0;
+                for (int j = 0; j < 5; j++) r += dca[i][j] * B[j];
+                s += row[i] * r;
+            }
+            return s;
+        };
+        for (int m = 0; m <= mmax - 2; m++) {
+            LN += logn[m];
+            const double scale = std::exp(LB - LN);
+            const double p0[3] = {M.b[m], M.a[m], M.rho[m]};
+            double out[3];
+            for (int q = 0; q < 3; q++) {
+                double pp[3] = {p0[0], p0[1], p0[2]}, pm[3] = {p0[0], p0[1], p0[2]};
+                const double h = 1e-6 * p0[q];
+                pp[q] += h;
+                pm[q] -= h;
+                double cp[5][5], cm[5][5], dca[5][5];
+                layer_ca(pp[1], pp[0], pp[2], M.d[m], wvno, omega, cp);
+                layer_ca(pm[1], pm[0], pm[2], M.d[m], wvno, omega, cm);
+                for (int i = 0; i < 5; i++)
+                    for (int j = 0; j < 5; j++) dca[i][j] = (cp[i][j] - cm[i][j]) / (2.0 * h);
+                out[q] = -(dF(&ein[5 * m], dca) * scale) / Fc;
+            }
+            // unflattened parameters: b_f = b tmp, a_f = a tmp, rho_f = rho btp^-2.275
+            const double tmp = M.btp[m];
+            const size_t o = static_cast<size_t>(k) * mmax + m;
+            dcdb[o] = out[0] * tmp;
+            dcda[o] = out[1] * tmp;
+            dcdr[o] = out[2] * std::pow(M.btp[m], -2.275f);
+            // B_{m+1} = CA_m B_m
+            layer_ca(M.a[m], M.b[m], M.rho[m], M.d[m], wvno, omega, ca);
+            double nb[5], bm = 0.0;
+            for (int i = 0; i < 5; i++) {
+                double r = 0.0;
+                for (int j = 0; j < 5; j++) r += ca[i][j] * B[j];
+                nb[i] = r;
+                bm = std::max(bm, std::abs(r));
+            }
+            if (bm < 1e-300) bm = 1.0;
+            for (int i = 0; i < 5; i++) B[i] = nb[i] / bm;
+            LB += std::log(bm);
+        }
+        // the half-space layer
+        {
+            const int m = mmax - 1;
+            const double scale = std::exp(LB - LN);
+            const double p0[3] = {M.b[m], M.a[m], M.rho[m]};
+            double out[3];
+            for (int q = 0; q < 3; q++) {
+                double pp[3] = {p0[0], p0[1], p0[2]}, pm[3] = {p0[0], p0[1], p0[2]};
+                const double h = 1e-6 * p0[q];
+                pp[q] += h;
+                pm[q] -= h;
+                double ep[5], em[5];
+                halfspace_e(pp[1], pp[0], pp[2], wvno, omega, ep);
+                halfspace_e(pm[1], pm[0], pm[2], wvno, omega, em);
+                double s = 0.0;
+                for (int i = 0; i < 5; i++) s += (ep[i] - em[i]) / (2.0 * h) * B[i];
+                out[q] = -(s * scale) / Fc;
+            }
+            const double tmp = M.btp[m];
+            const size_t o = static_cast<size_t>(k) * mmax + m;
+            dcdb[o] = out[0] * tmp;
+            dcda[o] = out[1] * tmp;
+            dcdr[o] = out[2] * std::pow(M.btp[m], -2.275f);
+        }
+    }
+    return 0;
+}
+
 extern "C" int orc_surfdisp96(const float* thkm, const float* vpm, const float* vsm,
                               const float* rhom, int nlayer, int iflsph, int iwave, int mode,
                               int igr, int kmax, const double* t, double* cg) {
