@@ -102,6 +102,19 @@ int sa_plan_set_graph(sa_plan* plan, int enable);
  * memory). */
 int sa_plan_set_deterministic(sa_plan* plan, int enable, size_t max_bytes);
 
+/* The adjoint a plan computes.  kind 0 (default): the reference's
+ * (eikonal::FSM_O1_JSE_lonlat_2d, src/eikonal_solver.cpp:323-511) with the
+ * reference's forward stopping rule.  kind 1 (FP64 plans; no reference
+ * counterpart): forward solves run to a fixed point (an iteration that
+ * changes no cell) and the adjoint is the exact discrete adjoint of the
+ * forward solve -- the derivative of the receiver times the plan computes,
+ * including the source's slowness -- so adj_s receives dchi/dsvel (per
+ * period plane) instead of the accumulated Ta svel^-3; is_kden is not
+ * computed.  sa_grad_run then chains adj_s with the derivatives of
+ * surfdisp96's phase-velocity roots (Rayleigh phase data), and
+ * sa_grad_vjp takes convention 2.  SA_ERR_ARG for an FP32 plan. */
+int sa_plan_set_adjoint(sa_plan* plan, int kind);
+
 /* is_kden on a plan: while kden_s (device, [nper][ny][nx]) is set, every
  * evaluation with the adjoint also solves the kernel-density adjoint
  * (src/preproc.cpp:128-137) and overwrites kden_s with its accumulation
@@ -497,11 +510,24 @@ int sa_grad_forward(sa_grad* grad, const double* vs3d, double* syn, double* svel
  *     kernels, the density kernel corrected for the flattened velocities its
  *     elastic terms carry once more (src/surfker/sregn96.f90:1132, :1176), and
  *     the half-space layer added to the deepest node.  The eikonal part stays
- *     the reference's continuous adjoint.
+ *     the reference's continuous adjoint;
+ *   convention 2 (the plan's adjoint kind 1, sa_plan_set_adjoint): the exact
+ *     gradient of the discrete forward model -- forward fields at a fixed
+ *     point, the discrete adjoint (dchi/dsvel per cell and period), chained
+ *     with dc/dvs from implicit differentiation of surfdisp96's Rayleigh
+ *     secular function (dltar4) at each phase velocity; matches central
+ *     differences of the receiver times' misfit.
  * vp3d NULL = vs2vp(vs3d).  svel_out, adj_s_out, status may be NULL. */
 int sa_grad_vjp(sa_grad* grad, const double* vs3d, const double* vp3d, const double* source_adj,
                 int convention, double* grad_out, double* svel_out, double* adj_s_out,
                 int* status, void* stream);
+
+/* dc/dvs of every node (nx, ny, nz, nper) row-major, device) from the
+ * Rayleigh phase velocities of vs3d (no reference counterpart): implicit
+ * differentiation of surfdisp96's secular function (dltar4) at each root,
+ * chained through the earth flattening and the Brocher vp, rho; the
+ * half-space layer adds to the deepest node.  Rayleigh phase data only. */
+int sa_grad_root_derivatives(sa_grad* grad, const double* vs3d, double* dcdvs, void* stream);
 
 /* Copies the last run's depth kernels into device arrays sen_vs, sen_vp,
  * sen_rho ((nx, ny, nz, nper) row-major; any may be NULL), on `stream`. */

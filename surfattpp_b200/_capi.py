@@ -31,6 +31,7 @@ EXPORTED = (
     "sa_eik_fwd_field_noalloc", "sa_math_eval", "sa_plan_adjoint_source",
     "sa_grad_forward", "sa_grad_vjp", "sa_plan_set_deterministic",
     "sa_grad_set_data_type", "sa_plan_kden_output", "sa_grad_set_kden", "sa_grad_ker_den",
+    "sa_plan_set_adjoint", "sa_grad_root_derivatives",
     "sa_kernel_precondition", "sa_multi_create", "sa_multi_destroy",
     "sa_multi_forward_adjoint", "sa_multi_kernel_ms", "sa_multi_status",
     "sa_depthkernel_columns_love", "sa_grad_set_wave_type", "sa_multigrid_create",
@@ -113,6 +114,8 @@ def lib():
     L.sa_multigrid_destroy.argtypes = [_vp]
     L.sa_multigrid_smooth.argtypes = [_vp, _vp, _vp, _vp]
     L.sa_plan_kden_output.argtypes = [_vp, _vp]
+    L.sa_plan_set_adjoint.argtypes = [_vp, i]
+    L.sa_grad_root_derivatives.argtypes = [_vp] * 4
     L.sa_grad_set_kden.argtypes = [_vp, i]
     L.sa_grad_ker_den.argtypes = [_vp] * 4 + [_vp]
     L.sa_kernel_precondition.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]

@@ -48,6 +48,7 @@ struct BatchArgs {
     Scratch sc;
     int maxr;              // largest receiver count of any event
     int mode;
+    int discrete;          // BatchDesc::discrete
 };
 
 // Scratch slot layout (bytes, every plane 256-byte aligned).  The packed
@@ -176,13 +177,17 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     }
     __syncwarp();
     iters = 0;
+    // stopping rule: the reference's (src/eikonal_solver.cpp:292-303), or,
+    // for the exact discrete adjoint, a fixed point (an iteration in which
+    // no cell changed: every cell's change times T0 is zero, T0 > 0 off the
+    // fixed source cells)
     for (int iter = 0; iter < 2000; iter++) {
         double l1 = 0.0, linf = 0.0;
         for (int sw = 0; sw < 4; sw++) systolic_sweep(P, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
         iters = iter + 1;
         const double L1 = warp_sum(l1) / (double)(nx * ny);
         const double Linf = warp_max(linf);
-        if (L1 < 1e-4 && Linf < 1e-4) break;
+        if (B.discrete ? (Linf == 0.0) : (L1 < 1e-4 && Linf < 1e-4)) break;
         if (iter == 1999) status = ST_NOCONV;
     }
     // T = tau * T0 in FP64 (src/eikonal_solver.cpp:317)
@@ -198,6 +203,281 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;
     __syncwarp();
     return fun0_64;
+}
+
+// ---------------------------------------------------------------------------
+// Exact discrete adjoint of the factored forward solve (FP64 plans, no
+// reference counterpart: the reference's adjoint, src/eikonal_solver.cpp:
+// 323-511, discretises the continuous adjoint equation).  At a fixed point of
+// the forward iteration every free cell satisfies tau_k = Phi_k(tau_x, tau_y,
+// f_k, t0_k, t0x_k, t0y_k), Phi_k its smallest admissible candidate of
+// :176-279 (a quadrant root, two upwind neighbours, or an axis update, one).
+// With T = tau T0 and T0 = G fun0 (fun0 the bilinear slowness at the source):
+//   lambda = g + J^T lambda,   g_k = sum_r dchi/dT_r beta_rk T0_k,
+//   dchi/dfun_m = lambda_m dPhi_m/df_m + alpha_m S,
+//   S = sum_k lambda_k (dPhi/dt0 G + dPhi/dt0x Gx + dPhi/dt0y Gy)_k
+//       + sum_r dchi/dT_r sum_k beta_rk tau_k G_k,
+// beta the receivers' interp2d weights, alpha the source's bilinear weights;
+// the partials by implicit differentiation of the quadratic (quadrant) or
+// of the axis formula.  lambda is swept to its fixed point with the same
+// engine (AdjPolicyLinear64), whose weights at cell j are the partials of the
+// neighbours' winning stencils with respect to tau_j.  The result,
+// dchi/dsvel = -dchi/dfun fun^2, is added to adj_s (or the event's
+// contribution plane).
+// Scratch reuse (after the forward): T -> dPhi/dtau of the x neighbour,
+// delta -> of the y neighbour (zeroed again at the end), DD -> {dPhi/df,
+// dPhi/dfun0}, flags -> which neighbours the winner reads, tau -> the
+// adjoint source g, PK -> the sweep weights, Ta / tst -> lambda.
+// ---------------------------------------------------------------------------
+struct WinD {
+    int dirx, diry;   // 0: none, 1: the neighbour at -1, 2: at +1
+    double jx, jy, df, dt0, dt0x, dt0y;
+    bool ok;
+};
+
+// The smallest admissible candidate of cell (ix, iy) and its partials; not
+// ok when that candidate is farther than 1e-9 relative from tau (the cell
+// was never reached).
+__device__ inline WinD discrete_winner(const double* tau, const Q4<double>* pk, int nx, int ny,
+                                       int ix, int iy, double aij, double bij, double cij,
+                                       double dx, double dy) {
+    const int k = iy * nx + ix;
+    const Q4<double> c0 = pk[k];
+    const double t0 = c0.x, t0x = c0.y, t0y = c0.z, fij = c0.w;
+    const double det = aij * bij - cij * cij;
+    WinD best{};
+    best.ok = false;
+    double bv = HUGE_VAL;
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) {
+        const int sx = (q < 2) ? -1 : 1;
+        const int sy = (q & 1) ? 1 : -1;
+        if (ix + sx < 0 || ix + sx >= nx || iy + sy < 0 || iy + sy >= ny) continue;
+        const double tx = tau[k + sx], ty = tau[k + sy * nx];
+        const double px = t0x - sx * (t0 / dx);
+        const double qx = sx * (t0 / dx) * tx;
+        const double py = t0y - sy * (t0 / dy);
+        const double qy = sy * (t0 / dy) * ty;
+        const double ea = aij * px * px + bij * py * py - 2.0 * cij * px * py;
+        const double eb = 2.0 * (aij * px * qx + bij * py * qy - cij * (px * qy + py * qx));
+        const double ec = aij * qx * qx + bij * qy * qy - 2.0 * cij * qx * qy - fij * fij;
+        const double Delta = eb * eb - 4.0 * ea * ec;
+        if (Delta < 0.0 || fabs(ea) < 1e-30) continue;
+        const double sq = sqrt(Delta);
+#pragma unroll 1
+        for (int sgn = 0; sgn < 2; sgn++) {
+            const double tt = (-eb + (sgn == 0 ? sq : -sq)) / (2.0 * ea);
+            const double Tx = px * tt + qx, Ty = py * tt + qy;
+            const double chx = aij * Tx - cij * Ty, chy = bij * Ty - cij * Tx;
+            if (!(-sx * chx >= 0.0 && -sy * chy >= 0.0) || !(tt < bv)) continue;
+            const double Qt = 2.0 * ea * tt + eb;
+            bv = tt;
+            best.dirx = sx < 0 ? 1 : 2;
+            best.diry = sy < 0 ? 1 : 2;
+            best.jx = -(2.0 * chx * sx * t0 / dx) / Qt;
+            best.jy = -(2.0 * chy * sy * t0 / dy) / Qt;
+            best.df = (2.0 * fij) / Qt;
+            best.dt0 = -(2.0 * chx * sx * (tx - tt) / dx + 2.0 * chy * sy * (ty - tt) / dy) / Qt;
+            best.dt0x = -(2.0 * tt * chx) / Qt;
+            best.dt0y = -(2.0 * tt * chy) / Qt;
+        }
+    }
+    if (det > 0.0) {
+#pragma unroll 1
+        for (int a = 0; a < 4; a++) {
+            const bool xdir = a < 2;
+            const int s = (a & 1) ? 1 : -1;
+            if (xdir ? (ix + s < 0 || ix + s >= nx) : (iy + s < 0 || iy + s >= ny)) continue;
+            const int kn = xdir ? k + s : k + s * nx;
+            const double h = xdir ? dx : dy;
+            const double p = (xdir ? t0x : t0y) - s * (t0 / h);
+            const double qv = s * (t0 / h) * tau[kn];
+            const double dis = sqrt(fij * fij * (xdir ? bij : aij) / det);
+            const double tn = tau[kn], T0n = pk[kn].x;
+#pragma unroll 1
+            for (int sgn = 0; sgn < 2; sgn++) {
+                const double sd = sgn == 0 ? 1.0 : -1.0;
+                const double tt = (sd * dis - qv) / p;
+                if (!(tt * t0 >= tn * T0n && tt > tn * 0.5) || !(tt < bv)) continue;
+                bv = tt;
+                best.dirx = xdir ? (s < 0 ? 1 : 2) : 0;
+                best.diry = xdir ? 0 : (s < 0 ? 1 : 2);
+                best.jx = xdir ? -(s * t0 / h) / p : 0.0;
+                best.jy = xdir ? 0.0 : -(s * t0 / h) / p;
+                best.df = sd * (dis / fij) / p;
+                best.dt0 = s * (tt - tn) / (h * p);
+                best.dt0x = xdir ? -tt / p : 0.0;
+                best.dt0y = xdir ? 0.0 : -tt / p;
+            }
+        }
+    }
+    best.ok = fabs(bv - tau[k]) <= 1e-9 * fabs(tau[k]);
+    return best;
+}
+
+template <bool ISO>
+__device__ inline void discrete_adjoint(const BatchArgs<double>& B, unsigned int e,
+                                        unsigned char* base, const SrcInfo& si, int ip, int nr,
+                                        int& status) {
+    const Grid& g = B.g;
+    const int nx = g.nx, ny = g.ny;
+    const size_t n = (size_t)nx * ny;
+    const int lane = threadIdx.x & 31;
+    const SlotLayout L = slot_layout<double>(nx, ny, B.maxr);
+    double* tau = reinterpret_cast<double*>(base + L.tau);
+    double* tst = reinterpret_cast<double*>(base + L.tst);
+    double* Jx = reinterpret_cast<double*>(base + L.T);
+    double* Jy = reinterpret_cast<double*>(base + L.delta);
+    double2* DD = reinterpret_cast<double2*>(base + L.DD);
+    Q4<double>* PK = reinterpret_cast<Q4<double>*>(base + L.PK);
+    unsigned char* fl = base + L.flags;
+    double* lam = reinterpret_cast<double*>(base + L.Ta);
+    const double* sadj = reinterpret_cast<const double*>(base + L.sadj);
+    int2* rng = reinterpret_cast<int2*>(base + L.rng);
+    const int src = B.ev.src[e];
+    const double* G = B.G + (size_t)src * n;
+    const double* Gx = B.Gx + (size_t)src * n;
+    const double* Gy = B.Gy + (size_t)src * n;
+    const Q4<double>* mt = ISO ? nullptr : B.mt + (size_t)ip * n;
+    const int r0 = B.ev.rec_ptr[e];
+    // fixed source cells (src/eikonal_solver.cpp:118-129)
+    int fy0 = ny, fy1 = -1;
+    for (int iy = lane; iy < ny; iy += 32)
+        if (fabs((g.yy[iy] - si.y0) / g.dy) <= 1.0) {
+            fy0 = min(fy0, iy);
+            fy1 = max(fy1, iy);
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        fy0 = min(fy0, __shfl_xor_sync(FULL_MASK, fy0, o));
+        fy1 = max(fy1, __shfl_xor_sync(FULL_MASK, fy1, o));
+    }
+    // 1. the winning stencils and their partials
+    for (size_t k = lane; k < n; k += 32) {
+        const int iy = (int)(k / nx), ix = (int)(k % nx);
+        const bool fixed = iy >= fy0 && iy <= fy1 && ix >= si.fix_x0 && ix <= si.fix_x1;
+        WinD w{};
+        w.ok = false;
+        if (!fixed) {
+            const double aij = ISO ? B.a_f_row[iy] : mt[k].x;
+            const double bij = ISO ? B.b_iso : mt[k].y;
+            const double cij = ISO ? 0.0 : mt[k].z;
+            w = discrete_winner(tau, PK, nx, ny, ix, iy, aij, bij, cij, g.dx, g.dy);
+        }
+        if (w.ok) {
+            fl[k] = (unsigned char)(16u | (unsigned)w.dirx | ((unsigned)w.diry << 2));
+            Jx[k] = w.jx;
+            Jy[k] = w.jy;
+            DD[k] = make_double2(w.df, w.dt0 * G[k] + w.dt0x * Gx[k] + w.dt0y * Gy[k]);
+        } else {
+            fl[k] = 0;
+            Jx[k] = 0.0;
+            Jy[k] = 0.0;
+            DD[k] = make_double2(0.0, 0.0);
+        }
+    }
+    __syncwarp();
+    // 2. the receivers' explicit fun0 term, then the adjoint source g in the
+    // tau plane (tau is no longer needed)
+    double srec = 0.0;
+    if (lane == 0)
+        for (int ir = 0; ir < nr; ir++) {
+            const double d = sadj[ir];
+            const int st = B.ev.rec_idx[r0 + ir];
+            size_t kq[4];
+            double wq[4];
+            if (!isfinite(d) ||
+                !interp2d_weights(g.xx_deg, nx, g.yy_deg, ny, B.ev.stlo[st], B.ev.stla[st], kq, wq))
+                continue;
+            for (int q = 0; q < 4; q++) srec += d * wq[q] * tau[kq[q]] * G[kq[q]];
+        }
+    srec = __shfl_sync(FULL_MASK, srec, 0);
+    __syncwarp();
+    for (size_t k = lane; k < n; k += 32) tau[k] = 0.0;
+    __syncwarp();
+    if (lane == 0)
+        for (int ir = 0; ir < nr; ir++) {
+            const double d = sadj[ir];
+            const int st = B.ev.rec_idx[r0 + ir];
+            size_t kq[4];
+            double wq[4];
+            if (!isfinite(d) ||
+                !interp2d_weights(g.xx_deg, nx, g.yy_deg, ny, B.ev.stlo[st], B.ev.stla[st], kq, wq))
+                continue;
+            for (int q = 0; q < 4; q++) tau[kq[q]] += d * wq[q] * PK[kq[q]].x;
+        }
+    __syncwarp();
+    // 3. the sweep weights at every cell: the partials of the neighbours'
+    // winners that read this cell
+    for (size_t k = lane; k < n; k += 32) {
+        const int iy = (int)(k / nx), ix = (int)(k % nx);
+        const double wxm = (ix > 0 && (fl[k - 1] & 3u) == 2u) ? Jx[k - 1] : 0.0;
+        const double wxp = (ix < nx - 1 && (fl[k + 1] & 3u) == 1u) ? Jx[k + 1] : 0.0;
+        const double wym = (iy > 0 && ((fl[k - nx] >> 2) & 3u) == 2u) ? Jy[k - nx] : 0.0;
+        const double wyp = (iy < ny - 1 && ((fl[k + nx] >> 2) & 3u) == 1u) ? Jy[k + nx] : 0.0;
+        st4(PK + k, wxm, wxp, wym, wyp);
+        lam[k] = 0.0;
+        tst[k] = 0.0;
+    }
+    for (int iy = lane; iy < ny; iy += 32) {
+        rng[iy] = make_int2(0, nx - 1);
+        rng[ny + iy] = make_int2(0x7fffffff, -1);
+        rng[2 * ny + iy] = make_int2(0x7fffffff, -1);
+    }
+    __syncwarp();
+    // 4. lambda to its fixed point
+    AdjPolicyLinear64 Q;
+    Q.nx = nx;
+    Q.ny = ny;
+    Q.rng = rng;
+    Q.crng = rng + ny;
+    Q.rng2 = rng + 2 * ny;
+    Q.W = PK;
+    Q.C0 = tau;
+    Q.Ta = lam;
+    Q.Ta_start = tst;
+    int iters = 0;
+    for (int iter = 0; iter < 2000; iter++) {
+        double l1 = 0.0, linf = 0.0;
+        for (int sw = 0; sw < 4; sw++) systolic_sweep(Q, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
+        iters = iter + 1;
+        if (warp_max(linf) == 0.0) break;
+        if (iter == 1999) status = ST_NOCONV;
+    }
+    if (lane == 0 && B.out.adj_iters) B.out.adj_iters[e] = iters;
+    // 5. dchi/dsvel = -dchi/dfun fun^2
+    const double* fun = B.fun64 + (size_t)ip * n;
+    double* acc = B.out.adj_s ? B.out.adj_s + (size_t)ip * n : nullptr;
+    double* con = B.out.contrib ? B.out.contrib + (size_t)(e - B.out.contrib_e0) * n : nullptr;
+    double s0 = 0.0;
+    bool finite = true;
+    for (size_t k = lane; k < n; k += 32) {
+        const double lk = lam[k];
+        s0 += lk * DD[k].y;
+        const double gf = (fl[k] & 16u) ? lk * DD[k].x : 0.0;
+        const double v = -gf * (fun[k] * fun[k]);
+        if (!isfinite(v)) finite = false;
+        if (con) con[k] = v;
+        else if (acc && v != 0.0) atomicAdd(acc + k, v);
+    }
+    const double S = srec + warp_sum(s0);
+    __syncwarp();
+    if (lane == 0) {
+        const int i0 = si.idx0, j0 = si.idy0;
+        const size_t kk[4] = {(size_t)j0 * nx + i0, (size_t)(j0 + 1) * nx + i0,
+                              (size_t)j0 * nx + i0 + 1, (size_t)(j0 + 1) * nx + i0 + 1};
+        const double al[4] = {(1 - si.r1) * (1 - si.r2), (1 - si.r1) * si.r2,
+                              si.r1 * (1 - si.r2), si.r1 * si.r2};
+        for (int q = 0; q < 4; q++) {
+            const double v = -(al[q] * S) * (fun[kk[q]] * fun[kk[q]]);
+            if (!isfinite(v)) finite = false;
+            if (con) con[kk[q]] += v;
+            else if (acc && v != 0.0) atomicAdd(acc + kk[q], v);
+        }
+    }
+    if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;
+    // the delta plane is zero between events
+    for (size_t k = lane; k < n; k += 32) Jy[k] = 0.0;
+    __syncwarp();
 }
 
 // One event of the batch on the warp's scratch slot `base` (laid out for
@@ -271,7 +551,15 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
         // pass 0: the adjoint of the residuals (or the given source); pass 1
         // (is_kden): the kernel-density adjoint, source -w at every receiver,
         // not masked and accumulated into kden_s (src/preproc.cpp:128-137)
-        const int npass = (B.mode == MODE_FWD) ? 0
+        // the exact discrete adjoint replaces the passes (FP64 plans)
+        bool discrete = false;
+        if constexpr (sizeof(S) == sizeof(double)) {
+            if (B.discrete && B.mode == MODE_FWD_ADJ) {
+                discrete_adjoint<ISO>(B, e, base, si, ip, nr, status);
+                discrete = true;
+            }
+        }
+        const int npass = (B.mode == MODE_FWD || discrete) ? 0
                           : (B.mode == MODE_FWD_ADJ && B.out.kden_s && !B.ev.sadj) ? 2
                                                                                    : 1;
         if (clear_delta && npass > 0) {
@@ -562,6 +850,7 @@ inline BatchArgs<double> make_batch_args<double>(const BatchDesc& d) {
     B.sc = d.sc;
     B.maxr = d.maxr;
     B.mode = d.mode;
+    B.discrete = d.discrete;
     return B;
 }
 
@@ -590,6 +879,7 @@ inline BatchArgs<float> make_batch_args<float>(const BatchDesc& d) {
     B.sc = d.sc;
     B.maxr = d.maxr;
     B.mode = d.mode;
+    B.discrete = d.discrete;
     return B;
 }
 

@@ -143,6 +143,7 @@ struct sa_plan {
     double* dbg_T = nullptr;
     double* dbg_Ta = nullptr;
     double* kden_out = nullptr;   // is_kden accumulation target (sa_plan_kden_output)
+    int discrete = 0;             // sa_plan_set_adjoint: 1 = exact discrete adjoint
     bool use_graph = true;
     bool have_graph = false;
     GraphKey key{};
@@ -467,6 +468,7 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
     d.sc.nslots = (P->active > 0 && P->active < P->nslots) ? P->active : P->nslots;
     d.sc.slot_bytes = P->slot_bytes;
     d.variant = P->prec == SA_FP32 ? P->variant : 0;
+    d.discrete = P->discrete;
     d.sc.base = P->scratch.p;
     d.sc.queue = P->queue.p;
     d.maxr = P->maxr;
@@ -825,6 +827,18 @@ extern "C" int sa_plan_adjoint_source(sa_plan* P, const double* svel, const doub
     if (!adj_s) return fail(P->ctx, SA_ERR_ARG, "adj_s is required");
     return plan_run(P, svel, m11, m12, m22, nullptr, nullptr, source_adj, 1, syn, adj_s,
                     nullptr, nullptr, nullptr, status, stream);
+}
+
+extern "C" int sa_plan_set_adjoint(sa_plan* P, int kind) {
+    if (!P) return SA_ERR_ARG;
+    if (kind != 0 && kind != 1) return fail(P->ctx, SA_ERR_ARG, "adjoint kind 0 or 1");
+    if (kind == 1 && P->prec != SA_FP64)
+        return fail(P->ctx, SA_ERR_ARG, "the exact discrete adjoint needs an FP64 plan");
+    if (kind != P->discrete) {
+        P->discrete = kind;
+        P->have_graph = false;   // recapture with the new kernel arguments
+    }
+    return SA_OK;
 }
 
 // ---- one launch over several plans (grid levels) ----------------------------
@@ -1363,6 +1377,7 @@ struct sa_grad {
     DArr<unsigned char> lc;
     DArr<double> periods, svel, adj_s, sen_vs, sen_vp, sen_rho;
     DArr<double> sen_hs;     // half-space layer kernels (derivative convention)
+    DArr<double> dcdvs;      // exact dc/dvs per node (convention 2)
     DArr<double> area;       // [ny] cell area dx R cos(lat) dy R, km^2
     DArr<int> colst, worst;
     // data type: 0 Rayleigh phase, 1 Rayleigh group (sa_grad_set_data_type).
@@ -1566,6 +1581,19 @@ extern "C" int sa_grad_run(sa_grad* g, const double* vs3d, const double* vp3d,
     rc = sa_plan_forward_adjoint(P, svel, nullptr, nullptr, nullptr, tt_obs, weight, 1, nullptr,
                                  adj_s, chi, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
+    if (P->discrete) {
+        // exact discrete adjoint (sa_plan_set_adjoint): adj_s = dchi/dsvel,
+        // chained with the derivatives of the phase-velocity roots
+        if (g->igr != 0 || g->iwave != 2)
+            return fail(ctx, SA_ERR_ARG, "the exact gradient is for Rayleigh phase data");
+        SA_CUDA(g->dcdvs.alloc((size_t)nx * ny * nz * nper));
+        SA_CUDA(launch_dispersion_dcdvs(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p,
+                                        g->dcdvs.p, st));
+        SA_CUDA(launch_combine_exact(nx, ny, nz, nper, adj_s, g->dcdvs.p, ker_vs, st));
+        SA_CUDA(launch_grad_status(grad_ncolst(g), g->colst.p, P->worst.p,
+                                   status ? status : g->worst.p, st));
+        return SA_OK;
+    }
     // compute_dispersion_kernel on a second stream: it needs only vs3d and the
     // velocities, so it runs while the event batch drains
     SA_CUDA(cudaStreamWaitEvent(g->side, g->e_disp, 0));
@@ -1611,14 +1639,34 @@ extern "C" int sa_grad_vjp(sa_grad* g, const double* vs3d, const double* vp3d,
     sa_ctx* ctx = P->ctx;
     if (!vs3d || !grad || (P->npair > 0 && !source_adj))
         return fail(ctx, SA_ERR_ARG, "vs3d, source_adj and grad are required");
-    if (convention != 0 && convention != 1) return fail(ctx, SA_ERR_ARG, "convention 0 or 1");
-    if (convention == 1 && (g->igr != 0 || g->iwave != 2))
-        return fail(ctx, SA_ERR_ARG, "the derivative convention is for Rayleigh phase data");
+    if (convention < 0 || convention > 2) return fail(ctx, SA_ERR_ARG, "convention 0, 1 or 2");
+    if (convention >= 1 && (g->igr != 0 || g->iwave != 2))
+        return fail(ctx, SA_ERR_ARG, "conventions 1 and 2 are for Rayleigh phase data");
+    if ((convention == 2) != (P->discrete == 1))
+        return fail(ctx, SA_ERR_ARG,
+                    "convention 2 goes with the exact discrete adjoint (sa_plan_set_adjoint)");
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const int nx = P->nx, ny = P->ny, nz = g->nz, nper = P->nper;
     double* svel = svel_out ? svel_out : g->svel.p;
     double* adj_s = adj_s_out ? adj_s_out : g->adj_s.p;
+    if (convention == 2) {
+        // the exact gradient of the discrete forward model: fwdsurf, every
+        // forward field to a fixed point, the discrete adjoint (adj_s =
+        // dchi/dsvel), the derivatives of the phase-velocity roots
+        SA_CUDA(g->dcdvs.alloc((size_t)nx * ny * nz * nper));
+        int rc = grad_velocities(g, vs3d, svel, st);
+        if (rc) return rc;
+        rc = plan_run(P, svel, nullptr, nullptr, nullptr, nullptr, nullptr, source_adj, 1,
+                      nullptr, adj_s, nullptr, nullptr, nullptr, nullptr, st);
+        if (rc) return rc;
+        SA_CUDA(launch_dispersion_dcdvs(nx, ny, nz, vs3d, nper, g->periods.p, svel, g->lc.p,
+                                        g->dcdvs.p, st));
+        SA_CUDA(launch_combine_exact(nx, ny, nz, nper, adj_s, g->dcdvs.p, grad, st));
+        SA_CUDA(launch_grad_status(grad_ncolst(g), g->colst.p, P->worst.p,
+                                   status ? status : g->worst.p, st));
+        return SA_OK;
+    }
     if (convention == 1) SA_CUDA(g->sen_hs.alloc((size_t)nx * ny * nper * 3));
     int rc = grad_velocities(g, vs3d, svel, st);
     if (rc) return rc;
@@ -1641,6 +1689,23 @@ extern "C" int sa_grad_vjp(sa_grad* g, const double* vs3d, const double* vp3d,
                                              g->lc.p, grad, st));
     SA_CUDA(launch_grad_status(grad_ncolst(g), g->colst.p, P->worst.p,
                                status ? status : g->worst.p, st));
+    return SA_OK;
+}
+
+extern "C" int sa_grad_root_derivatives(sa_grad* g, const double* vs3d, double* dcdvs,
+                                        void* stream) {
+    if (!g) return SA_ERR_ARG;
+    sa_plan* P = g->plan;
+    sa_ctx* ctx = P->ctx;
+    if (!vs3d || !dcdvs) return fail(ctx, SA_ERR_ARG, "vs3d and dcdvs are required");
+    if (g->igr != 0 || g->iwave != 2)
+        return fail(ctx, SA_ERR_ARG, "root derivatives are for Rayleigh phase velocities");
+    SA_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    int rc = grad_velocities(g, vs3d, g->svel.p, st);
+    if (rc) return rc;
+    SA_CUDA(launch_dispersion_dcdvs(P->nx, P->ny, g->nz, vs3d, P->nper, g->periods.p, g->svel.p,
+                                    g->lc.p, dcdvs, st));
     return SA_OK;
 }
 

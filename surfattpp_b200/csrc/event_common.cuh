@@ -52,9 +52,11 @@ __device__ inline SrcInfo source_info(const Grid& g, double evlo, double evla) {
 }
 
 // include/utils.h:358-409 (one query point).
-__device__ inline double interp2d_pt(const double* xg, int nx, const double* yg, int ny,
-                                     const double* z, double qx, double qy) {
-    if (qx < xg[0] || qx > xg[nx - 1] || qy < yg[0] || qy > yg[ny - 1]) return __longlong_as_double(0x7ff8000000000000ll);
+// The cell and bilinear weights interp2d uses for one point (row-major
+// offsets k[4] of (i, j), (i+1, j), (i, j+1), (i+1, j+1)); false outside.
+__device__ inline bool interp2d_weights(const double* xg, int nx, const double* yg, int ny,
+                                        double qx, double qy, size_t* k, double* w) {
+    if (qx < xg[0] || qx > xg[nx - 1] || qy < yg[0] || qy > yg[ny - 1]) return false;
     int lo = 0, hi = nx;   // lower_bound
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
@@ -80,10 +82,24 @@ __device__ inline double interp2d_pt(const double* xg, int nx, const double* yg,
     const double y1 = yg[j], y2 = yg[j + 1];
     const double tx = (qx - x1) / (x2 - x1);
     const double ty = (qy - y1) / (y2 - y1);
-    return (1 - tx) * (1 - ty) * z[(size_t)j * nx + i]
-         + (tx) * (1 - ty) * z[(size_t)j * nx + i + 1]
-         + (1 - tx) * (ty) * z[(size_t)(j + 1) * nx + i]
-         + (tx) * (ty) * z[(size_t)(j + 1) * nx + i + 1];
+    k[0] = (size_t)j * nx + i;
+    k[1] = (size_t)j * nx + i + 1;
+    k[2] = (size_t)(j + 1) * nx + i;
+    k[3] = (size_t)(j + 1) * nx + i + 1;
+    w[0] = (1 - tx) * (1 - ty);
+    w[1] = (tx) * (1 - ty);
+    w[2] = (1 - tx) * (ty);
+    w[3] = (tx) * (ty);
+    return true;
+}
+
+__device__ inline double interp2d_pt(const double* xg, int nx, const double* yg, int ny,
+                                     const double* z, double qx, double qy) {
+    size_t k[4];
+    double w[4];
+    if (!interp2d_weights(xg, nx, yg, ny, qx, qy, k, w))
+        return __longlong_as_double(0x7ff8000000000000ll);
+    return w[0] * z[k[0]] + w[1] * z[k[1]] + w[2] * z[k[2]] + w[3] * z[k[3]];
 }
 
 // Bilinear spreading of adjoint sources normalised by the cell area

@@ -481,6 +481,80 @@ struct AdjPolicyExact {
     }
 };
 
+// Sweep policy of the exact discrete adjoint (batch.cuh, discrete_adjoint):
+// lambda = c0 + wxm lambda(ix-1) + wxp lambda(ix+1) + wym lambda(iy-1) +
+// wyp lambda(iy+1) over the whole grid, FP64, the weights being the partial
+// derivatives of the neighbours' winning forward stencils with respect to
+// this cell's tau (zero where a neighbour's stencil does not read it).
+struct AdjPolicyLinear64 {
+    using V = double;
+    using X = float;
+    static constexpr int kLead = 2;
+    static constexpr bool kRolled = false;
+    static constexpr bool kFlags = false;
+    struct Cell {
+        double v;
+        float x;
+        Q4<double> w;
+        double c0;
+        double vs;
+        unsigned fl;
+    };
+    int nx, ny;
+    int2* rng;
+    int2* crng;
+    int2* rng2;
+    const Q4<double>* W;
+    const double* C0;
+    double* Ta;
+    double* Ta_start;
+
+    __device__ int nrows() const { return ny; }
+    __device__ int ncols() const { return nx; }
+    __device__ int stride() const { return nx; }
+    __device__ int row(int rp, int yd) const { return yd > 0 ? rp : ny - 1 - rp; }
+    __device__ int col(int cp, int xd) const { return xd > 0 ? cp : nx - 1 - cp; }
+    __device__ int cp_of(int ix, int xd) const { return xd > 0 ? ix : nx - 1 - ix; }
+    __device__ void begin_row(int, bool) {}
+    __device__ Cell load(int k, bool last) const {
+        Cell c;
+        c.v = Ta[k];
+        c.x = 0.f;
+        c.w = ld4(W + k);
+        c.c0 = C0[k];
+        c.vs = last ? Ta_start[k] : 0.0;
+        c.fl = 0u;
+        return c;
+    }
+    __device__ Cell load_nb(int k) const {
+        Cell c{};
+        c.v = Ta[k];
+        return c;
+    }
+    __device__ double update(const Cell& cur, int, const Nb<double, float>& um,
+                             const Nb<double, float>& dm, const Nb<double, float>& uy,
+                             const Nb<double, float>& dy_, int xd, int yd) const {
+        const Nb<double, float>& xm = xd > 0 ? um : dm;
+        const Nb<double, float>& xp = xd > 0 ? dm : um;
+        const Nb<double, float>& ym = yd > 0 ? uy : dy_;
+        const Nb<double, float>& yp = yd > 0 ? dy_ : uy;
+        const double txm = xm.has ? xm.v : 0.0;
+        const double txp = xp.has ? xp.v : 0.0;
+        const double tym = ym.has ? ym.v : 0.0;
+        const double typ = yp.has ? yp.v : 0.0;
+        return cur.c0 + cur.w.x * txm + cur.w.y * txp + cur.w.z * tym + cur.w.w * typ;
+    }
+    __device__ void account(const Cell& cur, double nv, double& l1, double& linf) const {
+        const double dv = fabs(nv - cur.vs);
+        l1 += dv;
+        linf = fmax(linf, dv);
+    }
+    __device__ void store(int k, double v, bool write_v, bool write_start) const {
+        if (write_v) Ta[k] = v;
+        if (write_start) Ta_start[k] = v;
+    }
+};
+
 // Adjoint sweep policy, FP32 weight form: the same Gauss-Seidel update
 // rewritten as Ta = c0 + wxm*Ta(ix-1) + wxp*Ta(ix+1) + wym*Ta(iy-1) + wyp*Ta(iy+1)
 // with FP32 weights computed in FP64 (w = {wxm, wxp, wym, wyp}, c0 separate).

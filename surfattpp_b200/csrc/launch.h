@@ -40,6 +40,11 @@ struct BatchDesc {
     int maxr;
     int mode;
     int variant;   // FP32 launch variant (batch.cuh), 0 = default
+    // 0: the reference's adjoint and forward stopping rule; 1 (FP64 plans):
+    // forward solves run to a fixed point and the adjoint is the exact
+    // discrete adjoint (batch.cuh, discrete_adjoint); adj_s then receives
+    // dchi/dsvel
+    int discrete;
 };
 
 // Number of FP32 batch-kernel launch variants (batch.cuh).
@@ -153,6 +158,12 @@ cudaError_t launch_depthkernel_group(int nx, int ny, int nz, const double* vs3d,
                                      const double* cp, const double* cp1, const double* cp2,
                                      const void* layer_const, double* sen_vs, double* sen_vp,
                                      double* sen_rho, cudaStream_t st);
+// exact dc/dvs per node from the phase-velocity roots (surfker.cu)
+cudaError_t launch_dispersion_dcdvs(int nx, int ny, int nz, const double* vs3d, int nper,
+                                    const double* periods, const double* svel,
+                                    const void* layer_const, double* dcdvs, cudaStream_t st);
+cudaError_t launch_combine_exact(int nx, int ny, int nz, int nper, const double* dchi_dsvel,
+                                 const double* dcdvs, double* grad, cudaStream_t st);
 cudaError_t launch_combine_vs(int nx, int ny, int nz, int nper, const double* adj_s,
                               const double* vs3d, const double* vp3d, const double* sen_vs,
                               const double* sen_vp, const double* sen_rho, double* ker_vs,

@@ -322,6 +322,87 @@ __global__ void combine_vs_derivative_kernel(int nx, int ny, int nz, int nper,
     grad[i3] = g;
 }
 
+// Exact dc/dvs of every node (no reference counterpart): one thread per
+// (column, period); the derivatives of surfdisp96's Rayleigh phase-velocity
+// root c (from the svel plane) with respect to each flattened layer's b, a,
+// rho (sk::root_dcdm), chained through the flattening (b_f = vs tmp, a_f =
+// vp tmp, rho_f = rho rhofac, sphere of surfdisp96.f:502-574) and the
+// Brocher relations (vp(vs), rho(vp)); the half-space layer, a copy of the
+// deepest node, adds to that node.  dcdvs [(col * nz + k) * nper + ip].
+__global__ void __launch_bounds__(64)
+dispersion_dcdvs_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
+                        const double* __restrict__ periods, const double* __restrict__ svel,
+                        const LayerConst* __restrict__ Lp, double* dcdvs) {
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= (long long)nx * ny * nper) return;
+    const int ip = (int)(gid % nper);
+    const int col = (int)(gid / nper);
+    const int ix = col / ny, iy = col % ny;
+    const LayerConst& L = *Lp;
+    float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];
+    const double* v1 = vs3d + (size_t)col * nz;
+    sk::column_model(v1, nz, L, vp, vs, rho);
+    sk::SDModel M;
+    const int mmax = L.mmax;
+    M.mmax = mmax;
+    M.llw = 1;
+    for (int i = 0; i < mmax; i++) {
+        M.d[i] = L.sd_d[i];
+        M.a[i] = (float)(vp[i] * L.sd_tmp[i]);
+        M.b[i] = (float)(vs[i] * L.sd_tmp[i]);
+        M.rho[i] = rho[i] * L.sd_rhofac[i];
+    }
+    M.del1st = 0.0;
+    double ein[5 * sk::MMAX], logn[sk::MMAX], db[sk::MMAX], da[sk::MMAX], dr[sk::MMAX];
+    const double c = svel[(size_t)ip * nx * ny + ix + (size_t)nx * iy];
+    sk::root_dcdm(M, periods[ip], c, db, da, dr, ein, logn);
+    for (int k = 0; k < nz; k++) {
+        const double b = v1[k];
+        const double a = sk::vs2vp(b);
+        const double dab = sk::dalpha_dbeta(b), dra = sk::drho_dalpha(a);
+        auto node = [&](int m) {
+            return db[m] * L.sd_tmp[m] + da[m] * L.sd_tmp[m] * dab
+                   + dr[m] * (double)L.sd_rhofac[m] * dra * dab;
+        };
+        double d = node(k);
+        if (k == nz - 1) d += node(nz);
+        dcdvs[((size_t)col * nz + k) * nper + ip] = d;
+    }
+}
+
+// grad(ix, iy, k) = sum_iper dchi/dsvel(iper, iy, ix) * dc/dvs(ix, iy, k, iper),
+// periods in order.
+__global__ void combine_exact_kernel(int nx, int ny, int nz, int nper,
+                                     const double* __restrict__ dchi_dsvel,
+                                     const double* __restrict__ dcdvs, double* grad) {
+    const size_t i3 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i3 >= (size_t)nx * ny * nz) return;
+    const int col = (int)(i3 / nz);
+    const int ix = col / ny, iy = col % ny;
+    double g = 0.0;
+    for (int ip = 0; ip < nper; ip++)
+        g += dchi_dsvel[(size_t)ip * nx * ny + ix + (size_t)nx * iy] * dcdvs[i3 * nper + ip];
+    grad[i3] = g;
+}
+
+cudaError_t launch_dispersion_dcdvs(int nx, int ny, int nz, const double* vs3d, int nper,
+                                    const double* periods, const double* svel,
+                                    const void* layer_const, double* dcdvs, cudaStream_t st) {
+    const long long n = (long long)nx * ny * nper;
+    dispersion_dcdvs_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
+        nx, ny, nz, vs3d, nper, periods, svel, reinterpret_cast<const LayerConst*>(layer_const),
+        dcdvs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_exact(int nx, int ny, int nz, int nper, const double* dchi_dsvel,
+                                 const double* dcdvs, double* grad, cudaStream_t st) {
+    const size_t n = (size_t)nx * ny * nz;
+    combine_exact_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(nx, ny, nz, nper,
+                                                                       dchi_dsvel, dcdvs, grad);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_combine_vs_derivative(int nx, int ny, int nz, int nper, const double* adj_s,
                                          const double* vs3d, const double* vp3d,
                                          const double* sen_vs, const double* sen_vp,

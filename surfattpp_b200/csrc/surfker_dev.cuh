@@ -191,10 +191,10 @@ __device__ inline VarOut var(double p, double q, double ra, double rb, double wv
     return o;
 }
 
-// surfdisp96.f:1054-1098 fused with the row-vector product of dltar4
-// (ee(i) = sum_j e(j)*ca(j,i), :868-874).
-__device__ inline void dnka_apply(const double* e, double* ee, double wvno2, double gam,
-                                  double gammk, double rho, const VarOut& v) {
+// surfdisp96.f:1054-1098: the 5x5 compound layer matrix, ca[j][i] holding
+// the Fortran ca(j+1, i+1).
+__device__ inline void dnka_matrix(double ca[5][5], double wvno2, double gam, double gammk,
+                                   double rho, const VarOut& v) {
     const double one = 1.0, two = 2.0;
     const double gamm1 = gam - one;
     const double twgm1 = gam + gamm1;
@@ -203,7 +203,6 @@ __device__ inline void dnka_apply(const double* e, double* ee, double wvno2, dou
     const double gm1sq = gamm1 * gamm1;
     const double rho2 = rho * rho;
     const double a0pq = v.a0 - v.cpcq;
-    double ca[5][5];
     ca[0][0] = v.cpcq - two * gmgm1 * a0pq - gmgmk * v.xz - wvno2 * gm1sq * v.wy;
     ca[0][1] = (wvno2 * v.cpy - v.cqx) / rho;
     ca[0][2] = -((twgm1 * a0pq + gammk * v.xz + wvno2 * gamm1 * v.wy) / rho);
@@ -230,6 +229,14 @@ __device__ inline void dnka_apply(const double* e, double* ee, double wvno2, dou
     ca[2][2] = v.a0 + two * (v.cpcq - ca[0][0]);
     ca[2][3] = t * ca[1][2];
     ca[2][4] = t * ca[0][2];
+}
+
+// dnka followed by the row-vector product of dltar4 (ee(i) = sum_j
+// e(j)*ca(j,i), surfdisp96.f:868-874).
+__device__ inline void dnka_apply(const double* e, double* ee, double wvno2, double gam,
+                                  double gammk, double rho, const VarOut& v) {
+    double ca[5][5];
+    dnka_matrix(ca, wvno2, gam, gammk, rho, v);
 #pragma unroll
     for (int i = 0; i < 5; i++) {
         double cr = 0.0;
@@ -361,6 +368,123 @@ __device__ SK_NOINLINE double dltar1(const SDModel& M, double wvno, double omega
         e2 = e20 / xnor;
     }
     return e1;
+}
+
+// ---------------------------------------------------------------------------
+// Derivatives of the Rayleigh phase-velocity root (no reference counterpart:
+// the reference's depth kernels come from sregn96's energy integrals, which
+// agree with differences of surfdisp96's phase velocities only to about
+// 1e-3).  dltar4's secular function is F = e_hs CA_{n} ... CA_0 u / N
+// (e_hs the half-space row vector, CA_m the compound layer matrices, u the
+// first unit vector, N the product of the normc scalings).  At the root F = 0,
+// so with B_m = CA_{m-1} ... CA_0 u and e_{m+1} the normalised row vector
+// entering layer m,
+//   dF/dp_m = e_{m+1} (dCA_m/dp_m) B_m / (n_m ... n_0),   dc/dp = -F_p / F_c,
+// dCA_m/dp_m and de_hs/dp by central differences of the one layer's matrix
+// (relative step 1e-6), F_c by central differences of dltar4.
+// ---------------------------------------------------------------------------
+__device__ inline void layer_matrix(double a, double b, double rho, double d, double wvno,
+                                    double omega, double ca[5][5]) {
+    const double wvno2 = wvno * wvno;
+    const double xka = omega / a, xkb = omega / b;
+    const double t = b / omega;
+    const double gammk = 2.0 * t * t;
+    const double gam = gammk * wvno2;
+    const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
+    const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+    const VarOut v = var(ra * d, rb * d, ra, rb, wvno, xka, xkb, d);
+    dnka_matrix(ca, wvno2, gam, gammk, rho, v);
+}
+__device__ inline void halfspace_vector(double a, double b, double rho, double wvno, double omega,
+                                        double e[5]) {
+    const double wvno2 = wvno * wvno;
+    const double xka = omega / a, xkb = omega / b;
+    const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
+    const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+    const double t = b / omega;
+    const double gammk = 2.0 * t * t;
+    const double gam = gammk * wvno2;
+    const double gamm1 = gam - 1.0;
+    e[0] = rho * rho * (gamm1 * gamm1 - gam * gammk * ra * rb);
+    e[1] = -(rho * ra);
+    e[2] = rho * (gamm1 - gammk * ra * rb);
+    e[3] = rho * rb;
+    e[4] = wvno2 - ra * rb;
+}
+
+// dc/d(b, a, rho) of the flattened layers of M (no water layer) at the root
+// c for period t; `ein` (5 * mmax) and `logn` (mmax) are scratch.
+__device__ inline void root_dcdm(const SDModel& M, double t, double c, double* dcb, double* dca,
+                                 double* dcr, double* ein, double* logn) {
+    const int mmax = M.mmax;
+    const double omega = fmax(2.0 * 3.141592653589793 / t, 1.0e-4);
+    const double wvno = omega / c;
+    double e[5], ca[5][5];
+    halfspace_vector(M.a[mmax - 1], M.b[mmax - 1], M.rho[mmax - 1], wvno, omega, e);
+    for (int m = mmax - 2; m >= 0; m--) {
+        for (int i = 0; i < 5; i++) ein[5 * m + i] = e[i];
+        layer_matrix(M.a[m], M.b[m], M.rho[m], M.d[m], wvno, omega, ca);
+        double ee[5], t1 = 0.0;
+        for (int i = 0; i < 5; i++) {
+            double cr = 0.0;
+            for (int j = 0; j < 5; j++) cr += e[j] * ca[j][i];
+            ee[i] = cr;
+            t1 = fmax(t1, fabs(cr));
+        }
+        if (t1 < 1.e-40) t1 = 1.0;
+        for (int i = 0; i < 5; i++) e[i] = ee[i] / t1;
+        logn[m] = sk_log(t1);
+    }
+    const double hc = 1e-7 * c;
+    const double Fc = (dltar4(M, omega / (c + hc), omega) - dltar4(M, omega / (c - hc), omega))
+                      / (2.0 * hc);
+    double B[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
+    double LB = 0.0, LN = 0.0;
+    for (int m = 0; m <= mmax - 1; m++) {
+        const bool hs = m == mmax - 1;
+        if (!hs) LN += logn[m];
+        const double scale = sk_exp(LB - LN);
+        const double p0[3] = {M.b[m], M.a[m], M.rho[m]};
+        double out[3];
+        for (int q = 0; q < 3; q++) {
+            double pp[3] = {p0[0], p0[1], p0[2]}, pm[3] = {p0[0], p0[1], p0[2]};
+            const double h = 1e-6 * p0[q];
+            pp[q] += h;
+            pm[q] -= h;
+            double s = 0.0;
+            if (hs) {
+                double ep[5], em[5];
+                halfspace_vector(pp[1], pp[0], pp[2], wvno, omega, ep);
+                halfspace_vector(pm[1], pm[0], pm[2], wvno, omega, em);
+                for (int i = 0; i < 5; i++) s += (ep[i] - em[i]) / (2.0 * h) * B[i];
+            } else {
+                double cp[5][5], cm[5][5];
+                layer_matrix(pp[1], pp[0], pp[2], M.d[m], wvno, omega, cp);
+                layer_matrix(pm[1], pm[0], pm[2], M.d[m], wvno, omega, cm);
+                for (int i = 0; i < 5; i++) {
+                    double r = 0.0;
+                    for (int j = 0; j < 5; j++) r += (cp[i][j] - cm[i][j]) / (2.0 * h) * B[j];
+                    s += ein[5 * m + i] * r;
+                }
+            }
+            out[q] = -(s * scale) / Fc;
+        }
+        dcb[m] = out[0];
+        dca[m] = out[1];
+        dcr[m] = out[2];
+        if (hs) break;
+        layer_matrix(M.a[m], M.b[m], M.rho[m], M.d[m], wvno, omega, ca);
+        double nb[5], bm = 0.0;
+        for (int i = 0; i < 5; i++) {
+            double r = 0.0;
+            for (int j = 0; j < 5; j++) r += ca[i][j] * B[j];
+            nb[i] = r;
+            bm = fmax(bm, fabs(r));
+        }
+        if (bm < 1e-300) bm = 1.0;
+        for (int i = 0; i < 5; i++) B[i] = nb[i] / bm;
+        LB += sk_log(bm);
+    }
 }
 
 __device__ __forceinline__ double dltar(const SDModel& M, double wvno, double omega, int kk) {

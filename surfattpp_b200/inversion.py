@@ -27,7 +27,12 @@ Conventions of the vs gradient:
     Jacobian, plain dc/dvs, corrected density kernel, half-space at the
     deepest node).  Its eikonal part is still the reference's continuous
     adjoint, which differs from the derivative of the discretised travel
-    times by the discretisation error (about 10 % on the checkerboard case).
+    times by the discretisation error (about 10 % on the checkerboard case);
+  * "exact" (the plan's adjoint set to "exact", FP64): the gradient of the
+    discrete forward model itself -- forward solves to a fixed point, the
+    exact discrete adjoint of the factored fast-sweeping solve, and dc/dvs by
+    implicit differentiation of surfdisp96's secular function; it matches
+    central differences of chi (2.4e-4 on the checkerboard case).
 Device memory is held in torch tensors; all arithmetic runs in
 libsurfatt_gpu.so.
 """
@@ -168,7 +173,7 @@ class MisfitGradient:
         p = self.plan
         if stream is None:
             stream = torch.cuda.current_stream(vs3d.device).cuda_stream
-        conv = {"reference": 0, "derivative": 1}[convention]
+        conv = {"reference": 0, "derivative": 1, "exact": 2}[convention]
         if grad is None:
             grad = torch.empty((p.nx, p.ny, self.nz), dtype=torch.float64, device=vs3d.device)
         st = torch.zeros(1, dtype=torch.int32, device=vs3d.device)
@@ -177,6 +182,18 @@ class MisfitGradient:
         _capi.check(p.ctx.h, rc)
         self.last_status = st
         return grad
+
+    def dcdvs(self, vs3d, stream=None):
+        """dc/dvs (nx, ny, nz, nper) of the Rayleigh phase velocities of vs3d
+        from the derivatives of surfdisp96's roots (sa_grad_root_derivatives)."""
+        import torch
+        p = self.plan
+        if stream is None:
+            stream = torch.cuda.current_stream(vs3d.device).cuda_stream
+        out = torch.empty((p.nx, p.ny, self.nz, p.nper), dtype=torch.float64, device=vs3d.device)
+        rc = _capi.lib().sa_grad_root_derivatives(self.h, ptr(vs3d), ptr(out), stream)
+        _capi.check(p.ctx.h, rc)
+        return out
 
     def sen(self, stream=None):
         """(sen_vs, sen_vp, sen_rho) of the last run as device tensors

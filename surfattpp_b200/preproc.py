@@ -59,6 +59,14 @@ class ForwardAdjointPlan:
         except Exception:
             pass
 
+    def set_adjoint(self, kind="reference"):
+        """"reference": the reference's adjoint and forward stopping rule;
+        "exact" (FP64 plans): forward solves to a fixed point and the exact
+        discrete adjoint, adj_s = dchi/dsvel (sa_plan_set_adjoint)."""
+        k = {"reference": 0, "exact": 1}[kind]
+        _capi.check(self.ctx.h, _capi.lib().sa_plan_set_adjoint(self.h, k))
+        self.adjoint = kind
+
     def set_deterministic(self, enable=True, max_bytes=0):
         """Sum adj_s and chi in event order (reproducible bit for bit; FP64:
         the reference's single-rank sums) instead of with atomics

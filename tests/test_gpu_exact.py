@@ -1,0 +1,124 @@
+"""The exact gradient of the discrete forward model on the device (FP64 plan
+with the adjoint set to "exact"), on the checkerboard case (41x41x30, 10
+periods, 250 events, observed times from the checkerboard model):
+
+* receiver times after forward solves to a fixed point equal the oracle's
+  (1e-12 relative; the FP64 sweeps round as the oracle's);
+* dchi/dsvel of the discrete adjoint equals the oracle's (1e-9 of its
+  maximum: the device sweeps lambda Gauss-Seidel, the oracle by Jacobi
+  iteration, so the sums round differently);
+* dc/dvs from the phase-velocity roots equals the oracle's (1e-6 relative
+  to each column's largest value: both difference the layer matrices);
+* the autograd gradient of chi built in torch on TravelTimes with
+  convention "exact" matches central differences of chi (+-1e-2 km/s,
+  oracle forward solves to a fixed point) within 1e-3 on 12 nodes where it
+  exceeds 5 % of its maximum, and sa_grad_run on the same plan returns the
+  same gradient (1e-12 of its maximum).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2(orc):
+    from surfattpp_b200 import workloads as W
+    w = W.config1()
+    ev = w.events()
+    m11, m12, m22 = w.media()
+    sv_true, st = orc.fwdsurf(w.zgrid, w.vs3d, w.periods, nthreads=8)
+    assert st.sum() == 0
+    ev["tt_obs"] = orc.discrete_for_events(w.xx_deg, w.yy_deg, sv_true, m11, m12, m22, ev,
+                                           tol=0.0, grad=False, nthreads=8)["syn"].copy()
+    return w, ev, w.meta["vs_start"]
+
+
+def _plan(w, ev):
+    from surfattpp_b200 import inversion, preproc
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision="fp64")
+    plan.set_adjoint("exact")
+    return plan, inversion.MisfitGradient(plan, w.zgrid, w.periods)
+
+
+def _t(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda:0")
+
+
+def test_discrete_adjoint_matches_oracle(c2, gpu, orc):
+    import torch
+    w, ev, vs0 = c2
+    plan, g = _plan(w, ev)
+    sv0, _ = orc.fwdsurf(w.zgrid, vs0, w.periods, nthreads=8)
+    m11, m12, m22 = w.media()
+    ref = orc.discrete_for_events(w.xx_deg, w.yy_deg, sv0, m11, m12, m22, ev, tol=0.0,
+                                  nthreads=8)
+    out = plan.run(_t(sv0), _t(ev["tt_obs"]), _t(ev["weight"]))
+    torch.cuda.synchronize()
+    assert int(out["status"][0]) == 0
+    syn = out["syn"].cpu().numpy()[: ref["syn"].size]
+    assert np.max(np.abs(syn - ref["syn"]) / ref["syn"]) <= 1e-12
+    assert abs(float(out["chi"][0]) - ref["chi"]) <= 1e-12 * ref["chi"]
+    got = out["adj_s"].cpu().numpy()
+    scale = np.abs(ref["grad_svel"]).max()
+    assert np.max(np.abs(got - ref["grad_svel"])) <= 1e-9 * scale
+
+
+def test_root_derivatives_match_oracle(c2, gpu, orc):
+    import torch
+    from exact_chain import dcdvs_nodes
+    w, ev, vs0 = c2
+    vs = vs0[::4, ::4].copy()
+    sv, _ = orc.fwdsurf(w.zgrid, vs, w.periods, nthreads=8)
+    ref = dcdvs_nodes(orc, w.zgrid, vs, w.periods, sv)
+    # a one-event plan on the coarse grid owns the handle
+    from surfattpp_b200 import preproc, inversion
+    xx, yy = w.xx_deg[::4], w.yy_deg[::4]
+    p2 = preproc.ForwardAdjointPlan(xx, yy, w.nper, np.array([xx[2]]), np.array([yy[2]]),
+                                    np.array([0]), np.array([0, 1]), np.array([0]),
+                                    np.array([xx[5]]), np.array([yy[6]]), precision="fp64")
+    g2 = inversion.MisfitGradient(p2, w.zgrid, w.periods)
+    got = g2.dcdvs(_t(vs))
+    torch.cuda.synchronize()
+    got = got.cpu().numpy()
+    colmax = np.abs(ref).max(axis=2, keepdims=True)
+    assert np.max(np.abs(got - ref) / np.maximum(colmax, 1e-30)) <= 1e-6
+
+
+def test_exact_gradient_matches_differences(c2, gpu, orc):
+    import torch
+    from surfattpp_b200 import inversion
+    w, ev, vs0 = c2
+    plan, g = _plan(w, ev)
+    tt, wt = _t(ev["tt_obs"]), _t(ev["weight"])
+    vs = _t(vs0).requires_grad_(True)
+    chi = inversion.misfit(g, vs, tt, wt, convention="exact")
+    chi.backward()
+    torch.cuda.synchronize()
+    ker = vs.grad.cpu().numpy()
+    assert int(g.last_status[0]) == 0
+    # the fused evaluation on the same plan gives the same gradient
+    out = g.run(_t(vs0), tt, wt)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(out["ker_vs"].cpu().numpy() - ker)) <= 1e-12 * np.abs(ker).max()
+    m11, m12, m22 = w.media()
+
+    def chi_of(v):
+        sv, _ = orc.fwdsurf(w.zgrid, v, w.periods, nthreads=8)
+        return orc.discrete_for_events(w.xx_deg, w.yy_deg, sv, m11, m12, m22, ev, tol=0.0,
+                                       grad=False, nthreads=8)["chi"]
+
+    big = np.argwhere(np.abs(ker[:, :, :-1]) > 0.05 * np.abs(ker).max())
+    nodes = big[np.random.default_rng(2002).choice(len(big), size=12, replace=False)]
+    h = 1e-2
+    ratios = []
+    for i, j, k in nodes:
+        vp, vm = vs0.copy(), vs0.copy()
+        vp[i, j, k] += h
+        vm[i, j, k] -= h
+        ratios.append((chi_of(vp) - chi_of(vm)) / (2 * h) / ker[i, j, k])
+    ratios = np.array(ratios)
+    assert np.all(np.abs(ratios - 1.0) <= 1e-3), ratios
