@@ -138,13 +138,13 @@ class Clocks:
 
 # DRAM bytes moved per algorithmic byte by batch_kernel<float>, from
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the same
-# kernel on the 151x151 / 3000-event case (50.645 GB moved for 73.430 GB of
-# algorithmic bytes).  The
-# algorithmic bytes count every cell of every sweep the reference performs;
-# the kernel skips cells that provably stay unchanged, so it moves less.
-# Traffic scales with cell updates, so a full launch moves algorithmic x this
-# ratio.
-TRAFFIC_PER_ALGO_BYTE = {"fp32": 50.645161e9 / 73.429994e9}
+# kernel on the 151x151 / 3000-event case (45.018 GB moved for 61.719 GB of
+# algorithmic bytes; the phase velocities are fwdsurf's of the random-field
+# model, as in the full workload).  The algorithmic bytes count every cell of
+# every sweep the reference performs; the kernel skips cells that provably
+# stay unchanged, so it moves less.  Traffic scales with cell updates, so a
+# full launch moves algorithmic x this ratio.
+TRAFFIC_PER_ALGO_BYTE = {"fp32": 45.018027e9 / 61.718708e9}
 
 
 def peaks():
