@@ -566,8 +566,8 @@ int sa_math_eval(int f, size_t n, const double* x, double* y, void* stream);
  * device ints.  All work is enqueued on `stream` (a cudaStream_t, NULL =
  * legacy stream); the call does not wait for the GPU.  Calls share the array:
  * calls that overlap on the GPU race and must be serialised.  The first call
- * on a device looks up the array's address; make it before any stream
- * capture. */
+ * in each context (after start-up or a device reset) looks up the array's
+ * address; make it before any stream capture. */
 int sa_eik_fwd_field_noalloc(int nx, int ny, const double* xx_deg, const double* yy_deg,
                              const double* spha, const double* sphb, const double* sphc,
                              const double* fun, double x0_deg, double y0_deg, double* T_out,

@@ -21,9 +21,9 @@
 //   * every call shares the array and it keeps the last call's contents, so
 //     calls that overlap on the GPU (different streams or host threads at the
 //     same time) race: serialise them;
-//   * the first call on a device looks up the array's device address
+//   * the first call in each context looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture (and again after a device reset).
 //
 // Compiled with -fmad=false: the grid, metric and geometry planes round as
 // the plan path's host arithmetic does, with correctly rounded sin and cos.
@@ -153,20 +153,41 @@ __global__ void noalloc_prep_kernel(int nx, int ny, const double* __restrict__ x
 
 std::mutex g_sym_mutex;
 unsigned char* g_sym_addr[64] = {};
+void* g_sym_ctx[64] = {};
 
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// The driver's cuCtxGetCurrent, through the runtime (no link to libcuda).
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn f = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<CtxGetCurrentFn>(nullptr);
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return f;
+}
+
+// Device address of g_noalloc_scratch in the current context, looked up on
+// the first call in each context (a device reset makes a new context and a
+// new module instance, so an address cached by device ordinal alone could
+// be stale).
 unsigned char* scratch_address(int device, cudaError_t* err) {
     *err = cudaSuccess;
     if (device < 0 || device >= 64) {
         *err = cudaErrorInvalidDevice;
         return nullptr;
     }
+    void* ctx = nullptr;
+    if (CtxGetCurrentFn f = ctx_get_current()) f(&ctx);
     std::lock_guard<std::mutex> lock(g_sym_mutex);
-    if (!g_sym_addr[device]) {
+    if (!g_sym_addr[device] || !ctx || ctx != g_sym_ctx[device]) {
         void* p = nullptr;
         *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (*err != cudaSuccess) return nullptr;
         g_sym_addr[device] = static_cast<unsigned char*>(p);
+        g_sym_ctx[device] = ctx;
     }
     return g_sym_addr[device];
 }
