@@ -103,6 +103,19 @@ CR_HD inline dd dd_add_d(dd a, double b) {
     s.lo += a.lo;
     return fast_two_sum(s.hi, s.lo);
 }
+// The same sums when |a.hi| >= |b.hi| (or a.hi == 0) and a and b do not
+// cancel: the leading error-free sum needs no ordering test, and the result
+// keeps the accurate sum's ~2^-105 relative error.
+CR_HD inline dd dd_add_ord(dd a, dd b) {
+    dd s = fast_two_sum(a.hi, b.hi);
+    s.lo += a.lo + b.lo;
+    return fast_two_sum(s.hi, s.lo);
+}
+CR_HD inline dd dd_add_d_ord(dd a, double b) {
+    dd s = fast_two_sum(a.hi, b);
+    s.lo += a.lo;
+    return fast_two_sum(s.hi, s.lo);
+}
 CR_HD inline dd dd_mul(dd a, dd b) {
     dd p = two_prod(a.hi, b.hi);
     p.lo = fma(a.hi, b.lo, fma(a.lo, b.hi, p.lo));
@@ -161,15 +174,15 @@ CR_HD inline double exp(double x) {
     tail = fma(h, tail, CR_IFACT4);
     tail = fma(h, tail, CR_IFACT3);
     tail = tail * (sq.hi * h);
-    dd s = dd_add(r, half_sq);
-    s = dd_add_d(s, tail);
+    // |r| <= ln2/8192 > r^2/2 > |tail|: ordered sums
+    dd s = dd_add_ord(r, half_sq);
+    s = dd_add_d_ord(s, tail);
     const int j1 = k & 63, j2 = (k >> 6) & 63, m = k >> 12;
     const dd T1 = {CR_TAB(kExpT1)[2 * j1], CR_TAB(kExpT1)[2 * j1 + 1]};
     const dd T2 = {CR_TAB(kExpT2)[2 * j2], CR_TAB(kExpT2)[2 * j2 + 1]};
     const dd P = dd_mul(T1, T2);
-    const dd res = dd_add(P, dd_mul(P, s));
-    const dd rn = fast_two_sum(res.hi, res.lo);
-    return scale2(rn.hi, m);
+    const dd res = dd_add_ord(P, dd_mul(P, s));   // |P s| < 2^-13 |P|; res normalised
+    return scale2(res.hi, m);
 }
 
 // ---- log ---------------------------------------------------------------------
@@ -256,17 +269,21 @@ CR_HD inline void sincos_reduced(double x, dd* s_out, dd* c_out, int* quadrant) 
     double ps = fma(z, CR_IFACT9, -CR_IFACT7);
     ps = fma(z, ps, CR_IFACT5);
     ps = ps * (z * z);
-    dd psd = dd_add_d(dd_neg(dd_mul(t2, dd{CR_INV6_HI, CR_INV6_LO})), ps);
-    const dd sint = dd_add(t, dd_mul(t, psd));
+    // |t| <= 2^-9: t^2/6 > |ps|, |t| > |t psd|, t^2/2 > |pc|: ordered sums
+    dd psd = dd_add_d_ord(dd_neg(dd_mul(t2, dd{CR_INV6_HI, CR_INV6_LO})), ps);
+    const dd sint = dd_add_ord(t, dd_mul(t, psd));
     double pc = fma(z, CR_IFACT8, -CR_IFACT6);
     pc = fma(z, pc, CR_IFACT4);
     pc = pc * (z * z);
-    const dd pcd = dd_add_d(dd{-0.5 * t2.hi, -0.5 * t2.lo}, pc);   // cos t - 1
+    const dd pcd = dd_add_d_ord(dd{-0.5 * t2.hi, -0.5 * t2.lo}, pc);   // cos t - 1
     const dd S = {CR_TAB(kSinT)[2 * j], CR_TAB(kSinT)[2 * j + 1]};
     const dd C = {CR_TAB(kCosT)[2 * j], CR_TAB(kCosT)[2 * j + 1]};
-    // sin r = S + (C sin t + S (cos t - 1)); cos r = C + (C (cos t - 1) - S sin t)
-    dd sr = dd_add(S, dd_add(dd_mul(C, sint), dd_mul(S, pcd)));
-    dd cr = dd_add(C, dd_add(dd_mul(C, pcd), dd_neg(dd_mul(S, sint))));
+    // sin r = S + (C sin t + S (cos t - 1)); cos r = C + (C (cos t - 1) - S sin t).
+    // C >= cos(pi/4): |C sin t| >= 0.7 |t| > t^2 > |S pcd|; S = 0 or S >=
+    // sin(1/256) > |t| + t^2 >= |C sint + S pcd|; C > 0.7 > 2^-8 > the cos
+    // correction.  C pcd and S sint are not ordered: accurate sum.
+    dd sr = dd_add_ord(S, dd_add_ord(dd_mul(C, sint), dd_mul(S, pcd)));
+    dd cr = dd_add_ord(C, dd_add(dd_mul(C, pcd), dd_neg(dd_mul(S, sint))));
     sr = {sg * sr.hi, sg * sr.lo};
     *s_out = sr;
     *c_out = cr;
@@ -279,8 +296,8 @@ CR_HD inline double sin(double x) {
     dd s, c;
     int q;
     sincos_reduced(x, &s, &c, &q);
-    dd v = (q == 0) ? s : (q == 1) ? c : (q == 2) ? dd_neg(s) : dd_neg(c);
-    return fast_two_sum(v.hi, v.lo).hi;
+    const dd v = (q == 0) ? s : (q == 1) ? c : (q == 2) ? dd_neg(s) : dd_neg(c);
+    return v.hi;   // normalised
 }
 
 CR_HD inline double cos(double x) {
@@ -290,8 +307,8 @@ CR_HD inline double cos(double x) {
     dd s, c;
     int q;
     sincos_reduced(x, &s, &c, &q);
-    dd v = (q == 0) ? c : (q == 1) ? dd_neg(s) : (q == 2) ? dd_neg(c) : s;
-    return fast_two_sum(v.hi, v.lo).hi;
+    const dd v = (q == 0) ? c : (q == 1) ? dd_neg(s) : (q == 2) ? dd_neg(c) : s;
+    return v.hi;   // normalised
 }
 
 // ---- x^-3 ------------------------------------------------------------------
@@ -327,8 +344,8 @@ CR_HD inline void sincos(double x, double* sn, double* cs) {
     sincos_reduced(x, &s, &c, &q);
     const dd vs = (q == 0) ? s : (q == 1) ? c : (q == 2) ? dd_neg(s) : dd_neg(c);
     const dd vc = (q == 0) ? c : (q == 1) ? dd_neg(s) : (q == 2) ? dd_neg(c) : s;
-    *sn = fast_two_sum(vs.hi, vs.lo).hi;
-    *cs = fast_two_sum(vc.hi, vc.lo).hi;
+    *sn = vs.hi;   // normalised
+    *cs = vc.hi;
 }
 
 }  // namespace cr
