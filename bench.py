@@ -348,6 +348,35 @@ def fp64_timing(a, w, sv, tt, wt, dev, stream, ctx, timed=True):
     return res, fi, ai
 
 
+def exact_gradient_timing(a, w, tt, wt, dev, stream, ctx):
+    """The exact gradient of the discrete forward model on the same
+    workload: an FP64 plan with the discrete adjoint (forward solves to a
+    fixed point), fwdsurf and the phase-velocity root derivatives, one fused
+    evaluation (sa_grad_run) per step."""
+    import torch
+    from surfattpp_b200 import inversion, preproc
+    cs = stream.cuda_stream
+    ev = w.events()
+    plan = preproc.ForwardAdjointPlan(w.xx_deg, w.yy_deg, w.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision="fp64", ctx=ctx, graph=True)
+    plan.set_adjoint("exact")
+    g = inversion.MisfitGradient(plan, w.zgrid, w.periods)
+    vs = torch.as_tensor(np.ascontiguousarray(w.vs3d), device=dev)
+    out = g.run(vs, tt, wt, stream=cs)
+    g.run(vs, tt, wt, out=out, stream=cs)
+    torch.cuda.synchronize()
+    steps = max(1, min(a.steps, 2))
+    ms = _event_ms(stream, lambda: g.run(vs, tt, wt, out=out, stream=cs), steps)
+    status = int(out["status"][0])
+    g.close()
+    plan.close()
+    return {"s_per_iter": ms * 1e-3, "unit": "s/iter", "steps": steps, "status": status,
+            "dtype": "f64",
+            "note": "fwdsurf, every forward solve to a fixed point, the exact discrete "
+                    "adjoint, dc/dvs from the phase-velocity roots, combination"}
+
+
 def per_solve_timing(w, svel, nev=4):
     """The plain per-solve form: FP64, one forward and one adjoint call per
     event through the single-solve C ABI with host arrays, as the reference's
@@ -675,6 +704,7 @@ def main():
     fp64, fi64, ai64 = fp64_timing(a, w, sv, tt, wt, dev, stream, ctx, timed=timed64)
     if timed64:
         extra["misfit_gradient"] = misfit_gradient_timing(a, w, plan, tt, wt, dev, stream)
+        extra["exact_gradient"] = exact_gradient_timing(a, w, tt, wt, dev, stream, ctx)
         extra["fp64_plain"] = fp64
         extra["fp64_per_solve"] = per_solve_timing(w, svel)
         extra["pde_smooth"] = pde_smooth_timing(a, w, dev, stream, peaks()[0])

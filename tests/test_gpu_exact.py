@@ -122,3 +122,45 @@ def test_exact_gradient_matches_differences(c2, gpu, orc):
         ratios.append((chi_of(vp) - chi_of(vm)) / (2 * h) / ker[i, j, k])
     ratios = np.array(ratios)
     assert np.all(np.abs(ratios - 1.0) <= 1e-3), ratios
+
+
+def test_discrete_adjoint_on_topography_and_deterministic(gpu, orc):
+    """General (anisotropic) metric from fractal topography: the winner's
+    metric comes from the per-period media planes.  With event-order
+    accumulation the result is reproducible bit for bit and agrees with the
+    atomic one."""
+    import torch
+    from surfattpp_b200 import preproc
+    from surfattpp_b200 import workloads as W
+    c4 = W.config4(level=61, nsta=41, nper=4, src_range=(3, 5), lam=8.0)
+    lon, lat, z = c4.meta["topo_raw"]
+    X, Y = np.meshgrid(c4.xx_deg, c4.yy_deg)
+    zg = orc.interp2d(lon, lat, z, X.ravel(), Y.ravel()).reshape(X.shape)
+    m11, m12, m22, _ = orc.topo_media(c4.xx_deg, c4.yy_deg, zg, np.full(c4.nper, 0.05))
+    svel, st = orc.fwdsurf(c4.zgrid, c4.vs3d, c4.periods, nthreads=8)
+    assert st.sum() == 0
+    ev = c4.events()
+    ev["tt_obs"] = np.asarray(ev["tt_obs"]) * 1.01
+    ref = orc.discrete_for_events(c4.xx_deg, c4.yy_deg, svel, m11, m12, m22, ev, tol=0.0,
+                                  nthreads=8)
+    plan = preproc.ForwardAdjointPlan(c4.xx_deg, c4.yy_deg, c4.nper, ev["evlo"], ev["evla"],
+                                      ev["iper"], ev["rec_ptr"], ev["rec_idx"], ev["stlo"],
+                                      ev["stla"], precision="fp64")
+    plan.set_adjoint("exact")
+    args = dict(m11=_t(m11), m12=_t(m12), m22=_t(m22))
+    tt, wt = _t(ev["tt_obs"]), _t(ev["weight"])
+    out = plan.run(_t(svel), tt, wt, **args)
+    torch.cuda.synchronize()
+    assert int(out["status"].max()) == 0
+    syn = out["syn"].cpu().numpy()[: ref["syn"].size]
+    assert np.max(np.abs(syn - ref["syn"]) / ref["syn"]) <= 1e-12
+    got = out["adj_s"].cpu().numpy()
+    scale = np.abs(ref["grad_svel"]).max()
+    assert scale > 0
+    assert np.max(np.abs(got - ref["grad_svel"])) <= 1e-9 * scale
+    plan.set_deterministic(True)
+    a = plan.run(_t(svel), tt, wt, **args)["adj_s"].clone()
+    b = plan.run(_t(svel), tt, wt, **args)["adj_s"].clone()
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert np.max(np.abs(a.cpu().numpy() - got)) <= 1e-12 * scale
