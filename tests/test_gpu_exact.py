@@ -164,3 +164,45 @@ def test_discrete_adjoint_on_topography_and_deterministic(gpu, orc):
     torch.cuda.synchronize()
     assert torch.equal(a, b)
     assert np.max(np.abs(a.cpu().numpy() - got)) <= 1e-12 * scale
+
+
+def test_exact_adjoint_edge_cases(c2, gpu, orc):
+    """An event without receivers, receivers outside the grid (NaN times, as
+    interp2d; they add nothing to the adjoint source) and a receiver on the
+    grid's edge, against the oracle; an FP32 plan refuses the exact adjoint."""
+    import torch
+    from surfattpp_b200 import _capi, preproc
+    w, ev, vs0 = c2
+    xx, yy = w.xx_deg, w.yy_deg
+    stlo = np.array([xx[5], xx[30], xx[0], xx[-1] + 1.0, xx[12]])
+    stla = np.array([yy[7], yy[33], yy[20], yy[10], yy[-1]])
+    evlo = np.array([xx[20], xx[10], xx[25]])
+    evla = np.array([yy[21], yy[30], yy[8]])
+    iper = np.array([0, 3, 7], np.int32)
+    rec_ptr = np.array([0, 4, 4, 8], np.int32)          # event 1 has no receivers
+    rec_idx = np.array([0, 1, 2, 3, 1, 2, 3, 4], np.int32)
+    e = dict(evlo=evlo, evla=evla, iper=iper, rec_ptr=rec_ptr, rec_idx=rec_idx, stlo=stlo,
+             stla=stla, weight=np.ones(8), tt_obs=np.full(8, 30.0))
+    sv0, _ = orc.fwdsurf(w.zgrid, vs0, w.periods, nthreads=8)
+    m11, m12, m22 = w.media()
+    ref = orc.discrete_for_events(xx, yy, sv0, m11, m12, m22, e, tol=0.0, nthreads=1)
+    plan = preproc.ForwardAdjointPlan(xx, yy, w.nper, evlo, evla, iper, rec_ptr, rec_idx, stlo,
+                                      stla, precision="fp64")
+    plan.set_adjoint("exact")
+    out = plan.run(_t(sv0), _t(e["tt_obs"]), _t(e["weight"]))
+    torch.cuda.synchronize()
+    syn = out["syn"].cpu().numpy()[:8]
+    assert np.array_equal(np.isnan(syn), np.isnan(ref["syn"]))
+    assert np.isnan(syn[3]) and np.isnan(syn[6])
+    ok = ~np.isnan(ref["syn"])
+    assert np.max(np.abs(syn[ok] - ref["syn"][ok]) / ref["syn"][ok]) <= 1e-12
+    got = out["adj_s"].cpu().numpy()
+    assert np.all(np.isfinite(got))
+    scale = np.abs(ref["grad_svel"]).max()
+    assert scale > 0
+    assert np.max(np.abs(got - ref["grad_svel"])) <= 1e-9 * scale
+    assert not np.any(got[3]) and not np.any(ref["grad_svel"][3])   # event 1's period
+    p32 = preproc.ForwardAdjointPlan(xx, yy, w.nper, evlo, evla, iper, rec_ptr, rec_idx, stlo,
+                                     stla, precision="fp32")
+    with pytest.raises(_capi.SAError):
+        p32.set_adjoint("exact")
