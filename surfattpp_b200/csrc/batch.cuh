@@ -162,14 +162,13 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     P.fy1 = fy1;
     // initial tau (src/eikonal_solver.cpp:118-129); FP32 stores u = tau - 1
     const S off = (sizeof(S) == sizeof(double)) ? S(0) : S(1);
-    for (size_t k = lane; k < n; k += 32) {
-        const int iy = (int)(k / nx), ix = (int)(k % nx);
+    for_cells(nx, n, lane, [&](size_t k, int ix, int iy) {
         const bool fixed = iy >= fy0 && iy <= fy1 && ix >= si.fix_x0 && ix <= si.fix_x1;
         const S v = (fixed ? S(1) : S(10)) - off;
         tau[k] = v;
         tst[k] = v;
         if (Pol::kFlags) flags[k] = 1;
-    }
+    });
     for (int iy = lane; iy < ny; iy += 32) {
         rng[iy] = make_int2(0, nx - 1);
         rng[ny + iy] = make_int2(0x7fffffff, -1);   // crng: nothing changed yet
@@ -352,8 +351,7 @@ __device__ inline void discrete_adjoint(const BatchArgs<double>& B, unsigned int
         fy1 = max(fy1, __shfl_xor_sync(FULL_MASK, fy1, o));
     }
     // 1. the winning stencils and their partials
-    for (size_t k = lane; k < n; k += 32) {
-        const int iy = (int)(k / nx), ix = (int)(k % nx);
+    for_cells(nx, n, lane, [&](size_t k, int ix, int iy) {
         const bool fixed = iy >= fy0 && iy <= fy1 && ix >= si.fix_x0 && ix <= si.fix_x1;
         WinD w{};
         w.ok = false;
@@ -374,7 +372,7 @@ __device__ inline void discrete_adjoint(const BatchArgs<double>& B, unsigned int
             Jy[k] = 0.0;
             DD[k] = make_double2(0.0, 0.0);
         }
-    }
+    });
     __syncwarp();
     // 2. the receivers' explicit fun0 term, then the adjoint source g in the
     // tau plane (tau is no longer needed)
@@ -408,8 +406,7 @@ __device__ inline void discrete_adjoint(const BatchArgs<double>& B, unsigned int
     __syncwarp();
     // 3. the sweep weights at every cell: the partials of the neighbours'
     // winners that read this cell
-    for (size_t k = lane; k < n; k += 32) {
-        const int iy = (int)(k / nx), ix = (int)(k % nx);
+    for_cells(nx, n, lane, [&](size_t k, int ix, int iy) {
         const double wxm = (ix > 0 && (fl[k - 1] & 3u) == 2u) ? Jx[k - 1] : 0.0;
         const double wxp = (ix < nx - 1 && (fl[k + 1] & 3u) == 1u) ? Jx[k + 1] : 0.0;
         const double wym = (iy > 0 && ((fl[k - nx] >> 2) & 3u) == 2u) ? Jy[k - nx] : 0.0;
@@ -417,7 +414,7 @@ __device__ inline void discrete_adjoint(const BatchArgs<double>& B, unsigned int
         st4(PK + k, wxm, wxp, wym, wyp);
         lam[k] = 0.0;
         tst[k] = 0.0;
-    }
+    });
     for (int iy = lane; iy < ny; iy += 32) {
         rng[iy] = make_int2(0, nx - 1);
         rng[ny + iy] = make_int2(0x7fffffff, -1);
@@ -594,8 +591,7 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                 double* P_Tst = reinterpret_cast<double*>(P_tst);
                 // face fluxes (src/eikonal_solver.cpp:404-441): a2(ix) is a1(ix+1)
                 // and b2(iy) is b1(iy+1), identical expressions in the reference
-                for (size_t k = lane; k < n; k += 32) {
-                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                for_cells(nx, n, lane, [&](size_t k, int ix, int iy) {
                     const bool interior = ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2;
                     double a1p = 0, a2m = 0, b1p = 0, b2m = 0, d = 0;
                     if (interior) {
@@ -616,7 +612,7 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                     const double v0 = interior ? 100.0 : 0.0;   // :446-449
                     P_Ta[k] = v0;
                     P_Tst[k] = v0;
-                }
+                });
                 for (int iy = lane; iy < ny; iy += 32) {
                     P_rng[iy] = make_int2(1, nx - 2);
                     P_rng[ny + iy] = make_int2(0x7fffffff, -1);
@@ -653,22 +649,24 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                 // (FP32 path: reciprocals instead of divisions)
                 const double idx = 1.0 / g.dx, idy = 1.0 / g.dy;
                 const double i4dx = 1.0 / (4.0 * g.dx), i4dy = 1.0 / (4.0 * g.dy);
+                // (isotropic media: no cross term, whose c is zero)
                 auto fA = [&](int ix, int iy) -> double {
                     const size_t k = (size_t)iy * nx + ix;
-                    const double av = ISO ? B.a_a_row64[iy] : 0.5 * (a_a[k] + a_a[k - 1]);
-                    const double cv = ISO ? 0.0 : 0.5 * (c_a[k] + c_a[k - 1]);
+                    if constexpr (ISO) return -(T[k] - T[k - 1]) * idx * B.a_a_row64[iy];
+                    const double av = 0.5 * (a_a[k] + a_a[k - 1]);
+                    const double cv = 0.5 * (c_a[k] + c_a[k - 1]);
                     return -(T[k] - T[k - 1]) * idx * av
                            + (T[k + nx] - T[k - nx] + T[k - 1 + nx] - T[k - 1 - nx]) * i4dy * cv;
                 };
                 auto fB = [&](int ix, int iy) -> double {
                     const size_t k = (size_t)iy * nx + ix;
-                    const double bv = ISO ? B.b_iso64 : 0.5 * (b_p[k] + b_p[k - nx]);
-                    const double cv = ISO ? 0.0 : 0.5 * (c_a[k] + c_a[k - nx]);
+                    if constexpr (ISO) return -(T[k] - T[k - nx]) * idy * B.b_iso64;
+                    const double bv = 0.5 * (b_p[k] + b_p[k - nx]);
+                    const double cv = 0.5 * (c_a[k] + c_a[k - nx]);
                     return -(T[k] - T[k - nx]) * idy * bv
                            + (T[k + 1] - T[k - 1] + T[k + 1 - nx] - T[k - 1 - nx]) * i4dx * cv;
                 };
-                for (size_t k = lane; k < n; k += 32) {
-                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                for_cells(nx, n, lane, [&](size_t k, int ix, int iy) {
                     const bool interior = ix >= 1 && ix <= nx - 2 && iy >= 1 && iy <= ny - 2;
                     float c0 = 0.f, wxm = 0.f, wxp = 0.f, wym = 0.f, wyp = 0.f;
                     if (interior) {
@@ -693,7 +691,7 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                     const float v0 = interior ? 100.f : 0.f;
                     P_Ta[k] = v0;
                     P_tst[k] = v0;
-                }
+                });
                 for (int iy = lane; iy < ny; iy += 32) {
                     P_rng[iy] = make_int2(1, nx - 2);
                     P_rng[ny + iy] = make_int2(0x7fffffff, -1);
@@ -761,8 +759,7 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                 double* con = B.out.contrib
                                   ? B.out.contrib + (size_t)(e - B.out.contrib_e0) * n
                                   : nullptr;
-                for (size_t k = lane; k < n; k += 32) {
-                    const int iy = (int)(k / nx), ix = (int)(k % nx);
+                for_cells(nx, n, lane, [&](size_t k, int ix, int iy) {
                     double v = (double)TaS[k];
                     if (ix >= mb.ix_lo && ix <= mb.ix_hi && iy >= mb.iy_lo && iy <= mb.iy_hi) v = 0.0;
                     if (!isfinite(v)) finite = false;
@@ -770,7 +767,7 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                     const double c = v * inv3[k];
                     if (con) con[k] = c;
                     else if (acc && c != 0.0) atomicAdd(acc + k, c);
-                }
+                });
             }
             if (!__all_sync(FULL_MASK, finite)) status = ST_NONFINITE;
             __syncwarp();

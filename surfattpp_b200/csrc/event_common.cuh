@@ -189,6 +189,22 @@ __device__ inline MaskBox mask_box(const Grid& g, double x0, double y0) {
     return m;
 }
 
+// Per-lane walk over the cells of an nx-wide plane of n cells in warp
+// stride: f(k, ix, iy) at k = lane, lane + 32, ...  The column and row are
+// carried along instead of divided out of k (a 64-bit division per cell).
+template <class F>
+__device__ __forceinline__ void for_cells(int nx, size_t n, int lane, F&& f) {
+    int ix = lane % nx, iy = lane / nx;
+    for (size_t k = lane; k < n; k += 32) {
+        f(k, ix, iy);
+        ix += 32;
+        while (ix >= nx) {
+            ix -= nx;
+            iy++;
+        }
+    }
+}
+
 __device__ __forceinline__ unsigned int warp_next_event(unsigned int* queue) {
     unsigned int e = 0;
     if ((threadIdx.x & 31) == 0) e = atomicAdd(queue, 1u);
