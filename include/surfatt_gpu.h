@@ -39,7 +39,8 @@ enum sa_status {
     SA_ERR_NOCONV = 3,     /* a sweep hit its iteration cap (reference: stderr warning) */
     SA_ERR_NOROOT = 4,     /* dispersion root not found (reference: stop 'Dispersion calculation failed') */
     SA_ERR_NONFINITE = 5,  /* NaN/Inf in an output field */
-    SA_ERR_NOMEM = 6       /* device allocation failed */
+    SA_ERR_NOMEM = 6,      /* device allocation failed */
+    SA_ERR_TEAM = 7        /* a cooperative sweep's wait gave up (FP32 tail teams; no reference counterpart) */
 };
 
 enum sa_precision { SA_FP64 = 0, SA_FP32 = 1 };
@@ -167,25 +168,30 @@ int sa_forward_for_events(sa_ctx* ctx, int precision, int nx, int ny, int nper,
 /* No counterpart in the reference, which has no GPU launch to configure.
  * Autotunes this plan's batch-kernel launch on its own workload: every
  * candidate configuration -- for FP32 plans the forward sweep step rolled or
- * unrolled times the adjoint sweep loading 2 or 3 steps ahead, for either
- * precision all or three quarters of the resident event slots -- runs the
- * plan's evaluation (arguments as sa_plan_forward_adjoint; adj_s may be NULL)
- * twice and its second batch launch is timed.  The fastest is kept by the
- * plan and by plans of the same grid size (nx, ny, precision) created later
- * on this context.  ms_out (may be NULL) receives up to 8 timings, n_out the
- * number of candidates, choice the index of the one kept.  FP64 outputs do
- * not depend on the configuration; FP32 variants may round differently (the
- * compiler fuses multiply-adds per variant), within the FP32 path's accuracy.
- * Synchronises `stream`. */
+ * unrolled times the adjoint sweep loading 2 or 3 steps ahead times tail
+ * teams on or off, for either precision all or three quarters of the resident
+ * event slots, with tail teams also a quarter (one solve per block) -- runs
+ * the plan's evaluation (arguments as sa_plan_forward_adjoint; adj_s may be
+ * NULL) twice and its second batch launch is timed.  The fastest is kept by
+ * the plan and by plans of the same grid size (nx, ny, precision) created
+ * later on this context.  ms_out (may be NULL) receives up to
+ * SA_TUNE_MAX_CANDIDATES timings, n_out the number of candidates, choice the
+ * index of the one kept.  Outputs do not depend on the configuration (FP32:
+ * every variant rounds the same explicit operations; adj_s up to the order
+ * of its FP64 atomic sums).  Synchronises `stream`. */
+#define SA_TUNE_MAX_CANDIDATES 32
 int sa_plan_autotune(sa_plan* plan, const double* svel, const double* m11, const double* m12,
                      const double* m22, const double* tt_obs, const double* weight,
                      int calc_adj, double* adj_s, float* ms_out, int* n_out, int* choice,
                      void* stream);
 
-/* The plan's launch configuration: variant (0-3 for FP32, bit 0 = unrolled
- * forward step, bit 1 = adjoint lead 3; 0 for FP64), event slots in use (set:
- * 0 = all; more than allocated = all), and slots allocated.  Setting it
- * (e.g. a configuration tuned in an earlier run) affects this plan only. */
+/* The plan's launch configuration: variant (0-7 for FP32, bit 0 = unrolled
+ * forward step, bit 1 = adjoint lead 3, bit 2 = tail teams: warps whose
+ * queue pull finds no event left join the solves still running in their
+ * block; 0 for FP64), event slots in use (set: 0 = all; more than allocated =
+ * all; with tail teams the other resident warps start as team members), and
+ * slots allocated.  Setting it (e.g. a configuration tuned in an earlier run)
+ * affects this plan only. */
 int sa_plan_set_tune(sa_plan* plan, int variant, int active_slots);
 int sa_plan_get_tune(sa_plan* plan, int* variant, int* active_slots, int* nslots);
 

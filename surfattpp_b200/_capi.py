@@ -14,10 +14,11 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 # SURFATT_GPU_LIB selects another build of the same library (same C ABI).
 LIB_PATH = os.environ.get("SURFATT_GPU_LIB") or os.path.join(_HERE, "libsurfatt_gpu.so")
 
-SA_OK, SA_ERR_ARG, SA_ERR_CUDA, SA_ERR_NOCONV, SA_ERR_NOROOT, SA_ERR_NONFINITE, SA_ERR_NOMEM = range(7)
+(SA_OK, SA_ERR_ARG, SA_ERR_CUDA, SA_ERR_NOCONV, SA_ERR_NOROOT, SA_ERR_NONFINITE, SA_ERR_NOMEM,
+ SA_ERR_TEAM) = range(8)
 SA_FP64, SA_FP32 = 0, 1
 STATUS_NAMES = {0: "SA_OK", 1: "SA_ERR_ARG", 2: "SA_ERR_CUDA", 3: "SA_ERR_NOCONV",
-                4: "SA_ERR_NOROOT", 5: "SA_ERR_NONFINITE", 6: "SA_ERR_NOMEM"}
+                4: "SA_ERR_NOROOT", 5: "SA_ERR_NONFINITE", 6: "SA_ERR_NOMEM", 7: "SA_ERR_TEAM"}
 
 # Every symbol include/surfatt_gpu.h declares.
 EXPORTED = (

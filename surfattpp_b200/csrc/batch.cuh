@@ -55,7 +55,7 @@ struct BatchArgs {
 // forward operands (PK) and the packed adjoint coefficients share one region:
 // the forward planes are dead once T is formed.
 struct SlotLayout {
-    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, flags, rng, total;
+    size_t tau, tst, T, delta, PK, AQ, DD, W, C0, Ta, sadj, syn, flags, rng, team, total;
 };
 template <class S>
 __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
@@ -90,22 +90,208 @@ __host__ __device__ inline SlotLayout slot_layout(int nx, int ny, int maxr) {
     // current sweep, [ny, 2 ny) cells changed in the current iteration,
     // [2 ny, 3 ny) the adjoint's ranges for the next sweep
     L.rng = take(3 * (size_t)ny * sizeof(int2));
+    // tail teams (systolic.cuh, Team): per strip its record and the last
+    // sweep's L1 partials of its 32 lanes
+    const size_t nstrip = ((size_t)ny + 31) / 32;
+    L.team = take(nstrip * sizeof(int4) + nstrip * 32 * sizeof(double));
     L.total = o;
     return L;
 }
 
 // Launch variants of the FP32 kernel (kBatchVariants, chosen per plan by
 // sa_plan_autotune): bit 0 = unrolled forward step (else one rolled copy),
-// bit 1 = FP32 adjoint loads 3 steps ahead (else 2).  The FP64 kernel has
-// variant 0 only.
+// bit 1 = FP32 adjoint loads 3 steps ahead (else 2), bit 2 = tail teams
+// (below).  The FP64 kernel has variant 0 only.
 __host__ __device__ constexpr bool variant_fwd_rolled(int v) { return (v & 1) == 0; }
 __host__ __device__ constexpr int variant_adj_lead(int v) { return (v & 2) ? 3 : 2; }
+__host__ __device__ constexpr bool variant_teams(int v) { return (v & 4) != 0; }
+
+// Tail teams (FP32 kernel, variant bit 2).  A warp whose queue pull finds no
+// event left offers itself to the warps of its block still solving one; at
+// its next iteration start such an owner takes the warps on offer, and the
+// team marches that iteration's four sweeps together (systolic.cuh, Team).
+// The owner keeps its team to the end of the forward (or adjoint)
+// iterations, then releases it.  Results are those of the warp alone (the
+// same cell updates; the L1 sums added per strip in strip order).  Every
+// wait is bounded; one that gives up sets the block's error flag, after
+// which no team forms and the events report ST_TEAM.
+constexpr int kTeamPolBytes = 256;
+struct TeamRec {
+    unsigned long long word[4];   // the members' progress words (systolic.cuh)
+    double linf[4];               // members' Linf of the iteration
+    int4* sinfo;                  // the owner's strip records and L1 partials
+    double* sums;
+    alignas(16) unsigned char pol[kTeamPolBytes];   // the owner's sweep policy
+};
+struct BlockTeams {
+    unsigned idle;      // bit w: warp w is on offer
+    int busy;           // warps that may still take a team
+    int err;
+    unsigned mail[4];   // per warp: job from an owner (0: none)
+    TeamRec rec[4];     // per owner warp
+};
+constexpr unsigned kMailRelease = 0x80000000u;
+constexpr long long kOfferNs = 30000000000ll;   // an offer is withdrawn after 30 s
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.cta.shared.u32 %0, [%1];"
+                 : "=r"(v)
+                 : "r"((unsigned)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.cta.shared.u32 [%0], %1;"
+                 :
+                 : "r"((unsigned)__cvta_generic_to_shared(p)), "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ unsigned mail_job(int owner, int role, int W, int kind) {
+    return 1u | (unsigned)owner << 1 | (unsigned)role << 3 | (unsigned)W << 5 |
+           (unsigned)kind << 8;
+}
+
+// Owner, at an iteration start: takes the warps on offer, posts the
+// iteration to its members and returns the team (W = 1: alone).  kind 0 =
+// forward sweeps, 1 = adjoint sweeps.
+template <class Pol>
+__device__ __forceinline__ Team team_begin(BlockTeams* bt, unsigned& helpers, int kind,
+                                           const Pol& P, int ny) {
+    const int lane = threadIdx.x & 31, me = threadIdx.x >> 5;
+    TeamRec& R = bt->rec[me];
+    // the slot's team region follows its range planes (slot_layout)
+    unsigned char* tr =
+        reinterpret_cast<unsigned char*>(P.rng) + align_up(3 * (size_t)ny * sizeof(int2), 256);
+    int4* sinfo = reinterpret_cast<int4*>(tr);
+    double* sums = reinterpret_cast<double*>(tr + (size_t)((ny + 31) / 32) * sizeof(int4));
+    Team T{1, 0, R.word, sinfo, sums, &bt->err};
+    const bool ok = __shfl_sync(FULL_MASK, *(volatile int*)&bt->err, 0) == 0;
+    if (ok && __popc(helpers) < 3) {
+        unsigned got = 0;
+        if (lane == 0) {
+            unsigned m = *(volatile unsigned*)&bt->idle & ~(1u << me);
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                if (atomicAnd(&bt->idle, ~(1u << b)) & (1u << b)) got |= 1u << b;
+            }
+        }
+        helpers |= __shfl_sync(FULL_MASK, got, 0);
+    }
+    if (!ok || helpers == 0) return T;
+    T.W = 1 + __popc(helpers);
+    static_assert(sizeof(Pol) <= kTeamPolBytes, "sweep policy larger than its team copy");
+    if (lane == 0) {
+        *reinterpret_cast<Pol*>(R.pol) = P;
+        R.sinfo = sinfo;
+        R.sums = sums;
+    }
+    if (lane < T.W) R.word[lane] = 0ull;
+    __threadfence_block();
+    __syncwarp();
+    if (lane == 0) {
+        int role = 1;
+        for (unsigned m = helpers; m; m &= m - 1)
+            st_release_u32(&bt->mail[__ffs(m) - 1], mail_job(me, role++, T.W, kind));
+    }
+    return T;
+}
+
+// Owner, after the team's sweeps: waits for every member, folds in their
+// Linf and forms the L1 sum in strip order (as the warp alone adds it).
+__device__ __forceinline__ void team_end(BlockTeams* bt, const Team& T, int nstrip, double& l1,
+                                         double& linf) {
+    const int lane = threadIdx.x & 31, me = threadIdx.x >> 5;
+    for (int r = 1; r < T.W; r++) {
+        team_wait(T, r, kTeamEnd - 1, kStripDone);
+        linf = fmax(linf, bt->rec[me].linf[r]);
+    }
+    double s = 0.0;
+    for (int j = 0; j < nstrip; j++) s += T.sums[j * 32 + lane];
+    l1 = s;
+}
+
+// One team iteration (four sweeps) of a member: out of line, so that owner
+// and helpers run one copy of the team sweeps (two copies of the long
+// forward step in flight on an SM thrash its instruction cache).  Returns the
+// member's Linf; the L1 partials go to the strip sums.
+template <class Pol>
+__device__ __noinline__ double team_sweeps(const Pol* pol, const Team T) {
+    Pol P = *pol;
+    double l1 = 0.0, linf = 0.0;
+    for (int sw = 0; sw < 4; sw++)
+        systolic_sweep(P, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf, &T, sw);
+    return linf;
+}
+
+__device__ __forceinline__ void team_release(BlockTeams* bt, unsigned& helpers) {
+    if ((threadIdx.x & 31) == 0)
+        for (unsigned m = helpers; m; m &= m - 1) st_release_u32(&bt->mail[__ffs(m) - 1], kMailRelease);
+    helpers = 0;
+    __syncwarp();
+}
+
+// A warp without events: on offer until every warp of the block is done;
+// runs the iterations its owners post.
+template <class PolF, class PolA>
+__device__ __forceinline__ void team_serve(BlockTeams* bt) {
+    const int lane = threadIdx.x & 31, me = threadIdx.x >> 5;
+    if (lane == 0) atomicOr(&bt->idle, 1u << me);
+    __syncwarp();
+    long long t0 = __shfl_sync(FULL_MASK, global_ns(), 0);
+    bool offered = true;
+    for (;;) {
+        const unsigned m = __shfl_sync(FULL_MASK, ld_acquire_u32(&bt->mail[me]), 0);
+        const long long now = __shfl_sync(FULL_MASK, global_ns(), 0);
+        if (m == 0u) {
+            if (__shfl_sync(FULL_MASK, *(volatile int*)&bt->busy, 0) == 0) break;
+            if (now - t0 > (offered ? kOfferNs : kTeamWaitNs)) {
+                if (!offered) {   // taken, but no job came
+                    if (lane == 0) atomicExch(&bt->err, 1);
+                    break;
+                }
+                // withdraw the offer; if an owner took it already, its job follows
+                unsigned old = 0;
+                if (lane == 0) old = atomicAnd(&bt->idle, ~(1u << me));
+                if (!((__shfl_sync(FULL_MASK, old, 0) >> me) & 1u)) {
+                    offered = false;
+                    t0 = now;
+                    continue;
+                }
+                break;
+            }
+            __nanosleep(256);
+            continue;
+        }
+        if (lane == 0) bt->mail[me] = 0u;
+        __syncwarp();
+        t0 = now;
+        if (m == kMailRelease) {
+            if (lane == 0) atomicOr(&bt->idle, 1u << me);
+            offered = true;
+            __syncwarp();
+            continue;
+        }
+        const int o = (m >> 1) & 3, role = (m >> 3) & 3, W = (m >> 5) & 7, kind = (m >> 8) & 1;
+        TeamRec& R = bt->rec[o];
+        const Team T{W, role, R.word, R.sinfo, R.sums, &bt->err};
+        double linf = kind == 0 ? team_sweeps(reinterpret_cast<const PolF*>(R.pol), T)
+                                : team_sweeps(reinterpret_cast<const PolA*>(R.pol), T);
+        linf = warp_max(linf);
+        if (lane == 0) R.linf[role] = linf;
+        __threadfence_block();
+        __syncwarp();
+        if (lane == 0) st_release_u64(&R.word[role], team_word(kTeamEnd, 0));
+        offered = false;
+    }
+}
 
 template <class S, bool ISO, int VAR>
 __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo& si, int ip,
                                             int src, S* tau, S* tst, Q4<S>* pk,
                                             unsigned char* flags, int2* rng, double* T,
-                                            int& iters, int& status) {
+                                            int& iters, int& status, BlockTeams* bt) {
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
     const size_t n = (size_t)nx * ny;
@@ -180,14 +366,35 @@ __device__ __forceinline__ double fwd_solve(const BatchArgs<S>& B, const SrcInfo
     // for the exact discrete adjoint, a fixed point (an iteration in which
     // no cell changed: every cell's change times T0 is zero, T0 > 0 off the
     // fixed source cells)
+    unsigned helpers = 0;   // tail team (FP32 variants with teams)
     for (int iter = 0; iter < 2000; iter++) {
         double l1 = 0.0, linf = 0.0;
-        for (int sw = 0; sw < 4; sw++) systolic_sweep(P, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
+        if constexpr (variant_teams(VAR) && sizeof(S) == sizeof(float)) {
+            // (alone: the sweeps of the variants without teams, the same code)
+            const Team tm = bt ? team_begin(bt, helpers, 0, P, ny)
+                               : Team{1, 0, nullptr, nullptr, nullptr, nullptr};
+            if (tm.W > 1) {
+                linf = team_sweeps(reinterpret_cast<const Pol*>(bt->rec[threadIdx.x >> 5].pol), tm);
+                team_end(bt, tm, (ny + 31) >> 5, l1, linf);
+            } else {
+                for (int sw = 0; sw < 4; sw++)
+                    systolic_sweep(P, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
+            }
+        } else {
+            for (int sw = 0; sw < 4; sw++)
+                systolic_sweep(P, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
+        }
         iters = iter + 1;
         const double L1 = warp_sum(l1) / (double)(nx * ny);
         const double Linf = warp_max(linf);
         if (B.discrete ? (Linf == 0.0) : (L1 < 1e-4 && Linf < 1e-4)) break;
         if (iter == 1999) status = ST_NOCONV;
+    }
+    if constexpr (variant_teams(VAR) && sizeof(S) == sizeof(float)) {
+        if (bt) {
+            team_release(bt, helpers);
+            if (__shfl_sync(FULL_MASK, *(volatile int*)&bt->err, 0)) status = ST_TEAM;
+        }
     }
     // T = tau * T0 in FP64 (src/eikonal_solver.cpp:317)
     const double* G64 = B.G64 + (size_t)src * n;
@@ -485,7 +692,8 @@ __device__ inline void discrete_adjoint(const BatchArgs<double>& B, unsigned int
 // a single-grid launch it is zero between events by construction).
 template <class S, bool ISO, int VAR>
 __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int e,
-                                            unsigned char* base, bool clear_delta = false) {
+                                            unsigned char* base, bool clear_delta = false,
+                                            BlockTeams* bt = nullptr) {
     const int lane = threadIdx.x & 31;
     const Grid& g = B.g;
     const int nx = g.nx, ny = g.ny;
@@ -511,7 +719,7 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
         if (B.mode != MODE_ADJ_ONLY) {
             int iters = 0;
             fwd_solve<S, ISO, VAR>(B, si, ip, B.ev.src[e], P_tau, P_tst, P_pk, P_fl, P_rng,
-                                   P_T, iters, status);
+                                   P_T, iters, status, bt);
             if (lane == 0 && B.out.fwd_iters) B.out.fwd_iters[e] = iters;
             if (B.out.T_out)
                 for (size_t k = lane; k < n; k += 32) B.out.T_out[(size_t)e * n + k] = P_T[k];
@@ -708,11 +916,27 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                 Q.rng = P_rng;
                 Q.crng = P_rng + ny;
                 Q.rng2 = P_rng + 2 * ny;
+                unsigned helpers = 0;   // tail team (variants with teams)
                 if (big)
                     for (int iter = 0; iter < 1000; iter++) {
                         double l1 = 0.0, linf = 0.0;
-                        for (int sw = 0; sw < 4; sw++)
-                            systolic_sweep(Q, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
+                        if constexpr (variant_teams(VAR)) {
+                            const Team tm = bt ? team_begin(bt, helpers, 1, Q, ny)
+                                               : Team{1, 0, nullptr, nullptr, nullptr, nullptr};
+                            if (tm.W > 1) {
+                                using PolA = AdjPolicyW32<variant_adj_lead(VAR)>;
+                                linf = team_sweeps(
+                                    reinterpret_cast<const PolA*>(bt->rec[threadIdx.x >> 5].pol), tm);
+                                team_end(bt, tm, (ny - 2 + 31) >> 5, l1, linf);
+                            } else {
+                                for (int sw = 0; sw < 4; sw++)
+                                    systolic_sweep(Q, sweep_xd(sw), sweep_yd(sw), sw == 3, l1,
+                                                   linf);
+                            }
+                        } else {
+                            for (int sw = 0; sw < 4; sw++)
+                                systolic_sweep(Q, sweep_xd(sw), sweep_yd(sw), sw == 3, l1, linf);
+                        }
                         iters = iter + 1;
                         const double L1 = warp_sum(l1) / (double)(nx * ny);
                         const double Linf = warp_max(linf);
@@ -731,6 +955,12 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
                         const double vmax = warp_max((double)vm);
                         if (Linf <= 4.0 * 5.960464477539063e-08 * vmax) break;
                     }
+                if constexpr (variant_teams(VAR)) {
+                    if (bt) {
+                        team_release(bt, helpers);
+                        if (__shfl_sync(FULL_MASK, *(volatile int*)&bt->err, 0)) status = ST_TEAM;
+                    }
+                }
             }
             if (lane == 0 && B.out.adj_iters && pass == 0) B.out.adj_iters[e] = iters;
             if (lane == 0) spread_delta(g, B.ev, r0, nr, P_sadj, P_delta, true);
@@ -782,14 +1012,46 @@ __device__ __forceinline__ void batch_event(const BatchArgs<S>& B, unsigned int 
 // scratch slot pulls events from the queue until it is empty.
 template <class S, bool ISO, int VAR>
 __device__ __forceinline__ void batch_body(const BatchArgs<S>& B) {
-    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (slot >= B.sc.nslots) return;
-    unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
-    for (;;) {
-        const unsigned int qi = warp_next_event(B.sc.queue);
-        if (qi >= (unsigned)B.ev.ne) break;
-        const unsigned int e = B.sc.order ? (unsigned)B.sc.order[qi] : qi;
-        batch_event<S, ISO, VAR>(B, e, base);
+    if constexpr (variant_teams(VAR) && sizeof(S) == sizeof(float)) {
+        // tail teams: block-shared offers, jobs and progress words.  Slots
+        // are numbered across the blocks first (warp w of block b: slot
+        // w * blocks + b), so that fewer slots in use than warps leave every
+        // block with owners and helpers (one slot per block: a block per solve)
+        const int slot = (int)(threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x;
+        __shared__ BlockTeams bt;
+        if (threadIdx.x == 0) {
+            int owners = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+                owners += (w * (int)gridDim.x + (int)blockIdx.x) < B.sc.nslots;
+            bt.idle = 0u;
+            bt.busy = owners;
+            bt.err = 0;
+            for (int w = 0; w < 4; w++) bt.mail[w] = 0u;
+        }
+        __syncthreads();
+        using PolF = FwdPolicyDelta32<ISO, variant_fwd_rolled(VAR)>;
+        using PolA = AdjPolicyW32<variant_adj_lead(VAR)>;
+        if (slot < B.sc.nslots) {
+            unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
+            for (;;) {
+                const unsigned int qi = warp_next_event(B.sc.queue);
+                if (qi >= (unsigned)B.ev.ne) break;
+                const unsigned int e = B.sc.order ? (unsigned)B.sc.order[qi] : qi;
+                batch_event<S, ISO, VAR>(B, e, base, false, &bt);
+            }
+            if ((threadIdx.x & 31) == 0) atomicSub(&bt.busy, 1);
+        }
+        team_serve<PolF, PolA>(&bt);
+    } else {
+        const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (slot >= B.sc.nslots) return;
+        unsigned char* base = B.sc.base + (size_t)slot * B.sc.slot_bytes;
+        for (;;) {
+            const unsigned int qi = warp_next_event(B.sc.queue);
+            if (qi >= (unsigned)B.ev.ne) break;
+            const unsigned int e = B.sc.order ? (unsigned)B.sc.order[qi] : qi;
+            batch_event<S, ISO, VAR>(B, e, base);
+        }
     }
 }
 

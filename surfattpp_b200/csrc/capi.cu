@@ -466,6 +466,7 @@ BatchDesc plan_desc(sa_plan* P, bool general) {
     d.ev.stla = P->stla.p;
     d.ev.cos_stla = P->cos_stla.p;
     d.sc.nslots = (P->active > 0 && P->active < P->nslots) ? P->active : P->nslots;
+    d.sc.nwarps = P->nslots;
     d.sc.slot_bytes = P->slot_bytes;
     d.variant = P->prec == SA_FP32 ? P->variant : 0;
     d.discrete = P->discrete;
@@ -589,15 +590,15 @@ extern "C" int sa_plan_create(sa_ctx* ctx, int precision, int nx, int ny, int np
 extern "C" void sa_plan_destroy(sa_plan* plan) { delete plan; }
 
 // Launch-configuration autotuner.  Candidates: every FP32 launch variant
-// (rolled / unrolled forward step x adjoint load lead 2 / 3; FP64: the one
-// kernel) x all or three quarters of the resident event slots.  Each
+// (rolled / unrolled forward step x adjoint load lead 2 / 3 x tail teams off
+// / on; FP64: the one kernel) x all or three quarters of the resident event
+// slots, and with tail teams also a quarter (one solve per block).  Each
 // candidate runs the plan's own evaluation twice, the second timed with
 // CUDA events around the batch kernel; the fastest is kept for this plan and
-// for plans of the same grid size created later on this context.  FP64
-// results do not depend on the choice (only the atomic accumulation order of
-// adj_s varies); the FP32 variants run the same arithmetic, but the compiler
-// may fuse multiply-adds differently in each, so their results differ by
-// FP32 rounding.
+// for plans of the same grid size created later on this context.  Results do
+// not depend on the choice: the FP32 sweeps spell out every rounding, so all
+// variants compute the same values (only the atomic accumulation order of
+// adj_s varies).
 extern "C" int sa_plan_autotune(sa_plan* P, const double* svel, const double* m11,
                                 const double* m12, const double* m22, const double* tt_obs,
                                 const double* weight, int calc_adj, double* adj_s,
@@ -611,8 +612,15 @@ extern "C" int sa_plan_autotune(sa_plan* P, const double* svel, const double* m1
     SA_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const int nvar = P->prec == SA_FP32 ? kBatchVariants : 1;
-    const int slots[2] = {0, std::max(1, P->nslots * 3 / 4)};
-    const int ncand = 2 * nvar;
+    // (variant, slots in use): all or three quarters; with tail teams also a
+    // quarter (one solve per block, its three other warps as the team)
+    std::vector<std::pair<int, int>> cand;
+    for (int v = 0; v < nvar; v++) {
+        cand.push_back({v, 0});
+        cand.push_back({v, std::max(1, P->nslots * 3 / 4)});
+        if (v & 4) cand.push_back({v, std::max(1, P->nslots / 4)});
+    }
+    const int ncand = (int)cand.size();
     const bool had_timing = P->timing;
     if (!P->tk0) {
         SA_CUDA(cudaEventCreate(&P->tk0));
@@ -622,8 +630,8 @@ extern "C" int sa_plan_autotune(sa_plan* P, const double* svel, const double* m1
     float best = 0.f;
     int best_c = 0;
     for (int c = 0; c < ncand; c++) {
-        P->variant = c % nvar;
-        P->active = slots[c / nvar];
+        P->variant = cand[c].first;
+        P->active = cand[c].second;
         float ms = 0.f;
         for (int rep = 0; rep < 2; rep++) {
             const int rc = plan_enqueue(P, svel, m11, m12, m22, tt_obs, weight, calc_adj,
@@ -635,15 +643,15 @@ extern "C" int sa_plan_autotune(sa_plan* P, const double* svel, const double* m1
         }
         SA_CUDA(cudaEventSynchronize(P->tk1));
         SA_CUDA(cudaEventElapsedTime(&ms, P->tk0, P->tk1));
-        if (ms_out) ms_out[c] = ms;
+        if (ms_out && c < SA_TUNE_MAX_CANDIDATES) ms_out[c] = ms;
         if (c == 0 || ms < best) {
             best = ms;
             best_c = c;
         }
     }
     P->timing = had_timing;
-    P->variant = best_c % nvar;
-    P->active = slots[best_c / nvar];
+    P->variant = cand[best_c].first;
+    P->active = cand[best_c].second;
     P->have_graph = false;
     ctx->tune[{P->nx, P->ny, P->prec}] = {P->variant, P->active};
     if (n_out) *n_out = ncand;

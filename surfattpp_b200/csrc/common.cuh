@@ -19,6 +19,7 @@ enum Status : int {
     ST_OK = 0,
     ST_NOCONV = 3,        // sweep iteration cap reached (reference only warns)
     ST_NONFINITE = 5,     // NaN/Inf in a travel-time or adjoint field
+    ST_TEAM = 7,          // a cooperative sweep's wait gave up (FP32 tail teams)
 };
 
 // Surface grid (device pointers).  Trigonometric row tables are produced on
@@ -102,7 +103,8 @@ enum Mode : int { MODE_FWD = 0, MODE_FWD_ADJ = 1, MODE_ADJ_ONLY = 2 };
 // Per-warp scratch slot.  Planes of nx*ny elements of type T (sweep fields)
 // plus FP64 planes where the reference's arithmetic must stay FP64.
 struct Scratch {
-    int nslots;
+    int nslots;            // event slots in use
+    int nwarps;            // FP32 kernel with tail teams: warps launched (all slots)
     size_t slot_bytes;
     unsigned char* base;
     unsigned int* queue;   // work-queue counter (reset to 0 before each launch)

@@ -2,6 +2,7 @@
 // kernel.  Sweeps run in FP32 (fast division and square root); T0 and T,
 // residuals, adjoint coefficients, convergence sums and the kernel
 // accumulation stay FP64 (see batch.cuh).
+#include <algorithm>
 #include <vector>
 
 #include "batch.cuh"
@@ -50,11 +51,18 @@ void launch_variant(const BatchDesc& d, const BatchArgs<float>& B, int blocks, c
 
 cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st) {
     const BatchArgs<float> B = make_batch_args<float>(d);
-    const int blocks = (d.sc.nslots + 3) / 4;
+    // with tail teams every resident warp runs (the slots in use are spread
+    // over the blocks, the other warps start as helpers)
+    const int blocks =
+        (((d.variant & 4) ? std::max(d.sc.nwarps, d.sc.nslots) : d.sc.nslots) + 3) / 4;
     switch (d.variant) {
         case 1: launch_variant<1>(d, B, blocks, st); break;
         case 2: launch_variant<2>(d, B, blocks, st); break;
         case 3: launch_variant<3>(d, B, blocks, st); break;
+        case 4: launch_variant<4>(d, B, blocks, st); break;
+        case 5: launch_variant<5>(d, B, blocks, st); break;
+        case 6: launch_variant<6>(d, B, blocks, st); break;
+        case 7: launch_variant<7>(d, B, blocks, st); break;
         default: launch_variant<0>(d, B, blocks, st); break;
     }
     return cudaGetLastError();
@@ -63,7 +71,7 @@ cudaError_t launch_batch32(const BatchDesc& d, cudaStream_t st) {
 // One launch over several plans' events (batch_multi_kernel): the levels'
 // arguments are copied to `dev_args` (nlev BatchArgs<float>), `code` lists
 // level << 24 | event in queue order.  One variant and one metric kind (iso
-// or general) for all levels.
+// or general) for all levels; no tail teams (variant bit 2 is ignored).
 namespace {
 template <int VAR>
 void launch_multi_variant(bool iso, const BatchArgs<float>* args, unsigned ntotal,
@@ -83,7 +91,7 @@ cudaError_t launch_batch32_multi(const BatchDesc* d, int nlev, void* dev_args, u
     const auto* args = static_cast<const BatchArgs<float>*>(dev_args);
     const int blocks = (sc.nslots + 3) / 4;
     const bool iso = d[0].iso != 0;
-    switch (d[0].variant) {
+    switch (d[0].variant & 3) {
         case 1: launch_multi_variant<1>(iso, args, ntotal, code, sc, blocks, st); break;
         case 2: launch_multi_variant<2>(iso, args, ntotal, code, sc, blocks, st); break;
         case 3: launch_multi_variant<3>(iso, args, ntotal, code, sc, blocks, st); break;

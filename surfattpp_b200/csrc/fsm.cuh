@@ -159,6 +159,8 @@ struct FwdBase {
     // to pay for them: the FP64 update (IEEE division and sqrt); the FP32
     // march updates every cell of its range (10 % faster on C3)
     static constexpr bool kFlags = sizeof(S) == sizeof(double);
+    // the FP32 sweeps can run as a team (systolic.cuh)
+    static constexpr bool kCoop = sizeof(S) == sizeof(float);
     struct Cell {
         S v;    // field before this update
         S x;    // T0 of the cell
@@ -265,12 +267,27 @@ struct FwdPolicy64 : FwdBase<double, ISO> {
     }
 };
 
-// FP32 division in the FP32 forward update: the hardware approximate
-// reciprocal (2 ulp over the operand range used here: |denominator| in
-// [1e-30, 2^126]).
-#ifndef SA_FDIV
-#define SA_FDIV(a, b) __fdividef((a), (b))
-#endif
+// FP32 arithmetic of the sweeps, spelled out: every product, sum and fused
+// multiply-add is an explicit round-to-nearest operation, so no compiled copy
+// of the sweep (the batch kernel's variants, a tail team's out-of-line copy)
+// contracts differently from another, and all round identically.
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ff(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// approximate reciprocal (hardware, 1 ulp; flushes subnormals): divisions
+// of the FP32 forward update are a * rcp(b), |b| in [1e-30, 2^126]
+__device__ __forceinline__ float frcp(float b) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+    return r;
+}
+__device__ __forceinline__ float fdiv(float a, float b) { return __fmul_rn(a, frcp(b)); }
+__device__ __forceinline__ float fsqrt(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // FP32 forward update in increment form.  The stored field is u = tau - 1
 // (tau ~ 1 everywhere, so u keeps ~20x more absolute resolution than tau),
@@ -295,10 +312,11 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
                                                   const Nb<float, float>& xp,
                                                   const Nb<float, float>& ym,
                                                   const Nb<float, float>& yp) {
-    const float det = ISO ? aij * bij : aij * bij - cij * cij;
-    const float k = t0 * idx;
-    const float m = t0 * idy;
-    const float f2 = fij * fij;
+    const float det = ISO ? fm(aij, bij) : ff(aij, bij, -fm(cij, cij));
+    const float k = fm(t0, idx);
+    const float m = fm(t0, idy);
+    const float f2 = fm(fij, fij);
+    const float c2 = fm(2.f, cij);
     float best = u;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -307,57 +325,58 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
         const Nb<float, float>& nxn = (sx < 0) ? xm : xp;
         const Nb<float, float>& nyn = (sy < 0) ? ym : yp;
         const float ux = nxn.v, uy = nyn.v;
-        const float A0 = fmaf(t0x, ux, t0x);
-        const float A1 = t0x - sx * k;
-        const float B0 = fmaf(t0y, ux, t0y) - sy * m * (ux - uy);
-        const float B1 = t0y - sy * m;
+        const float A0 = ff(t0x, ux, t0x);
+        const float A1 = sx < 0 ? fa(t0x, k) : fs(t0x, k);
+        const float B0 = ff(sy < 0 ? m : -m, fs(ux, uy), ff(t0y, ux, t0y));
+        const float B1 = sy < 0 ? fa(t0y, m) : fs(t0y, m);
+        const float aA0 = fm(aij, A0), bB0 = fm(bij, B0);
         float al, be, ga;
         if (ISO) {
-            al = aij * A1 * A1 + bij * B1 * B1;
-            be = 2.f * (aij * A0 * A1 + bij * B0 * B1);
-            ga = aij * A0 * A0 + bij * B0 * B0 - f2;
+            al = ff(fm(aij, A1), A1, fm(fm(bij, B1), B1));
+            be = fm(2.f, ff(aA0, A1, fm(bB0, B1)));
+            ga = ff(aA0, A0, ff(bB0, B0, -f2));
         } else {
-            al = aij * A1 * A1 + bij * B1 * B1 - 2.f * cij * A1 * B1;
-            be = 2.f * (aij * A0 * A1 + bij * B0 * B1 - cij * (A0 * B1 + A1 * B0));
-            ga = aij * A0 * A0 + bij * B0 * B0 - 2.f * cij * A0 * B0 - f2;
+            al = ff(fm(aij, A1), A1, ff(fm(bij, B1), B1, -fm(fm(c2, A1), B1)));
+            be = fm(2.f, ff(aA0, A1, ff(bB0, B1, -fm(cij, ff(A0, B1, fm(A1, B0))))));
+            ga = ff(aA0, A0, ff(bB0, B0, ff(-fm(c2, A0), B0, -f2)));
         }
-        const float disc = be * be - 4.f * al * ga;
+        const float disc = ff(be, be, -fm(fm(4.f, al), ga));
         const bool ok = nxn.has && nyn.has && disc >= 0.f && fabsf(al) >= 1e-30f;
-        const float sq = sqrtf(fmaxf(disc, 0.f));
-        const float qq = -0.5f * (be + copysignf(sq, be));
+        const float sq = fsqrt(fmaxf(disc, 0.f));
+        const float qq = fm(-0.5f, fa(be, copysignf(sq, be)));
         // the second root as ga / qq also when qq == 0: then it is +-inf or
         // NaN and fails the tests below, and the first root is the only one
         float Dr[2];
-        Dr[0] = SA_FDIV(qq, al);
-        Dr[1] = SA_FDIV(ga, qq);
+        Dr[0] = fdiv(qq, al);
+        Dr[1] = fdiv(ga, qq);
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const float D = Dr[r];
-            const float Tx = fmaf(A1, D, A0);
-            const float Ty = fmaf(B1, D, B0);
-            const float char_x = ISO ? Tx : aij * Tx - cij * Ty;
-            const float char_y = ISO ? Ty : bij * Ty - cij * Tx;
+            const float Tx = ff(A1, D, A0);
+            const float Ty = ff(B1, D, B0);
+            const float char_x = ISO ? Tx : ff(aij, Tx, -fm(cij, Ty));
+            const float char_y = ISO ? Ty : ff(bij, Ty, -fm(cij, Tx));
             // both characteristic components point away from the neighbours
             // (a NaN root makes both NaN and fails)
             const bool take = ok && fminf(-sx * char_x, -sy * char_y) >= 0.f;
-            best = take ? fminf(best, ux + D) : best;
+            best = take ? fminf(best, fa(ux, D)) : best;
         }
     }
     const bool okd = det > 0.f;
-    const float disx = sqrtf(fmaxf(SA_FDIV(f2 * bij, det), 0.f));
-    const float disy = sqrtf(fmaxf(SA_FDIV(f2 * aij, det), 0.f));
+    const float disx = fsqrt(fmaxf(fdiv(fm(f2, bij), det), 0.f));
+    const float disy = fsqrt(fmaxf(fdiv(fm(f2, aij), det), 0.f));
     auto one_point = [&](const Nb<float, float>& n, float g, float kk, int s, float dis) {
         // (T0 tau)_axis = g*tau - s*kk*(tau - tau_n) = +-dis
-        const float g1 = fmaf(g, n.v, g);
-        const float rden = SA_FDIV(1.f, g - s * kk);
+        const float g1 = ff(g, n.v, g);
+        const float rden = frcp(s < 0 ? fa(g, kk) : fs(g, kk));
         const bool ok = okd && n.has;
         // (1+c)*t0 >= (1+u_n)*T0_n  and  1+c > 0.5*(1+u_n)
-        const float kn = t0 - fmaf(n.v, n.x, n.x);
-        const float half = fmaf(0.5f, n.v, -0.5f);
+        const float kn = fs(t0, ff(n.v, n.x, n.x));
+        const float half = ff(0.5f, n.v, -0.5f);
 #pragma unroll
         for (int sgn = 0; sgn < 2; sgn++) {
-            const float c = n.v + ((sgn == 0 ? dis : -dis) - g1) * rden;
-            const bool take = ok && fmaf(c, t0, kn) >= 0.f && c > half;
+            const float c = ff(fs(sgn == 0 ? dis : -dis, g1), rden, n.v);
+            const bool take = ok && ff(c, t0, kn) >= 0.f && c > half;
             best = take ? fminf(best, c) : best;
         }
     };
@@ -389,8 +408,8 @@ struct FwdPolicyDelta32 : FwdBase<float, ISO, ROLLED> {
                                      ym, yp);
     }
     __device__ void account(const Cell& cur, float nv, double& l1, double& linf) const {
-        const double d = fabs((double)nv - (double)cur.vs) * (double)cur.x;
-        l1 += d;
+        const double d = __dmul_rn(fabs(__dsub_rn((double)nv, (double)cur.vs)), (double)cur.x);
+        l1 = __dadd_rn(l1, d);
         linf = fmax(linf, d);
     }
 };
@@ -405,6 +424,7 @@ struct AdjPolicyExact {
     static constexpr int kLead = 2;
     static constexpr bool kRolled = false;
     static constexpr bool kFlags = false;   // ranges from changes (systolic.cuh)
+    static constexpr bool kCoop = false;
     struct Cell {
         double v;
         float x;
@@ -492,6 +512,7 @@ struct AdjPolicyLinear64 {
     static constexpr int kLead = 2;
     static constexpr bool kRolled = false;
     static constexpr bool kFlags = false;
+    static constexpr bool kCoop = false;
     struct Cell {
         double v;
         float x;
@@ -566,6 +587,7 @@ struct AdjPolicyW32 {
     static constexpr int kLead = LEAD;
     static constexpr bool kRolled = false;
     static constexpr bool kFlags = false;   // ranges from changes (systolic.cuh)
+    static constexpr bool kCoop = true;
     struct Cell {
         float v;
         float x;
@@ -617,11 +639,11 @@ struct AdjPolicyW32 {
         const float txp = xp.has ? xp.v : 0.f;
         const float tym = ym.has ? ym.v : 0.f;
         const float typ = yp.has ? yp.v : 0.f;
-        return cur.c0 + cur.w.x * txm + cur.w.y * txp + cur.w.z * tym + cur.w.w * typ;
+        return ff(cur.w.w, typ, ff(cur.w.z, tym, ff(cur.w.y, txp, ff(cur.w.x, txm, cur.c0))));
     }
     __device__ void account(const Cell& cur, float nv, double& l1, double& linf) const {
-        const double dv = fabs((double)nv - (double)cur.vs);
-        l1 += dv;
+        const double dv = fabs(__dsub_rn((double)nv, (double)cur.vs));
+        l1 = __dadd_rn(l1, dv);
         linf = fmax(linf, dv);
     }
     __device__ void store(int k, float v, bool write_v, bool write_start) const {

@@ -48,7 +48,7 @@ struct BatchDesc {
 };
 
 // Number of FP32 batch-kernel launch variants (batch.cuh).
-constexpr int kBatchVariants = 4;
+constexpr int kBatchVariants = 8;
 
 size_t batch64_slot_bytes(int nx, int ny, int maxr);
 int batch64_max_slots(int device);

@@ -71,6 +71,83 @@ __device__ __forceinline__ bool same_bits<double>(double a, double b) {
     return __double_as_longlong(a) == __double_as_longlong(b);
 }
 
+// A team of warps of one block marching one solve (cooperative sweeps).
+// Strip j of a sweep (in sweep order) is marched by member j % W, each strip
+// a fixed lag behind the one before it: a strip's first lane streams the row
+// above from memory, so at its step t it needs the previous strip's last row
+// finished up to column t + 1 + lead.  Every member publishes, in its word,
+// the strip it marches and the last column its last row has finished (or
+// that the strip is done: its stores, its range updates and its strip
+// record are then visible); a member waits on the word of the strip before
+// its own.  A strip is finished only after the strip before it, so the last
+// strip of a sweep being done means the whole sweep is.  Cells are updated
+// exactly as by one warp (the same neighbour values reach every update); a
+// member that cannot yet know where the previous strip's last row changed
+// starts its march at the previous strip's first column, and marching more
+// cells than needed changes nothing (an update whose inputs did not change
+// reproduces the cell).  Every wait is bounded: when it gives up, the team's
+// error flag is set and the march goes on without it.
+struct Team {
+    int W;                       // members (1: the warp alone)
+    int r;                       // this warp's role
+    unsigned long long* word;    // [W] (shared): strip id << 32 | (column + 1)
+    int4* sinfo;                 // per solve [strips]: {first, lf, ll, -} of strip j
+    double* sums;                // per solve [strips][32]: last-sweep L1 partials
+    int* err;                    // set when a wait gave up
+};
+constexpr int kStripDone = 0x7ffffff0;          // column value: strip finished
+constexpr unsigned kTeamEnd = 0xffffffffu;       // strip id: member finished its sweeps
+constexpr long long kTeamWaitNs = 2000000000ll;  // a wait gives up after 2 s
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.cta.shared.u64 %0, [%1];"
+                 : "=l"(v)
+                 : "r"((unsigned)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.cta.shared.u64 [%0], %1;"
+                 :
+                 : "r"((unsigned)__cvta_generic_to_shared(p)), "l"(v)
+                 : "memory");
+}
+__device__ __forceinline__ long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (long long)t;
+}
+__device__ __forceinline__ unsigned long long team_word(unsigned id, int col) {
+    return ((unsigned long long)id << 32) | (unsigned)(col + 1);
+}
+
+// Waits (all lanes) until strip `id`, marched by member `role`, has its last
+// row finished up to column c or is done; returns the column reached
+// (kStripDone when the strip is finished, or when the wait gave up).
+__device__ __forceinline__ int team_wait(const Team& T, int role, unsigned id, int c) {
+    long long t0 = 0;
+    for (int spin = 0;; spin++) {
+        // after a wait of the block gave up, none waits any more
+        if (__shfl_sync(FULL_MASK, *(volatile int*)T.err, 0) != 0) return kStripDone;
+        // every lane acquires; lane 0's value decides, so the warp stays converged
+        const unsigned long long w =
+            __shfl_sync(FULL_MASK, ld_acquire_u64(T.word + role), 0);
+        const unsigned wid = (unsigned)(w >> 32);
+        const int col = (int)(unsigned)(w & 0xffffffffu) - 1;
+        if (wid > id) return kStripDone;   // the member moved on: strip done
+        if (wid == id && col >= c) return col;
+        const long long now = __shfl_sync(FULL_MASK, global_ns(), 0);
+        if (spin == 0) {
+            t0 = now;
+        } else if (now - t0 > kTeamWaitNs) {
+            if ((threadIdx.x & 31) == 0) atomicExch(T.err, 1);
+            return kStripDone;
+        }
+        if (spin >= 16) __nanosleep(32);
+    }
+}
+
 // Per-lane state of one strip's march.
 template <class V, class X>
 struct March {
@@ -210,9 +287,14 @@ __device__ __forceinline__ void systolic_step(P& p, March<V, X>& L, const int t,
 //
 // P::kLead = how many steps ahead a lane loads its row (1 for the long
 // forward update, more for the short adjoint update).
+//
+// P::kCoop policies (the FP32 sweeps) accumulate the last sweep's L1 sum per
+// strip and add the strip sums in strip order, so that a team (`tm`, `sweep`
+// = 0..3 within the iteration) and a warp alone round it identically.
 template <class P>
 __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd, const bool last,
-                                               double& l1, double& linf) {
+                                               double& l1, double& linf,
+                                               const Team* tm = nullptr, const int sweep = 0) {
     using V = typename P::V;
     using X = typename P::X;
     using Cell = typename P::Cell;
@@ -222,18 +304,42 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
     const int NR = p.nrows();
     const int NC = p.ncols();
     const int S = p.stride();
+    const int nstrip = (NR + 31) >> 5;
+    const bool coop = P::kCoop && tm != nullptr && tm->W > 1;
+    const int W = coop ? tm->W : 1;
+    const int me = coop ? tm->r : 0;
+    const unsigned id0 = 1u + (unsigned)sweep * (unsigned)nstrip;   // strip id of strip 0
+    if (coop && me == 0) {
+        // strip 0 follows the previous sweep's last strip; once that one is
+        // done the whole sweep is, and next sweep's ranges can be cleared
+        if (sweep > 0 && (nstrip - 1) % W != 0) team_wait(*tm, (nstrip - 1) % W, id0 - 1, kStripDone);
+        if constexpr (!P::kFlags)
+            for (int iy = lane; iy < p.ny; iy += 32) p.rng2[iy] = make_int2(0x7fffffff, -1);
+        __threadfence();
+        __syncwarp();
+    }
     int uf = NC, ul = -1;   // changes of the row above the current strip
-    for (int k0 = 0; k0 < NR; k0 += 32) {
+    for (int j = me; j < nstrip; j += W) {
+        const int k0 = j * 32;
+        const unsigned id = id0 + (unsigned)j;
         const int rp = k0 + lane;
         const bool act = rp < NR;
         const int nr_strip = min(32, NR - k0);
         const int iy = act ? p.row(rp, yd) : 0;
+        // team: nothing of the strip is read before the strip ahead of it
+        // has started -- then the previous sweep, whose strips wrote this
+        // strip's ranges and rows in the reversed order, is complete
+        const int prole = (coop && j > 0) ? (j - 1) % W : -1;
+        int avail = kStripDone;
+        if (prole >= 0) avail = team_wait(*tm, prole, id - 1, -1);
         // columns (sweep order) this strip's march must cover
         int fc = NC, lc = -1;
         if (act) {
-            int2 r = p.rng[iy];
+            // (a team merges the ranges with atomics, performed in L2: read
+            // them from there, not from a line this SM's L1 may hold)
+            int2 r = coop ? __ldcg(p.rng + iy) : p.rng[iy];
             if (last) {
-                const int2 q = p.crng[iy];
+                const int2 q = coop ? __ldcg(p.crng + iy) : p.crng[iy];
                 r.x = min(r.x, q.x);
                 r.y = max(r.y, q.y);
             }
@@ -243,13 +349,68 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
                 lc = max(a, b);
             }
         }
-        const int first = min(__reduce_min_sync(FULL_MASK, fc), uf);
-        const int lastd = max(__reduce_max_sync(FULL_MASK, lc), ul);
+        const int fcm = __reduce_min_sync(FULL_MASK, fc);
+        const int lcm = __reduce_max_sync(FULL_MASK, lc);
+        // team: the strip before this one (its member, and how far its last
+        // row is).  uf / ul are final once it is done; before that, once its
+        // last row has passed column fcm - 1, the first column where that row
+        // changed (kept current in its record) decides min(fcm, uf) exactly,
+        // and ul stays unknown (no early stop until it is done)
+        bool known = true;
+        if (prole >= 0) {
+            const int want = fcm < NC ? fcm - 1 : kStripDone;
+            if (avail < want) avail = team_wait(*tm, prole, id - 1, want);
+            const int4 q = tm->sinfo[j - 1];
+            uf = q.y;
+            ul = q.z;
+            if (avail != kStripDone) {
+                known = false;
+                ul = -1;
+            }
+        }
+        const int first = min(fcm, uf);
+        int lastd = max(lcm, ul);
         if (first >= NC) {   // no cell of the strip can change
+            if (coop) {
+                // (one lane, the strip's last, writes its record and word)
+                if (last) tm->sums[j * 32 + lane] = 0.0;
+                __threadfence();
+                __syncwarp();
+                if (lane == nr_strip - 1) {
+                    tm->sinfo[j] = make_int4(NC, NC, -1, 0);
+                    st_release_u64(tm->word + me, team_word(id, kStripDone));
+                }
+            }
             uf = NC;
             ul = -1;
             continue;
         }
+        // Progress is the last column the strip's last lane has visited (not
+        // merely one its row cannot change at): up to there that lane has also
+        // read the next strip's first row, which the next strip may then
+        // overwrite.
+        if (coop) {
+            if (lane == nr_strip - 1) {
+                tm->sinfo[j] = make_int4(first, NC, -1, 0);
+                st_release_u64(tm->word + me, team_word(id, -1));
+            }
+        }
+        // the next column the first lane streams from the row above must be
+        // finished by the strip before (coop only); kStripDone: wait until
+        // that strip is done
+        auto need = [&](int c) {
+            if (known || c <= avail) return;
+            if (c < kStripDone) {
+                if (avail >= NC - 1) return;
+                c = min(c, NC - 1);
+            }
+            avail = team_wait(*tm, prole, id - 1, c);
+            if (avail == kStripDone) {
+                known = true;
+                ul = tm->sinfo[j - 1].z;
+                lastd = max(lastd, ul);
+            }
+        };
         March<V, X> L;
         L.lane = lane;
         L.NC = NC;
@@ -282,6 +443,9 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         L.prev_v = V(0);
         L.prev_x = X(0);
         p.begin_row(iy, act);
+        // the last sweep's L1 sum of this strip (kCoop) or the running sum
+        double l1s = 0.0;
+        double& l1r = P::kCoop ? l1s : l1;
         // this lane's first column and the cell before it
         const int c0 = first - lane;
         if (act && c0 >= 1) {
@@ -290,6 +454,7 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
             L.prev_x = q.x;
             L.pfl = q.fl;
         }
+        need(first + LEAD);
         Cell buf[NB], eb[NB];
         // columns c0 .. c0+LEAD (what earlier steps would have loaded)
 #pragma unroll
@@ -306,35 +471,48 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         // one step more than the march: the last cell's flags are written
         // one step after its visit
         const int nsteps = NC + nr_strip;
+        const bool pub = coop && lane == nr_strip - 1;   // publishes the last row's progress
         if constexpr (P::kRolled && LEAD == 1) {
             // one copy of the step (long updates: instruction-cache footprint
             // over register moves); the load of this step lands in `ld` and
             // moves down the buffer at the end of the step
             Cell cur = buf[0], nx1 = buf[1], ecur = eb[0], enx1 = eb[1];
             for (int t = first; t < nsteps; t++) {
+                if (coop) need(t + 1 + LEAD);
                 Cell ld = cur, eld = ecur;
-                systolic_step<LEAD>(p, L, t, cur, nx1, ld, ecur, eld, l1, linf);
+                systolic_step<LEAD>(p, L, t, cur, nx1, ld, ecur, eld, l1r, linf);
                 cur = nx1;
                 nx1 = ld;
                 ecur = enx1;
                 enx1 = eld;
-                if (t - 31 > lastd && L.bal == 0u) break;
+                if (pub && (t & 7) == 7) {
+                    tm->sinfo[j].y = L.lf;
+                    st_release_u64(tm->word + me, team_word(id, min(max(t - lane, -1), NC - 1)));
+                }
+                if (known && t - 31 > lastd && L.bal == 0u) break;
             }
         } else {
             for (int t = first; t < nsteps; t += NB) {
+                if (coop) need(t + NB + LEAD);
 #pragma unroll
                 for (int i = 0; i < NB; i++) {
                     if (t + i < nsteps)
                         systolic_step<LEAD>(p, L, t + i, buf[i % NB], buf[(i + 1) % NB],
                                             buf[(i + 1 + LEAD) % NB], eb[i % NB],
-                                            eb[(i + 1 + LEAD) % NB], l1, linf);
+                                            eb[(i + 1 + LEAD) % NB], l1r, linf);
                 }
-                if (t + NB - 1 - 31 > lastd && L.bal == 0u) break;
+                if (pub) {
+                    tm->sinfo[j].y = L.lf;
+                    st_release_u64(tm->word + me,
+                                   team_word(id, min(max(t + NB - 1 - lane, -1), NC - 1)));
+                }
+                if (known && t + NB - 1 - 31 > lastd && L.bal == 0u) break;
             }
         }
         if constexpr (!P::kFlags) {
             // next sweep's ranges: this row's changes widened by a column, in
-            // this row and the rows above and below
+            // this row and the rows above and below (a team's neighbouring
+            // strips merge into the same rows: atomics)
             const bool any = L.cmin <= L.cmax;
             const int lo = any ? max(L.cmin - 1, p.col(0, 1)) : 0x7fffffff;
             const int hi = any ? min(L.cmax + 1, p.col(NC - 1, 1)) : -1;
@@ -351,21 +529,22 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
                 nlo = min(nlo, blo);
                 nhi = max(nhi, bhi);
             }
-            if (act && nlo <= nhi) {
-                int2 r = p.rng2[iy];
-                r.x = min(r.x, nlo);
-                r.y = max(r.y, nhi);
-                p.rng2[iy] = r;
-            }
+            auto merge = [&](int row, int a, int b) {
+                if (coop) {
+                    int* q = reinterpret_cast<int*>(p.rng2 + row);
+                    atomicMin(q, a);
+                    atomicMax(q + 1, b);
+                } else {
+                    int2 r = p.rng2[row];
+                    r.x = min(r.x, a);
+                    r.y = max(r.y, b);
+                    p.rng2[row] = r;
+                }
+            };
+            if (act && nlo <= nhi) merge(iy, nlo, nhi);
             __syncwarp();
             // the rows outside the strip
-            if (any && (L.eup || L.edn)) {
-                const int iy_o = L.eup ? iy_up : p.row(rp + 1, yd);
-                int2 r = p.rng2[iy_o];
-                r.x = min(r.x, lo);
-                r.y = max(r.y, hi);
-                p.rng2[iy_o] = r;
-            }
+            if (any && (L.eup || L.edn)) merge(L.eup ? iy_up : p.row(rp + 1, yd), lo, hi);
         }
         // every cell of the row that had bit 0 set was visited: the range is
         // replaced; lane 0 then adds where it set bit 0 in the row above.
@@ -376,7 +555,7 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
             if (last) {
                 p.crng[iy] = make_int2(0x7fffffff, -1);
             } else if (L.cmin <= L.cmax) {
-                int2 q = p.crng[iy];
+                int2 q = coop ? __ldcg(p.crng + iy) : p.crng[iy];
                 q.x = min(q.x, L.cmin);
                 q.y = max(q.y, L.cmax);
                 p.crng[iy] = q;
@@ -389,6 +568,22 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
             r.y = max(r.y, L.umax);
             p.rng[iy_up] = r;
         }
+        if constexpr (P::kCoop) {
+            if (!coop) l1 += l1s;
+            else if (last) tm->sums[j * 32 + lane] = l1s;
+        }
+        if (coop) {
+            // finished after the strip before it (then ul is final), with its
+            // stores, range updates and record visible
+            need(kStripDone);
+            __threadfence();
+            __syncwarp();
+            if (lane == nr_strip - 1) {
+                tm->sinfo[j].y = L.lf;
+                tm->sinfo[j].z = L.ll;
+                st_release_u64(tm->word + me, team_word(id, kStripDone));
+            }
+        }
         uf = L.lf;
         ul = L.ll;
         __syncwarp();
@@ -397,8 +592,11 @@ __device__ __forceinline__ void systolic_sweep(P& p, const int xd, const int yd,
         int2* nxt = p.rng2;
         p.rng2 = p.rng;
         p.rng = nxt;
-        for (int iy = lane; iy < p.ny; iy += 32) p.rng2[iy] = make_int2(0x7fffffff, -1);
-        __syncwarp();
+        // (a team clears them at the next sweep's start, after this sweep)
+        if (!coop) {
+            for (int iy = lane; iy < p.ny; iy += 32) p.rng2[iy] = make_int2(0x7fffffff, -1);
+            __syncwarp();
+        }
     }
 }
 

@@ -90,7 +90,7 @@ class ForwardAdjointPlan:
         workload (sa_plan_autotune); kept for this plan and later plans of the
         same grid size on its context.  Returns dict(ms=[per candidate],
         choice=index, variant, active_slots, nslots)."""
-        ms = (C.c_float * 8)()
+        ms = (C.c_float * 32)()
         n, ch = C.c_int(0), C.c_int(0)
         rc = _capi.lib().sa_plan_autotune(self.h, ptr(svel), ptr(m11), ptr(m12), ptr(m22),
                                           ptr(tt_obs), ptr(weight), int(bool(calc_adj)),

@@ -4,10 +4,11 @@ Bars (written here):
   * FP64 plans (one kernel, all or part of the slots): synthetic times and
     iteration counts bit for bit, misfit to 1e-12 relative, adj_s to 1e-12 of
     its maximum (FP64 atomics accumulate in completion order).
-  * FP32 variants run the same arithmetic, but the compiler may fuse
-    multiply-adds differently in each variant's code, so results move by FP32
-    rounding: synthetic times within 1e-4 s, misfit 1e-4 relative, adj_s
-    1e-4 relative L2 (the FP32 path's bars against the FP64 oracle).
+  * FP32 variants (forward step rolled or unrolled, adjoint lead 2 or 3,
+    tail teams on or off) run the same explicit operations -- every product,
+    sum and fused multiply-add of the sweeps is spelled out -- so synthetic
+    times and iteration counts are bit for bit the same, the misfit to 1e-12
+    relative and adj_s to 1e-12 of its maximum (FP64 atomics).
 The autotuner times every candidate on the plan's own workload, keeps the
 fastest and hands it to later plans of the same grid size.
 """
@@ -47,24 +48,18 @@ def test_every_configuration_gives_the_same_results(gpu, precision):
     plan = mk()
     ref = _run(plan, sv, tt, wt)
     nslots = plan.tune()["nslots"]
-    nvar = 4 if precision == "fp32" else 1
+    nvar = 8 if precision == "fp32" else 1
     for v in range(nvar):
         for active in (0, max(1, nslots // 3)):
             plan.set_tune(v, active)
             got = _run(plan, sv, tt, wt)
             assert plan.tune()["variant"] == v
-            if precision == "fp64":
-                assert np.array_equal(got["syn"], ref["syn"]), (v, active)
-                assert np.array_equal(got["fwd_iters"], ref["fwd_iters"])
-                assert np.array_equal(got["adj_iters"], ref["adj_iters"])
-                assert abs(got["chi"][0] - ref["chi"][0]) <= 1e-12 * abs(ref["chi"][0])
-                scale = np.abs(ref["adj_s"]).max()
-                assert np.abs(got["adj_s"] - ref["adj_s"]).max() <= 1e-12 * scale
-            else:
-                assert np.abs(got["syn"] - ref["syn"]).max() <= 1e-4, (v, active)
-                assert abs(got["chi"][0] - ref["chi"][0]) <= 1e-4 * abs(ref["chi"][0])
-                l2 = np.linalg.norm(got["adj_s"] - ref["adj_s"]) / np.linalg.norm(ref["adj_s"])
-                assert l2 <= 1e-4, (v, active, l2)
+            assert np.array_equal(got["syn"], ref["syn"]), (v, active)
+            assert np.array_equal(got["fwd_iters"], ref["fwd_iters"]), (v, active)
+            assert np.array_equal(got["adj_iters"], ref["adj_iters"]), (v, active)
+            assert abs(got["chi"][0] - ref["chi"][0]) <= 1e-12 * abs(ref["chi"][0])
+            scale = np.abs(ref["adj_s"]).max()
+            assert np.abs(got["adj_s"] - ref["adj_s"]).max() <= 1e-12 * scale
     with pytest.raises(RuntimeError):
         plan.set_tune(nvar, 0)
 
@@ -76,11 +71,11 @@ def test_autotune_picks_and_hands_on(gpu):
     ref = _run(plan, sv, tt, wt)
     adj = torch.empty_like(torch.as_tensor(ref["adj_s"], device=sv.device))
     res = plan.autotune(sv, tt, wt, adj_s=adj)
-    assert len(res["ms"]) == 8 and all(m > 0 for m in res["ms"])
+    # 8 variants x (all, 3/4 of the slots) + the 4 team variants x 1/4
+    assert len(res["ms"]) == 20 and all(m > 0 for m in res["ms"])
     assert res["choice"] == int(np.argmin(res["ms"]))
-    assert res["variant"] == res["choice"] % 4
     got = _run(plan, sv, tt, wt)
-    assert np.abs(got["syn"] - ref["syn"]).max() <= 1e-4
+    assert np.array_equal(got["syn"], ref["syn"])
     # a later plan of the same grid size starts from the tuned configuration
     plan2 = mk()
     assert plan2.tune()["variant"] == res["variant"]

@@ -4,8 +4,7 @@ metric from the fractal topography, a handful of sources per period) solved
 in one launch must give each plan's own results -- FP64: synthetic times
 and misfit bit for bit, adj_s to 1e-12 of its maximum (FP64 atomics in
 completion order); FP32: within the FP32 path's bars (1e-4 s, 1e-4 relative
-L2; the multi-grid kernel is compiled separately and may fuse multiply-adds
-differently) -- on the first evaluation and on the second, whose queue is
+L2) -- on the first evaluation and on the second, whose queue is
 ordered by the first one's work across the levels."""
 import numpy as np
 import pytest
