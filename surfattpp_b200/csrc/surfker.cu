@@ -53,7 +53,11 @@ surfdisp_columns_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
         t[i] = periods[i];
         cg[i] = 0.0;
     }
+#ifdef SK_DISP_SERIAL
     const int st = sk::surfdisp96(L, vp, vs, rho, iflsph, iwave, 1, igr, nper, t, cg);
+#else
+    const int st = sk::surfdisp96_lockstep(L, vp, vs, rho, iflsph, iwave, igr, nper, t, cg);
+#endif
     if (status) status[ix + nx * iy] = st;
     for (int ip = 0; ip < nper; ip++) svel[(size_t)ip * nx * ny + ix + (size_t)nx * iy] = cg[ip];
 }

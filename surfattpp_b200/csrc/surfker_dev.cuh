@@ -626,12 +626,11 @@ __device__ inline float gtsolh(float a, float b) {
     return c;
 }
 
-// surfdisp96.f:57-373 for one column.  vp/vs/rho: unflattened float model
-// (mmax layers).  Returns 0, or 1 when the fundamental-mode search fails.
-static __device__ int surfdisp96(const LayerConst& L, const float* vpm, const float* vsm,
-                          const float* rhom, int iflsph, int iwave, int mode, int igr, int kmax,
-                          const double* t, double* cg) {
-    SDModel M;
+// surfdisp96.f:57-373 up to the root searches: the (flattened) layer model,
+// the bracket step dc and the starting velocity cc of the first search.
+__device__ inline void sd_setup(const LayerConst& L, const float* vpm, const float* vsm,
+                                const float* rhom, int iflsph, int iwave, SDModel& M,
+                                float& betmx, double& cc, double& dc) {
     const int mmax = L.mmax;
     M.mmax = mmax;
     float vmin = vsm[0];
@@ -640,7 +639,6 @@ static __device__ int surfdisp96(const LayerConst& L, const float* vpm, const fl
     if (vmin < 1.0f) ddc0 = 0.001f;
     else if (vmin < 2.0f) ddc0 = 0.002f;
     else ddc0 = 0.005f;
-    const float h0 = 0.005f;
     M.llw = 1;
     if (vsm[0] <= 0.0f) M.llw = 2;
     for (int i = 0; i < mmax; i++) {
@@ -656,9 +654,9 @@ static __device__ int surfdisp96(const LayerConst& L, const float* vpm, const fl
         M.rho[i] = rhom[i];
     }
     M.del1st = 0.0;
-    const double one = 1.0e-2;
     int jmn = 1, jsol = 1;
-    float betmx = -1.e20f, betmn = 1.e20f;
+    float betmn = 1.e20f;
+    betmx = -1.e20f;
     for (int i = 0; i < mmax; i++) {
         if (M.b[i] > 0.01f && M.b[i] < betmn) {
             betmn = M.b[i];
@@ -675,18 +673,32 @@ static __device__ int surfdisp96(const LayerConst& L, const float* vpm, const fl
     if (iflsph == 1)   // sphere(ifunc,1): density mapping
         for (int i = 0; i < mmax; i++)
             M.rho[i] = rhom[i] * (ifunc == 1 ? L.sd_rhofac_love[i] : L.sd_rhofac[i]);
-    double c[KMAX], cb[KMAX];
     const float ddc = ddc0;
-    const float sone = 1.500f;
-    const float h = h0;
-    const double onea = (double)sone;
     float cc1;
     if (jsol == 0) cc1 = betmn;
     else cc1 = gtsolh(M.a[jmn - 1], M.b[jmn - 1]);
     cc1 = 0.95f * cc1;
     cc1 = 0.90f * cc1;
-    const double cc = (double)cc1;
-    const double dc = fabs((double)ddc);
+    cc = (double)cc1;
+    dc = fabs((double)ddc);
+}
+
+// surfdisp96.f:57-373 for one column, the searches in the reference's
+// order.  vp/vs/rho: unflattened float model (mmax layers).  Returns 0, or
+// 1 when the fundamental-mode search fails.
+static __device__ int surfdisp96(const LayerConst& L, const float* vpm, const float* vsm,
+                          const float* rhom, int iflsph, int iwave, int mode, int igr, int kmax,
+                          const double* t, double* cg) {
+    SDModel M;
+    float betmx;
+    double cc, dc;
+    sd_setup(L, vpm, vsm, rhom, iflsph, iwave, M, betmx, cc, dc);
+    const int ifunc = (iwave == 1) ? 1 : 2;
+    const double one = 1.0e-2;
+    const float sone = 1.500f;
+    const float h = 0.005f;
+    const double onea = (double)sone;
+    double c[KMAX], cb[KMAX];
     double c1 = cc;
     const double cm = cc;
     double clow = cc;
@@ -763,6 +775,290 @@ static __device__ int surfdisp96(const LayerConst& L, const float* vpm, const fl
         ift = kfail;
     }
     return 0;
+}
+
+// surfdisp96's fundamental-mode searches (getsol's bracket march, nevill's
+// refinement, the period loop and the group velocity's second search) as a
+// resumable state machine: advance() runs the control flow up to the next
+// secular-function evaluation, leaves the requested (wvno, omega) in the
+// state and returns true; the caller evaluates dltar there and passes the
+// value back at the next advance().  Each lane's sequence of evaluations,
+// and every operation on their values, are those of surfdisp96() above (the
+// same trial velocities, brackets and Neville tables), so the results are
+// bit-identical; what changes is that all lanes of a warp meet at one dltar
+// call site, whichever period, march step or refinement step each is in,
+// instead of running the march and the refinements of differently long
+// brackets one after another.  Only mode 1 (the fundamental mode, what every
+// caller here asks for).
+struct RootSearch {
+    enum : int { kStart = 0, kGsFirst, kGsMarch, kGsStep, kNvFirst, kNvTop, kNvTopEval,
+                 kNvMid, kNvEnd, kDone };
+    // per column
+    double cc, dc, cm;
+    float betmx;
+    int igr, kmax;
+    // progress
+    int ph, k, stage, status;
+    float t1a, t1b;
+    double cprev;                      // c(k-1) of the period before
+    double ck;                         // this period's phase velocity
+    // getsol
+    double t1, c1, clow, del1, c2;
+    int idir, guard, ifirst;
+    // nevill
+    double n1, n2, nd1, nd2, c3, del3, nomega;
+    int nev, nctrl, m;
+    double x[11], y[11];
+    // the requested evaluation
+    double wvno, omega;
+};
+
+// surfdisp96.f:57-373 period loop, one step (see RootSearch).
+__device__ inline bool root_advance(RootSearch& S, SDModel& M, double del, const double* t,
+                                    double* cg) {
+    const double twopi = 2.0 * 3.141592653589793;
+    const double one = 1.0e-2;
+    const double onea = (double)1.500f;
+    const float h = 0.005f;
+    for (;;) {
+        switch (S.ph) {
+            case RootSearch::kStart: {   // next period (surfdisp96.f:121-160)
+                S.k++;
+                if (S.k > S.kmax) {
+                    S.ph = RootSearch::kDone;
+                    S.status = 0;
+                    return false;
+                }
+                double t1 = t[S.k - 1];
+                S.t1b = 0.0f;
+                if (S.igr > 0) {
+                    S.t1a = (float)(t1 / (double)(1.0f + h));
+                    S.t1b = (float)(t1 / (double)(1.0f - h));
+                    t1 = (double)S.t1a;
+                } else {
+                    S.t1a = (float)t1;
+                }
+                if (S.k == 1) {
+                    S.c1 = S.cc;
+                    S.clow = S.cc;
+                    S.ifirst = 1;
+                } else {
+                    S.ifirst = 0;
+                    S.c1 = S.cprev - onea * S.dc;
+                    S.clow = S.cm;
+                }
+                S.t1 = t1;
+                S.stage = 0;
+                // getsol entry: del1 at c1 (surfdisp96.f:413-416)
+                S.omega = twopi / S.t1;
+                S.wvno = S.omega / S.c1;
+                S.ph = RootSearch::kGsFirst;
+                return true;
+            }
+            case RootSearch::kGsFirst: {
+                S.del1 = del;
+                if (S.ifirst == 1) M.del1st = S.del1;
+                const double plmn = dsign1(M.del1st) * dsign1(S.del1);
+                if (S.ifirst == 1) S.idir = +1;
+                else if (plmn >= 0.0) S.idir = +1;
+                else S.idir = -1;
+                S.guard = 0;
+                S.ph = RootSearch::kGsMarch;
+                break;
+            }
+            case RootSearch::kGsMarch: {   // next trial velocity (surfdisp96.f:431-446)
+                if (S.guard >= 100000) goto getsol_fail;
+                if (S.idir > 0) S.c2 = S.c1 + S.dc;
+                else S.c2 = S.c1 - S.dc;
+                if (S.c2 <= S.clow) {
+                    S.idir = +1;
+                    S.c1 = S.clow;
+                    S.guard++;
+                    break;
+                }
+                S.omega = twopi / S.t1;
+                S.wvno = S.omega / S.c2;
+                S.ph = RootSearch::kGsStep;
+                return true;
+            }
+            case RootSearch::kGsStep: {
+                const double del2 = del;
+                if (dsign1(S.del1) != dsign1(del2)) {
+                    // nevill entry (surfdisp96.f:578-590)
+                    S.n1 = S.c1;
+                    S.n2 = S.c2;
+                    S.nd1 = S.del1;
+                    S.nd2 = del2;
+                    S.nomega = twopi / S.t1;
+                    S.c3 = 0.5 * (S.n1 + S.n2);
+                    S.omega = S.nomega;
+                    S.wvno = S.nomega / S.c3;
+                    S.ph = RootSearch::kNvFirst;
+                    return true;
+                }
+                S.c1 = S.c2;
+                S.del1 = del2;
+                if (S.c1 < S.cm) goto getsol_fail;
+                if (S.c1 >= ((double)S.betmx + S.dc)) goto getsol_fail;
+                S.guard++;
+                S.ph = RootSearch::kGsMarch;
+                break;
+            }
+            case RootSearch::kNvFirst:
+                S.del3 = del;
+                S.nev = 1;
+                S.nctrl = 1;
+                S.m = 1;
+                S.ph = RootSearch::kNvTop;
+                break;
+            case RootSearch::kNvTop:   // surfdisp96.f:593-600
+                S.nctrl = S.nctrl + 1;
+                if (S.nctrl >= 100) goto nevill_done;
+                if (S.c3 < fmin(S.n1, S.n2) || S.c3 > fmax(S.n1, S.n2)) {
+                    S.nev = 0;
+                    S.c3 = 0.5 * (S.n1 + S.n2);
+                    S.omega = S.nomega;
+                    S.wvno = S.nomega / S.c3;
+                    S.ph = RootSearch::kNvTopEval;
+                    return true;
+                }
+                S.ph = RootSearch::kNvMid;
+                break;
+            case RootSearch::kNvTopEval:
+                S.del3 = del;
+                S.ph = RootSearch::kNvMid;
+                break;
+            case RootSearch::kNvMid: {   // surfdisp96.f:601-696
+                const double s13 = S.nd1 - S.del3;
+                const double s32 = S.del3 - S.nd2;
+                if (dsign1(S.del3) * dsign1(S.nd1) < 0.0) {
+                    S.n2 = S.c3;
+                    S.nd2 = S.del3;
+                } else {
+                    S.n1 = S.c3;
+                    S.nd1 = S.del3;
+                }
+                if (fabs(S.n1 - S.n2) <= 1.e-6 * S.n1) goto nevill_done;
+                if (dsign1(s13) != dsign1(s32)) S.nev = 0;
+                const double p01 = (double)0.01f;
+                const double ss1 = fabs(S.nd1);
+                const double s1 = p01 * ss1;
+                const double ss2 = fabs(S.nd2);
+                const double s2 = p01 * ss2;
+                bool halve = s1 > ss2 || s2 > ss1 || S.nev == 0;
+                if (!halve) {
+                    int m = S.m;
+                    if (S.nev == 2) {
+                        S.x[m] = S.c3;
+                        S.y[m] = S.del3;
+                    } else {
+                        S.x[0] = S.n1;
+                        S.y[0] = S.nd1;
+                        S.x[1] = S.n2;
+                        S.y[1] = S.nd2;
+                        m = 1;
+                    }
+                    bool bad = false;
+                    for (int kk = 1; kk <= m; kk++) {
+                        const int j = m - kk + 1;
+                        const double denom = S.y[m] - S.y[j - 1];
+                        if (fabs(denom) < 1.0e-10 * fabs(S.y[m])) {
+                            bad = true;
+                            break;
+                        }
+                        S.x[j - 1] = (-(S.y[j - 1] * S.x[j]) + S.y[m] * S.x[j - 1]) / denom;
+                    }
+                    if (!bad) {
+                        S.c3 = S.x[0];
+                        S.nev = 2;
+                        m = m + 1;
+                        if (m > 10) m = 10;
+                        S.m = m;
+                    } else {
+                        halve = true;
+                    }
+                }
+                if (halve) {
+                    S.c3 = 0.5 * (S.n1 + S.n2);
+                    S.nev = 1;
+                    S.m = 1;
+                }
+                S.omega = S.nomega;
+                S.wvno = S.nomega / S.c3;
+                S.ph = RootSearch::kNvEnd;
+                return true;
+            }
+            case RootSearch::kNvEnd:
+                S.del3 = del;
+                S.ph = RootSearch::kNvTop;
+                break;
+            default:
+                return false;
+        }
+        continue;
+    nevill_done:   // getsol after nevill (surfdisp96.f:455-459)
+        S.c1 = S.c3;
+        if (S.c1 > (double)S.betmx) goto getsol_fail;
+        // getsol found its root: c1
+        if (S.stage == 0) {
+            S.ck = S.c1;
+            if (S.igr > 0) {   // the group velocity's second search (surfdisp96.f:181-192)
+                S.stage = 1;
+                S.t1 = (double)S.t1b;
+                S.ifirst = 0;
+                S.clow = 0.0 + one * S.dc;   // cb(k) is still 0 in mode 1
+                S.c1 = S.c1 - onea * S.dc;
+                S.omega = twopi / S.t1;
+                S.wvno = S.omega / S.c1;
+                S.ph = RootSearch::kGsFirst;
+                return true;
+            }
+            cg[S.k - 1] = (float)S.ck;
+        } else {
+            const float cc0 = (float)S.ck;
+            const float ccg = (float)S.c1;
+            cg[S.k - 1] = (1.0f / S.t1a - 1.0f / S.t1b) / (1.0f / (S.t1a * cc0) - 1.0f / (S.t1b * ccg));
+        }
+        S.cprev = S.ck;
+        S.ph = RootSearch::kStart;
+        continue;
+    getsol_fail:
+        if (S.stage == 0) {   // the fundamental mode fails from this period on
+            for (int i = S.k; i <= S.kmax; i++) cg[i - 1] = 0.0;
+            S.ph = RootSearch::kDone;
+            S.status = 1;
+            return false;
+        }
+        {   // the second search failed: the group velocity uses c itself
+            const float cc0 = (float)S.ck;
+            const float ccg = (float)S.ck;
+            cg[S.k - 1] = (1.0f / S.t1a - 1.0f / S.t1b) / (1.0f / (S.t1a * cc0) - 1.0f / (S.t1b * ccg));
+        }
+        S.cprev = S.ck;
+        S.ph = RootSearch::kStart;
+    }
+}
+
+// surfdisp96() with the searches of all lanes meeting at one dltar call
+// (see RootSearch); same arguments and results, mode 1.
+static __device__ int surfdisp96_lockstep(const LayerConst& L, const float* vpm, const float* vsm,
+                                          const float* rhom, int iflsph, int iwave, int igr,
+                                          int kmax, const double* t, double* cg) {
+    SDModel M;
+    RootSearch S;
+    sd_setup(L, vpm, vsm, rhom, iflsph, iwave, M, S.betmx, S.cc, S.dc);
+    const int ifunc = (iwave == 1) ? 1 : 2;
+    S.cm = S.cc;
+    S.igr = igr;
+    S.kmax = kmax;
+    S.ph = RootSearch::kStart;
+    S.k = 0;
+    S.status = 0;
+    S.cprev = 0.0;
+    S.ck = 0.0;
+    double del = 0.0;
+    while (root_advance(S, M, del, t, cg)) del = dltar(M, S.wvno, S.omega, ifunc);
+    return S.status;
 }
 
 // ---------------------------------------------------------------------------
