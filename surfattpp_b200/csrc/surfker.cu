@@ -95,8 +95,12 @@ depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int 
                    double* sen_rho, double* sen_hs) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= (long long)nx * ny * nper) return;
-    const int ip = (int)(gid % nper);
-    const int col = (int)(gid / nper);
+    // period-major: a warp takes 32 neighbouring columns at one period, whose
+    // phase velocities stand alike against the layer velocities, so its lanes
+    // take the same evanescent / oscillatory branches layer by layer
+    const long long ncol = (long long)nx * ny;
+    const int ip = (int)(gid / ncol);
+    const int col = (int)(gid % ncol);
     const int ix = col / ny, iy = col % ny;
     const LayerConst& L = *Lp;
     float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];
@@ -172,8 +176,12 @@ depthkernel_love_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
                         const LayerConst* __restrict__ Lp, double* sen_vs, double* sen_rho) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= (long long)nx * ny * nper) return;
-    const int ip = (int)(gid % nper);
-    const int col = (int)(gid / nper);
+    // period-major: a warp takes 32 neighbouring columns at one period, whose
+    // phase velocities stand alike against the layer velocities, so its lanes
+    // take the same evanescent / oscillatory branches layer by layer
+    const long long ncol = (long long)nx * ny;
+    const int ip = (int)(gid / ncol);
+    const int col = (int)(gid % ncol);
     const int ix = col / ny, iy = col % ny;
     const LayerConst& L = *Lp;
     float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];
@@ -339,8 +347,12 @@ dispersion_dcdvs_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
                         const LayerConst* __restrict__ Lp, double* dcdvs) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= (long long)nx * ny * nper) return;
-    const int ip = (int)(gid % nper);
-    const int col = (int)(gid / nper);
+    // period-major: a warp takes 32 neighbouring columns at one period, whose
+    // phase velocities stand alike against the layer velocities, so its lanes
+    // take the same evanescent / oscillatory branches layer by layer
+    const long long ncol = (long long)nx * ny;
+    const int ip = (int)(gid / ncol);
+    const int col = (int)(gid % ncol);
     const int ix = col / ny, iy = col % ny;
     const LayerConst& L = *Lp;
     float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];

@@ -33,8 +33,12 @@ depthkernel_group_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d
                          double* sen_vs, double* sen_vp, double* sen_rho) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= (long long)nx * ny * nper) return;
-    const int ip = (int)(gid % nper);
-    const int col = (int)(gid / nper);
+    // period-major: a warp takes 32 neighbouring columns at one period, whose
+    // phase velocities stand alike against the layer velocities, so its lanes
+    // take the same evanescent / oscillatory branches layer by layer
+    const long long ncol = (long long)nx * ny;
+    const int ip = (int)(gid / ncol);
+    const int col = (int)(gid % ncol);
     const int ix = col / ny, iy = col % ny;
     const LayerConst& L = *Lp;
     float vp[sk::MMAX], vs[sk::MMAX], rho[sk::MMAX];
