@@ -9,8 +9,8 @@
 // every boundary cell equal to the updated cell at the clamped index
 // (ix, iy, k) -> (clamp(ix, 1, nx-2), clamp(iy, 1, ny-2), clamp(k, 1, nz-2)),
 // so one pass writes the whole step: a boundary thread recomputes the update
-// of its clamped interior cell.  HBM-bound: one read and one write of the
-// field per step, neighbours from L1/L2.
+// of its clamped interior cell.  One read and one write of the field per
+// step, neighbours from L1/L2.
 #include "launch.h"
 
 namespace sa {
@@ -56,6 +56,63 @@ __global__ void __launch_bounds__(256) pde_step_kernel(PdeConst P, const double*
     }
 }
 
+// Division by an invariant divisor d as a multiply-high and a shift
+// (Granlund and Montgomery, PLDI 1994, section 4): s = ceil(log2 d),
+// m = floor(2^32 (2^s - d) / d) + 1, q = (umulhi(n, m) + n) >> s, exact for
+// every n < 2^31 (the sum then fits 32 bits).
+struct FastDiv {
+    unsigned d, m, s;
+};
+static FastDiv make_fastdiv(unsigned d) {
+    unsigned s = 0;
+    while ((1ull << s) < d) s++;
+    const unsigned long long m = ((1ull << 32) * ((1ull << s) - d)) / d + 1;
+    return {d, (unsigned)m, s};
+}
+__device__ __forceinline__ unsigned fdiv_q(unsigned n, const FastDiv& f) {
+    return (__umulhi(n, f.m) + n) >> f.s;
+}
+
+// The same step with 32-bit cell indices (fields below 2^31 cells): the
+// row, column and depth of a cell from two multiply-high divisions instead
+// of 64-bit divisions, which made the index arithmetic the bulk of the
+// instructions.
+__global__ void __launch_bounds__(256) pde_step_kernel32(PdeConst P, FastDiv fz, FastDiv fy,
+                                                         const double* __restrict__ u,
+                                                         double* __restrict__ out,
+                                                         const double* __restrict__ rowX,
+                                                         const double* __restrict__ rowY,
+                                                         const double* __restrict__ depE) {
+    const unsigned n = (unsigned)P.nx * P.ny * P.nz;
+    const unsigned sy = (unsigned)P.nz, sx = (unsigned)P.ny * P.nz;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned col = fdiv_q(i, fz);
+        const int k = (int)(i - col * fz.d);
+        const unsigned ixu = fdiv_q(col, fy);
+        const int iy = (int)(col - ixu * fy.d);
+        const int ix = (int)ixu;
+        const int cx = min(max(ix, 1), P.nx - 2);
+        const int cy = min(max(iy, 1), P.ny - 2);
+        const int ck = min(max(k, 1), P.nz - 2);
+        const unsigned c = ((unsigned)cx * P.ny + cy) * P.nz + ck;
+        const double center = u[c];
+        // src/postproc.cpp:91-124
+        const double d2u_dx2 = rowX[cy] * (u[c + sx] + u[c - sx] - 2.0 * center);
+        const double u_jp1 = u[c + sy];
+        const double u_jm1 = u[c - sy];
+        const double d2u_dy2 = P.B * (u_jp1 + u_jm1 - 2.0 * center);
+        const double du_dy = rowY[cy] * (u_jp1 - u_jm1);
+        const double lat_term = d2u_dy2 - du_dy;
+        const double u_kp1 = u[c + 1];
+        const double u_km1 = u[c - 1];
+        const double d2u_dz2 = P.D * (u_kp1 + u_km1 - 2.0 * center);
+        const double du_dz = depE[ck] * (u_kp1 - u_km1);
+        const double depth_term = d2u_dz2 - du_dz;
+        // :453, dt = 1
+        out[i] = center + 1.0 * (d2u_dx2 + lat_term + depth_term);
+    }
+}
+
 cudaError_t launch_pde_smooth(int nx, int ny, int nz, double B, double D, const double* rowX,
                               const double* rowY, const double* depE, int nstep, double* field,
                               double* work, cudaStream_t st) {
@@ -67,8 +124,11 @@ cudaError_t launch_pde_smooth(int nx, int ny, int nz, double B, double D, const 
     const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
     double* a = field;
     double* b = work;
+    const bool idx32 = n < (1ull << 31);
+    const FastDiv fz = make_fastdiv((unsigned)nz), fy = make_fastdiv((unsigned)ny);
     for (int s = 0; s < nstep; s++) {
-        pde_step_kernel<<<blocks, 256, 0, st>>>(P, a, b, rowX, rowY, depE);
+        if (idx32) pde_step_kernel32<<<blocks, 256, 0, st>>>(P, fz, fy, a, b, rowX, rowY, depE);
+        else pde_step_kernel<<<blocks, 256, 0, st>>>(P, a, b, rowX, rowY, depE);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         double* t = a;

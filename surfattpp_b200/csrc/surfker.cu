@@ -85,16 +85,17 @@ __global__ void math_eval_kernel(int f, size_t n, const double* __restrict__ x,
 // SurfGrid::compute_dispersion_kernel (src/surf_grid.cpp:247-305) through
 // depthkernelHTI1d (src/surfdisp.cpp:481-547): one thread per (column, period)
 // runs sregn96_hti at the column's phase velocity cp.
-#ifndef SK_DEPTH_MINB
-#define SK_DEPTH_MINB 10
-#endif
-__global__ void __launch_bounds__(64, SK_DEPTH_MINB)
+__global__ void SK_DEPTH_BOUNDS
 depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
                    const double* __restrict__ periods, const double* __restrict__ cp_plane,
                    const LayerConst* __restrict__ Lp, double* sen_vs, double* sen_vp,
                    double* sen_rho, double* sen_hs) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= (long long)nx * ny * nper) return;
+    long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool live = gid < (long long)nx * ny * nper;
+    if (!live) {
+        if (SK_DEPTH_PHASED == 0) return;
+        gid = (long long)nx * ny * nper - 1;   // meets the barriers, stores nothing
+    }
     // period-major: a warp takes 32 neighbouring columns at one period, whose
     // phase velocities stand alike against the layer velocities, so its lanes
     // take the same evanescent / oscillatory branches layer by layer
@@ -133,9 +134,10 @@ depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int 
     const double omega = twopi / periods[ip];
     double c = cp_plane[(size_t)ip * nx * ny + ix + (size_t)nx * iy];
     const double wvno = omega / c;
-    sk::svfunc(W, omega, wvno);
+    sk::svfunc_phased(W, omega, wvno);
     double ugr, fac;
     sk::energy(W, omega, wvno, ugr, fac);
+    if (!live) return;
     if (fabs(c) < 1.0e-36) c = 0.0;
     // sprayl (sregn96.f90:1592-1638): only the velocity and density kernels
     // are returned here
@@ -167,15 +169,19 @@ depthkernel_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int 
 // t1 = t(1 + 0.005), t2 = t(1 - 0.005) from cp, cp1, cp2).  sen_vs = dc/db
 // (du/db), sen_rho = dc/drho (du/drho) of the first nz layers,
 // earth-flattening corrected (splove, :631-670).  Models without water.
-__global__ void __launch_bounds__(64, SK_DEPTH_MINB)
+__global__ void SK_DEPTH_BOUNDS
 depthkernel_love_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
                         const double* __restrict__ periods, const double* __restrict__ p1,
                         const double* __restrict__ p2, const double* __restrict__ cp_plane,
                         const double* __restrict__ cp1_plane,
                         const double* __restrict__ cp2_plane, int igr,
                         const LayerConst* __restrict__ Lp, double* sen_vs, double* sen_rho) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= (long long)nx * ny * nper) return;
+    long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool live = gid < (long long)nx * ny * nper;
+    if (!live) {
+        if (SK_DEPTH_PHASED == 0) return;
+        gid = (long long)nx * ny * nper - 1;   // meets the barriers, stores nothing
+    }
     // period-major: a warp takes 32 neighbouring columns at one period, whose
     // phase velocities stand alike against the layer velocities, so its lanes
     // take the same evanescent / oscillatory branches layer by layer
@@ -193,9 +199,12 @@ depthkernel_love_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
     const size_t pix = (size_t)ip * nx * ny + ix + (size_t)nx * iy;
     const double t = periods[ip], cp = cp_plane[pix];
     double omega = twopi / t;
+    SK_PHASE();
     sk::lv_shfunc(W, omega, omega / cp);
+    SK_PHASE();
     sk::lv_energy(W, omega, omega / cp);
     if (!igr) {
+        if (!live) return;
         const double x = (3.0 * cp) / ((2.0 * ar) * omega);
         const double tm = sqrt(1.0 + x * x);
         const double tm3 = tm * tm * tm;
@@ -215,7 +224,9 @@ depthkernel_love_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
     const double t1 = p1[ip], t2 = p2[ip];
     omega = twopi / t1;
     const double c1 = cp1_plane[pix];
+    SK_PHASE();
     sk::lv_shfunc(W, omega, omega / c1);
+    SK_PHASE();
     sk::lv_energy(W, omega, omega / c1);
     for (int k = 0; k < nz; k++) {
         b1[k] = W.dcdb[k];
@@ -223,8 +234,11 @@ depthkernel_love_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
     }
     omega = twopi / t2;
     const double c2 = cp2_plane[pix];
+    SK_PHASE();
     sk::lv_shfunc(W, omega, omega / c2);
+    SK_PHASE();
     sk::lv_energy(W, omega, omega / c2);   // W.dc* now hold this evaluation
+    if (!live) return;
     const double uc1 = cg / cp;
     omega = twopi / t;
     const double x = (3.0 * cp) / ((2.0 * ar) * omega);
@@ -246,7 +260,8 @@ cudaError_t launch_depthkernel_love(int nx, int ny, int nz, const double* vs3d, 
                                     int igr, const void* layer_const, double* sen_vs,
                                     double* sen_rho, cudaStream_t st) {
     const long long n = (long long)nx * ny * nper;
-    depthkernel_love_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
+    depthkernel_love_kernel<<<(unsigned)((n + SK_DEPTH_BLOCK - 1) / SK_DEPTH_BLOCK), SK_DEPTH_BLOCK, 0,
+                              st>>>(
         nx, ny, nz, vs3d, nper, periods, p1, p2, cp, cp1, cp2, igr,
         reinterpret_cast<const LayerConst*>(layer_const), sen_vs, sen_rho);
     return cudaGetLastError();
@@ -448,7 +463,7 @@ cudaError_t launch_depthkernel(int nx, int ny, int nz, const double* vs3d, int n
                                double* sen_vs, double* sen_vp, double* sen_rho, cudaStream_t st,
                                double* sen_hs) {
     const long long n = (long long)nx * ny * nper;
-    depthkernel_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
+    depthkernel_kernel<<<(unsigned)((n + SK_DEPTH_BLOCK - 1) / SK_DEPTH_BLOCK), SK_DEPTH_BLOCK, 0, st>>>(
         nx, ny, nz, vs3d, nper, periods, cp, reinterpret_cast<const LayerConst*>(layer_const),
         sen_vs, sen_vp, sen_rho, sen_hs);
     return cudaGetLastError();

@@ -1445,9 +1445,9 @@ __device__ inline void down(RW& W, double omega, double wvno) {
 }
 
 // sregn96.f90:193-399
-__device__ inline void svfunc(RW& W, double omega, double wvno) {
-    up(W, omega, wvno);
-    down(W, omega, wvno);
+// svfunc after up() and down(): the eigenfunctions from the compound
+// matrices and the propagator vectors.
+__device__ inline void svfunc_combine(RW& W) {
     const double f1213 = -W.cd[0][1];
     W.ur[0] = W.cd[0][2] / W.cd[0][1];
     W.uz[0] = 1.0;
@@ -1488,6 +1488,43 @@ __device__ inline void svfunc(RW& W, double omega, double wvno) {
             W.tr[i - 1] = 0.0;
         }
     }
+}
+
+__device__ inline void svfunc(RW& W, double omega, double wvno) {
+    up(W, omega, wvno);
+    down(W, omega, wvno);
+    svfunc_combine(W);
+}
+
+// The depth kernels run blocks of SK_DEPTH_PHASED threads, one block per SM
+// (96 registers each), and a block barrier between the eigenfunction
+// routines keeps all warps of an SM on the same routine: up, down, the
+// eigenfunctions, the energy integrals.  Launched as 64-thread blocks at 10
+// per SM without barriers (SK_DEPTH_PHASED 0), the blocks drift apart, every
+// routine's code is in flight on an SM at once and the warps stall on
+// instruction fetch (C3 Rayleigh phase kernels: 71.2 ms against 55.2 ms
+// phased).  Threads past the last item repeat it, to meet the barriers, and
+// store nothing.
+#ifndef SK_DEPTH_PHASED
+#define SK_DEPTH_PHASED 640
+#endif
+#if SK_DEPTH_PHASED > 0
+#define SK_DEPTH_BLOCK SK_DEPTH_PHASED
+#define SK_DEPTH_BOUNDS __launch_bounds__(SK_DEPTH_PHASED, 1)
+#define SK_PHASE() __syncthreads()
+#else
+#define SK_DEPTH_BLOCK 64
+#define SK_DEPTH_BOUNDS __launch_bounds__(64, 10)
+#define SK_PHASE() ((void)0)
+#endif
+__device__ inline void svfunc_phased(RW& W, double omega, double wvno) {
+    SK_PHASE();
+    up(W, omega, wvno);
+    SK_PHASE();
+    down(W, omega, wvno);
+    SK_PHASE();
+    svfunc_combine(W);
+    SK_PHASE();
 }
 
 // sregn96.f90:1326-1404

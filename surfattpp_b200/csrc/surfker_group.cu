@@ -11,9 +11,6 @@
 #define SK_MATH_NOINLINE 0
 #include "surfker_dev.cuh"
 
-#ifndef SK_DEPTH_MINB
-#define SK_DEPTH_MINB 10
-#endif
 
 namespace sa {
 using sk::LayerConst;
@@ -24,15 +21,19 @@ using sk::LayerConst;
 // the three phase-velocity planes, the finite-difference group kernels and
 // their earth-flattening conversion.  As in the reference, the first term of
 // du/dm reads the kernels left by the last (t2) evaluation.
-__global__ void __launch_bounds__(64, SK_DEPTH_MINB)
+__global__ void SK_DEPTH_BOUNDS
 depthkernel_group_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
                          const double* __restrict__ periods, const double* __restrict__ p1,
                          const double* __restrict__ p2, const double* __restrict__ cp_plane,
                          const double* __restrict__ cp1_plane,
                          const double* __restrict__ cp2_plane, const LayerConst* __restrict__ Lp,
                          double* sen_vs, double* sen_vp, double* sen_rho) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= (long long)nx * ny * nper) return;
+    long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool live = gid < (long long)nx * ny * nper;
+    if (!live) {
+        if (SK_DEPTH_PHASED == 0) return;
+        gid = (long long)nx * ny * nper - 1;   // meets the barriers, stores nothing
+    }
     // period-major: a warp takes 32 neighbouring columns at one period, whose
     // phase velocities stand alike against the layer velocities, so its lanes
     // take the same evanescent / oscillatory branches layer by layer
@@ -73,7 +74,7 @@ depthkernel_group_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d
     double ugr, fac;
     // period t (:1908-1918)
     double omega = twopi / t;
-    sk::svfunc(W, omega, omega / cp);
+    sk::svfunc_phased(W, omega, omega / cp);
     sk::energy(W, omega, omega / cp, ugr, fac);
     const double cg = ugr;
     double a0[sk::MMAX], b0[sk::MMAX], r0[sk::MMAX], a1[sk::MMAX], b1[sk::MMAX], r1[sk::MMAX];
@@ -85,7 +86,7 @@ depthkernel_group_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d
     // period t1 (:1921-1930)
     omega = twopi / t1;
     const double c1 = cp1_plane[pix];
-    sk::svfunc(W, omega, omega / c1);
+    sk::svfunc_phased(W, omega, omega / c1);
     sk::energy(W, omega, omega / c1, ugr, fac);
     for (int k = 0; k < nz; k++) {
         a1[k] = W.dcda[k];
@@ -95,8 +96,9 @@ depthkernel_group_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d
     // period t2 (:1933-1942); W.dc* now hold this evaluation
     omega = twopi / t2;
     const double c2 = cp2_plane[pix];
-    sk::svfunc(W, omega, omega / c2);
+    sk::svfunc_phased(W, omega, omega / c2);
     sk::energy(W, omega, omega / c2, ugr, fac);
+    if (!live) return;
     // :1945-1971
     const double uc1 = cg / cp;
     const double ar = 6371.0;
@@ -122,7 +124,8 @@ cudaError_t launch_depthkernel_group(int nx, int ny, int nz, const double* vs3d,
                                      const void* layer_const, double* sen_vs, double* sen_vp,
                                      double* sen_rho, cudaStream_t st) {
     const long long n = (long long)nx * ny * nper;
-    depthkernel_group_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(
+    depthkernel_group_kernel<<<(unsigned)((n + SK_DEPTH_BLOCK - 1) / SK_DEPTH_BLOCK), SK_DEPTH_BLOCK,
+                               0, st>>>(
         nx, ny, nz, vs3d, nper, periods, p1, p2, cp, cp1, cp2,
         reinterpret_cast<const LayerConst*>(layer_const), sen_vs, sen_vp, sen_rho);
     return cudaGetLastError();
