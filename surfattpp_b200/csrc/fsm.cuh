@@ -387,6 +387,183 @@ __device__ __forceinline__ float fsm_update_delta(float u, float t0, float t0x, 
     return best;
 }
 
+// Pairs of FP32 values in one 64-bit register, for the packed FP32
+// operations of sm_100 (add / sub / mul / fma .rn.f32x2).  Each half rounds
+// exactly as the scalar operation of the same name, so an update written
+// with them returns the scalar update's bits.
+struct F2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ F2 p2(float a, float b) {
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ F2 b2(float a) { return p2(a, a); }
+__device__ __forceinline__ void u2(F2 x, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ F2 fa2(F2 a, F2 b) {
+    F2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 fs2(F2 a, F2 b) {
+    F2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 fm2(F2 a, F2 b) {
+    F2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 ff2(F2 a, F2 b, F2 c) {
+    F2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+// exact negation of both halves (signs of zeros included)
+__device__ __forceinline__ F2 neg2(F2 a) { return {a.v ^ 0x8000000080000000ull}; }
+
+// fsm_update_delta with the arithmetic of two stencils in each packed
+// operation: the quadrants sharing an x neighbour (y neighbour below /
+// above) and the axis updates of one axis (neighbour before / after), every
+// candidate then tested and folded into the minimum in the scalar form's
+// order.  Same operations, operands and order per stencil as
+// fsm_update_delta: the result is bit for bit the same.
+template <bool ISO>
+__device__ __forceinline__ float fsm_update_delta2(float u, float t0, float t0x, float t0y,
+                                                   float aij, float bij, float cij, float fij,
+                                                   float idx, float idy,
+                                                   const Nb<float, float>& xm,
+                                                   const Nb<float, float>& xp,
+                                                   const Nb<float, float>& ym,
+                                                   const Nb<float, float>& yp) {
+    const float det = ISO ? fm(aij, bij) : ff(aij, bij, -fm(cij, cij));
+    const float k = fm(t0, idx);
+    const float m = fm(t0, idy);
+    const float f2 = fm(fij, fij);
+    const float c2 = fm(2.f, cij);
+    float best = u;
+    // members: sy = -1 (ym), sy = +1 (yp)
+    const F2 uy = p2(ym.v, yp.v);
+    const F2 msy = p2(m, -m);
+    const F2 B1 = fa2(b2(t0y), msy);
+#pragma unroll
+    for (int px = 0; px < 2; px++) {   // sx = -1: quadrants 0, 1; sx = +1: 2, 3
+        const int sx = px == 0 ? -1 : 1;
+        const Nb<float, float>& nxn = (sx < 0) ? xm : xp;
+        const float ux = nxn.v;
+        const float A0 = ff(t0x, ux, t0x);
+        const float A1 = sx < 0 ? fa(t0x, k) : fs(t0x, k);
+        const F2 B0 = ff2(msy, fs2(b2(ux), uy), b2(ff(t0y, ux, t0y)));
+        const float aA0 = fm(aij, A0);
+        const F2 bB0 = fm2(b2(bij), B0);
+        F2 al, be, ga;
+        if (ISO) {
+            al = ff2(b2(fm(aij, A1)), b2(A1), fm2(fm2(b2(bij), B1), B1));
+            be = fm2(b2(2.f), ff2(b2(aA0), b2(A1), fm2(bB0, B1)));
+            ga = ff2(b2(aA0), b2(A0), ff2(bB0, B0, b2(-f2)));
+        } else {
+            al = ff2(b2(fm(aij, A1)), b2(A1),
+                     ff2(fm2(b2(bij), B1), B1, neg2(fm2(b2(fm(c2, A1)), B1))));
+            be = fm2(b2(2.f),
+                     ff2(b2(aA0), b2(A1),
+                         ff2(bB0, B1, neg2(fm2(b2(cij), ff2(b2(A0), B1, fm2(b2(A1), B0)))))));
+            ga = ff2(b2(aA0), b2(A0), ff2(bB0, B0, ff2(b2(-fm(c2, A0)), B0, b2(-f2))));
+        }
+        const F2 disc = ff2(be, be, neg2(fm2(fm2(b2(4.f), al), ga)));
+        float dv[2], alv[2], bev[2];
+        u2(disc, dv[0], dv[1]);
+        u2(al, alv[0], alv[1]);
+        u2(be, bev[0], bev[1]);
+        bool ok[2];
+        float sq[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            ok[e] = nxn.has && (e == 0 ? ym.has : yp.has) && dv[e] >= 0.f &&
+                    fabsf(alv[e]) >= 1e-30f;
+            sq[e] = copysignf(fsqrt(fmaxf(dv[e], 0.f)), bev[e]);
+        }
+        const F2 qq = fm2(b2(-0.5f), fa2(be, p2(sq[0], sq[1])));
+        float qv[2];
+        u2(qq, qv[0], qv[1]);
+        // the second root as ga / qq also when qq == 0 (see fsm_update_delta)
+        F2 Dr[2];
+        Dr[0] = fm2(qq, p2(frcp(alv[0]), frcp(alv[1])));
+        Dr[1] = fm2(ga, p2(frcp(qv[0]), frcp(qv[1])));
+        bool take[2][2];
+        float cand[2][2];
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const F2 Tx = ff2(b2(A1), Dr[r], b2(A0));
+            const F2 Ty = ff2(B1, Dr[r], B0);
+            F2 chx = Tx, chy = Ty;
+            if (!ISO) {
+                chx = ff2(b2(aij), Tx, neg2(fm2(b2(cij), Ty)));
+                chy = ff2(b2(bij), Ty, neg2(fm2(b2(cij), Tx)));
+            }
+            float xv[2], yv[2], cv[2];
+            u2(chx, xv[0], xv[1]);
+            u2(chy, yv[0], yv[1]);
+            u2(fa2(b2(ux), Dr[r]), cv[0], cv[1]);
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int sy = e == 0 ? -1 : 1;
+                take[r][e] = ok[e] && fminf(-sx * xv[e], -sy * yv[e]) >= 0.f;
+                cand[r][e] = cv[e];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 2; e++)
+#pragma unroll
+            for (int r = 0; r < 2; r++) best = take[r][e] ? fminf(best, cand[r][e]) : best;
+    }
+    const bool okd = det > 0.f;
+    const float disx = fsqrt(fmaxf(fdiv(fm(f2, bij), det), 0.f));
+    const float disy = fsqrt(fmaxf(fdiv(fm(f2, aij), det), 0.f));
+    // axis updates, the neighbours before (s = -1) and after (s = +1) of one
+    // axis in one pair: (T0 tau)_axis = g*tau - s*kk*(tau - tau_n) = +-dis
+    auto axis_pair = [&](const Nb<float, float>& n0, const Nb<float, float>& n1, float g, float kk,
+                         float dis) {
+        const F2 nv = p2(n0.v, n1.v), nx = p2(n0.x, n1.x);
+        const F2 g1 = ff2(b2(g), nv, b2(g));
+        float den[2];
+        u2(fa2(b2(g), p2(kk, -kk)), den[0], den[1]);
+        const F2 rden = p2(frcp(den[0]), frcp(den[1]));
+        // (1+c)*t0 >= (1+u_n)*T0_n  and  1+c > 0.5*(1+u_n)
+        const F2 kn = fs2(b2(t0), ff2(nv, nx, nx));
+        float hv[2];
+        u2(ff2(b2(0.5f), nv, b2(-0.5f)), hv[0], hv[1]);
+        float cv[2][2], tv[2][2];
+#pragma unroll
+        for (int sgn = 0; sgn < 2; sgn++) {
+            const F2 c = ff2(fs2(b2(sgn == 0 ? dis : -dis), g1), rden, nv);
+            u2(c, cv[sgn][0], cv[sgn][1]);
+            u2(ff2(c, b2(t0), kn), tv[sgn][0], tv[sgn][1]);
+        }
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const bool ok = okd && (e == 0 ? n0.has : n1.has);
+#pragma unroll
+            for (int sgn = 0; sgn < 2; sgn++) {
+                const bool take = ok && tv[sgn][e] >= 0.f && cv[sgn][e] > hv[e];
+                best = take ? fminf(best, cv[sgn][e]) : best;
+            }
+        }
+    };
+    axis_pair(xm, xp, t0x, k, disx);
+    axis_pair(ym, yp, t0y, m, disy);
+    return best;
+}
+
+// FSM_PACKED 1: the forward update in packed FP32 pairs (fsm_update_delta2),
+// 0: the scalar form; both give the same bits.
+#ifndef FSM_PACKED
+#define FSM_PACKED 1
+#endif
+
 // FP32 forward: field u = tau - 1, increment-form update.
 template <bool ISO, bool ROLLED = true>
 struct FwdPolicyDelta32 : FwdBase<float, ISO, ROLLED> {
@@ -402,10 +579,17 @@ struct FwdPolicyDelta32 : FwdBase<float, ISO, ROLLED> {
                             const Nb<float, float>& xp, const Nb<float, float>& ym,
                             const Nb<float, float>& yp, int xd, int yd) const {
         if (row_fixed && ix >= fix_x0 && ix <= fix_x1) return cur.v;
+#if FSM_PACKED
+        return fsm_update_delta2<ISO>(cur.v, cur.x, (float)xd * cur.gx, (float)yd * cur.gy,
+                                      this->ca(cur), this->cb(cur),
+                                      (float)(xd * yd) * this->cc(cur), cur.f, idx, idy, xm, xp,
+                                      ym, yp);
+#else
         return fsm_update_delta<ISO>(cur.v, cur.x, (float)xd * cur.gx, (float)yd * cur.gy,
                                      this->ca(cur), this->cb(cur),
                                      (float)(xd * yd) * this->cc(cur), cur.f, idx, idy, xm, xp,
                                      ym, yp);
+#endif
     }
     __device__ void account(const Cell& cur, float nv, double& l1, double& linf) const {
         const double d = __dmul_rn(fabs(__dsub_rn((double)nv, (double)cur.vs)), (double)cur.x);
