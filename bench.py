@@ -144,7 +144,7 @@ class Clocks:
 # every sweep the reference performs; the kernel skips cells that provably
 # stay unchanged, so it moves less.  Traffic scales with cell updates, so a
 # full launch moves algorithmic x this ratio.
-TRAFFIC_PER_ALGO_BYTE = {"fp32": 45.018027e9 / 61.718708e9}
+TRAFFIC_PER_ALGO_BYTE = {"fp32": (36.528193e9 + 8.616214e9) / 61.718708e9}
 
 
 def peaks():
