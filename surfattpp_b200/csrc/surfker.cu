@@ -35,10 +35,13 @@ using sk::LayerConst;
 // the C3 dispersion 1.5x and the depth kernels 1.2x faster than the
 // unconstrained allocation (128 / 202 registers), and put the 90,601 C3
 // columns in one wave.
-#ifndef SK_DISP_MINB
-#define SK_DISP_MINB 10
-#endif
-__global__ void __launch_bounds__(64, SK_DISP_MINB)
+// Grids with more columns than one wave at 10 blocks per SM take the
+// 16-block form (64 registers, a few more spills): with several waves the
+// extra warps hide more FP64 latency (C5, 361,201 columns: 700 -> 659 ms),
+// while a one-wave grid gains no warps and only pays the spills (C3: 122 ->
+// 134 ms).  Both forms compute the same bits.
+template <int MINB>
+__global__ void __launch_bounds__(64, MINB)
 surfdisp_columns_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d, int nper,
                         const double* __restrict__ periods, int iflsph, int iwave, int igr,
                         const LayerConst* __restrict__ Lp, double* svel, int* status) {
@@ -452,9 +455,16 @@ cudaError_t launch_surfdisp_columns(int nx, int ny, int nz, const double* vs3d, 
                                     const void* layer_const, double* svel, int* status,
                                     cudaStream_t st) {
     const int n = nx * ny;
-    surfdisp_columns_kernel<<<(n + 63) / 64, 64, 0, st>>>(
-        nx, ny, nz, vs3d, nper, periods, iflsph, iwave, igr,
-        reinterpret_cast<const LayerConst*>(layer_const), svel, status);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const LayerConst* Lp = reinterpret_cast<const LayerConst*>(layer_const);
+    if (n > nsm * 10 * 64)
+        surfdisp_columns_kernel<16><<<(n + 63) / 64, 64, 0, st>>>(
+            nx, ny, nz, vs3d, nper, periods, iflsph, iwave, igr, Lp, svel, status);
+    else
+        surfdisp_columns_kernel<10><<<(n + 63) / 64, 64, 0, st>>>(
+            nx, ny, nz, vs3d, nper, periods, iflsph, iwave, igr, Lp, svel, status);
     return cudaGetLastError();
 }
 

@@ -58,6 +58,24 @@ def test_fwdsurf_c3_rows_match_oracle(orc, gpu):
     assert np.array_equal(got.cpu().numpy(), ref)
 
 
+def test_fwdsurf_multi_wave_grid_matches_oracle(orc, gpu):
+    """A grid of more columns than one wave of the 10-block launch holds
+    (24 copies of 20 C3 rows: 144,480 columns), which takes the 16-block
+    form of the dispersion kernel: every copy bit-identical to the oracle's
+    phase velocities of the 20 rows."""
+    from surfattpp_b200 import surfker
+    from surfattpp_b200 import workloads as W
+    w = W.config3()
+    vs = np.ascontiguousarray(w.vs3d[100:120])
+    ref, st = orc.fwdsurf(w.zgrid, vs, w.periods, nthreads=8)
+    big = np.ascontiguousarray(np.tile(vs, (24, 1, 1)))
+    got, status = surfker.fwdsurf(w.zgrid, _dev(big), w.periods)
+    assert st.sum() == 0 and int(status.max()) == 0
+    got = got.cpu().numpy()
+    for t in range(24):
+        assert np.array_equal(got[:, :, 20 * t:20 * (t + 1)], ref)
+
+
 @pytest.mark.parametrize("igr,iwave", [(1, 2), (0, 1), (1, 1)])
 def test_fwdsurf_group_and_love(orc, gpu, c1, igr, iwave):
     from surfattpp_b200 import surfker
