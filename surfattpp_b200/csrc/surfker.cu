@@ -56,6 +56,8 @@ surfdisp_columns_kernel(int nx, int ny, int nz, const double* __restrict__ vs3d,
         t[i] = periods[i];
         cg[i] = 0.0;
     }
+    // SK_DISP_SERIAL builds the searches in the Fortran's call structure
+    // (same bits; 1.2-1.3x slower, lanes diverge across the call sites)
 #ifdef SK_DISP_SERIAL
     const int st = sk::surfdisp96(L, vp, vs, rho, iflsph, iwave, 1, igr, nper, t, cg);
 #else
